@@ -1,0 +1,352 @@
+/*
+ * rt_capi.h - C ABI of the B200 path tracer (optixrender_b200).
+ *
+ * This is the drop-in boundary for the reference renderer's host API
+ * (GraphicsEnthusiast/OptiXRender).  Each entry point names the reference
+ * interface it replaces as `file:line` inside that project.  All functions
+ * return an rt_status (0 = RT_OK); nothing throws across the ABI and nothing
+ * calls exit().  rt_last_error_message() returns a thread-local description of
+ * the last failure on the calling thread.
+ *
+ * Pointers are plain host pointers unless a parameter says "device".  The
+ * library copies everything it needs, so a scene may be destroyed once a
+ * renderer has been created from it.
+ */
+#ifndef RT_CAPI_H
+#define RT_CAPI_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define RT_API __declspec(dllexport)
+#else
+#define RT_API __attribute__((visibility("default")))
+#endif
+
+typedef int32_t rt_status;
+
+enum {
+    RT_OK = 0,
+    RT_ERR_INVALID_ARG = 1,
+    RT_ERR_CUDA = 2,
+    RT_ERR_OUT_OF_MEMORY = 3,
+    RT_ERR_IO = 4,
+    RT_ERR_PARSE = 5,
+    RT_ERR_STATE = 6,
+    RT_ERR_TIMEOUT = 7,
+    RT_ERR_UNSUPPORTED = 8,
+    RT_ERR_DEVICE_WATCHDOG = 9
+};
+
+/* ---------------------------------------------------------------------- */
+/* Scene description types                                                 */
+/* ---------------------------------------------------------------------- */
+
+/* Material types; values match enum MaterialType, core/include/Scene.h:59-68. */
+enum {
+    RT_MAT_DIFFUSE = 0,
+    RT_MAT_CONDUCTOR = 1,
+    RT_MAT_DIELECTRIC = 2,
+    RT_MAT_PLASTIC = 3,
+    RT_MAT_METAL_WORKFLOW = 4,
+    RT_MAT_THIN_DIELECTRIC = 5,
+    RT_MAT_CLEARCOATED_CONDUCTOR = 6,
+    RT_MAT_DIFFUSE_TRANSMITTER = 7
+};
+
+/* struct Material, core/include/Scene.h:70-116 (texture objects are replaced
+ * by texture ids; the LUT pointers are owned by the renderer).  Call
+ * rt_material_default() for the reference's field defaults. */
+typedef struct rt_material {
+    int32_t type;
+    float albedo[3];
+    float roughness;          /* reference units: alpha = roughness^2 */
+    float anisotropy;
+    float eta[3];
+    float k[3];
+    float int_ior;
+    float ext_ior;
+    int32_t nonlinear;
+    float specular[3];
+    float metallic;
+    float coat_weight;
+    float coat_roughness_u;
+    float coat_roughness_v;
+    /* texture ids (-1 = constant): albedo, roughness, anisotropy, specular,
+     * metallic, coat_roughness_u, coat_roughness_v, normal */
+    int32_t texture_ids[8];
+} rt_material;
+
+/* Light types: enum LightType, core/include/Scene.h:138-141, plus a point light. */
+enum { RT_LIGHT_QUAD = 0, RT_LIGHT_SPHERE = 1, RT_LIGHT_POINT = 2 };
+
+/* struct Light, core/include/Scene.h:143-155.  A quad emits towards
+ * -normalize(cross(u, v)) unless double_side is set.  A point light uses
+ * `radiance` as radiant intensity (W/sr) at `position`. */
+typedef struct rt_light {
+    int32_t type;
+    int32_t double_side;
+    float radiance[3];
+    float position[3];
+    float u[3];
+    float v[3];
+    float radius;
+    int32_t medium;
+} rt_light;
+
+/* Phase types: enum PhaseType, core/include/Scene.h:33-36. */
+enum { RT_PHASE_ISOTROPIC = 0, RT_PHASE_HENYEY_GREENSTEIN = 1 };
+/* Medium types: enum MediumType, core/include/Scene.h:44-46, plus a density grid. */
+enum { RT_MEDIUM_HOMOGENEOUS = 0, RT_MEDIUM_GRID = 1 };
+
+/* struct Medium, core/include/Scene.h:48-55.  For RT_MEDIUM_GRID the
+ * coefficients are multiplied by a trilinearly interpolated density read from
+ * `density` (grid_res[0]*grid_res[1]*grid_res[2] floats, x fastest) over the
+ * box [bounds_min, bounds_max]; outside the box the density is zero.  The grid
+ * is tracked with delta tracking against a majorant grid of majorant_res^3
+ * cells (0 = 8). */
+typedef struct rt_medium {
+    int32_t type;
+    int32_t phase;
+    float g[3];
+    float sigma_s[3];
+    float sigma_a[3];
+    float scale;
+    int32_t grid_res[3];
+    int32_t majorant_res;
+    float bounds_min[3];
+    float bounds_max[3];
+    const float* density;
+} rt_medium;
+
+/* One triangle mesh, the input of Scene::AddMesh (core/src/Scene.cpp:22-64,
+ * TriangleMesh::LoadMesh core/src/Scene.cpp:83-179).  If `indices` is NULL the
+ * positions are already de-indexed (3 vertices per triangle).  Missing normals
+ * become the face normal and missing texcoords become (0,0),(1,0),(0,1), as
+ * in Scene.cpp:150-165. */
+typedef struct rt_mesh_desc {
+    const float* positions;   /* 3 floats per vertex */
+    const float* normals;     /* optional, 3 floats per vertex */
+    const float* texcoords;   /* optional, 2 floats per vertex */
+    const int32_t* indices;   /* optional, 3 per triangle */
+    int64_t num_vertices;
+    int64_t num_triangles;
+} rt_mesh_desc;
+
+/* struct Camera, core/include/Scene.h:11-20.  fov_y_deg <= 0 keeps the
+ * reference's fixed screen height of 0.66 (core/src/Renderer.cpp:803). */
+typedef struct rt_camera {
+    float from[3];
+    float at[3];
+    float up[3];
+    int32_t medium;
+    float fov_y_deg;
+} rt_camera;
+
+/* enum FilterType, core/include/Scene.h:24-29. */
+enum { RT_FILTER_BOX = 0, RT_FILTER_TENT = 1, RT_FILTER_TRIANGLE = 2, RT_FILTER_GAUSSIAN = 3 };
+/* Random streams: RT_RNG_LCG is the reference's gdt::LCG<16> seeded per pixel
+ * and frame (common/gdt/gdt/random/random.h:29-68), consumed sample after
+ * sample; RT_RNG_PCG32 gives every (pixel, sample) path its own PCG32 stream. */
+enum { RT_RNG_LCG = 0, RT_RNG_PCG32 = 1 };
+/* Output mappings: the reference's luminance Reinhard + gamma 2.2
+ * (core/cuda/PostProcessing.cu:18-48), ACES filmic + sRGB, or a plain clamp. */
+enum { RT_TONEMAP_REINHARD = 0, RT_TONEMAP_ACES_SRGB = 1, RT_TONEMAP_CLAMP = 2 };
+
+/* Renderer settings.  The reference keeps these in LaunchParams
+ * (core/include/LaunchParams.h:28-69) and Renderer's public fields
+ * (core/include/Renderer.h:139-143). */
+typedef struct rt_options {
+    int32_t width;
+    int32_t height;
+    int32_t spp;              /* numPixelSamples per Render() */
+    int32_t max_depth;        /* maxBounce (reference default 25) */
+    int32_t filter;           /* RT_FILTER_* (reference default Gaussian) */
+    int32_t rng;              /* RT_RNG_* */
+    int32_t rr_depth;         /* first bounce with Russian roulette (reference: 0) */
+    int32_t progressive;      /* running mean over Render() calls */
+    uint64_t seed;            /* PCG32 seed (ignored by RT_RNG_LCG) */
+    int32_t tonemap;          /* RT_TONEMAP_* */
+    int32_t wave_paths;       /* paths in flight per wave (0 = automatic) */
+    int32_t collect_stats;    /* count rays, nodes and triangles */
+    float exposure;           /* multiplier before tonemapping (1) */
+} rt_options;
+
+/* Per-render statistics. */
+typedef struct rt_render_stats {
+    int64_t paths;
+    int64_t extend_rays;
+    int64_t shadow_rays;
+    int64_t nodes_visited;     /* wide nodes fetched, extend + shadow */
+    int64_t tris_tested;
+    int64_t extend_nodes;
+    int64_t extend_tris;
+    int64_t nan_samples;
+    int32_t waves;
+    int32_t launches;          /* kernels launched by the last Render() */
+    float ms_total;            /* device time of the last Render() */
+    float ms_extend;           /* per-kernel device time (collect_stats only) */
+    float ms_shade;
+    float ms_shadow;
+    float ms_other;
+    int64_t extend_launches;
+} rt_render_stats;
+
+/* AOV kinds for rt_renderer_download_aov. */
+enum { RT_AOV_COLOR = 0, RT_AOV_ALBEDO = 1, RT_AOV_NORMAL = 2 };
+
+typedef struct rt_scene rt_scene;
+typedef struct rt_renderer rt_renderer;
+
+/* ---------------------------------------------------------------------- */
+/* Library                                                                 */
+/* ---------------------------------------------------------------------- */
+
+RT_API const char* rt_last_error_message(void);
+RT_API int32_t rt_version(void);
+
+/* Field defaults of Material (Scene.h:70-116), Light (Scene.h:143-155),
+ * Medium (Scene.h:48-55), Camera, and LaunchParams (LaunchParams.h:28-69). */
+RT_API void rt_material_default(rt_material* m);
+RT_API void rt_light_default(rt_light* l);
+RT_API void rt_medium_default(rt_medium* m);
+RT_API void rt_camera_default(rt_camera* c);
+RT_API void rt_options_default(rt_options* o);
+
+/* ---------------------------------------------------------------------- */
+/* Scene: replaces class Scene, core/include/Scene.h:195-214               */
+/* ---------------------------------------------------------------------- */
+
+/* Scene::Scene() */
+RT_API rt_status rt_scene_create(rt_scene** out);
+/* Scene::~Scene(), core/src/Scene.cpp:10-20 */
+RT_API rt_status rt_scene_destroy(rt_scene* s);
+/* Scene::AddMesh, core/src/Scene.cpp:22-64 (the material is copied per mesh
+ * as in the reference's hit records, core/src/Renderer.cpp:590). */
+RT_API rt_status rt_scene_add_mesh(rt_scene* s, const rt_mesh_desc* mesh, const rt_material* material,
+                                   int32_t out_medium, int32_t in_medium, int32_t* out_mesh_id);
+/* Scene::AddMesh with an OBJ path (TriangleMesh::LoadMesh, Scene.cpp:83-179). */
+RT_API rt_status rt_scene_add_mesh_obj(rt_scene* s, const char* obj_path, const rt_material* material,
+                                       int32_t out_medium, int32_t in_medium, int32_t* out_mesh_id);
+/* Scene::AddLight, core/src/Scene.cpp:71-73 */
+RT_API rt_status rt_scene_add_light(rt_scene* s, const rt_light* light);
+/* Scene::AddMedium, core/src/Scene.cpp:75-77 (grid media copy `density`). */
+RT_API rt_status rt_scene_add_medium(rt_scene* s, const rt_medium* medium);
+/* Scene::AddEnv, core/src/Scene.cpp:79-81 + HdrTexture, Scene.cpp:197-313:
+ * an equirectangular RGBA float image (w*h*4 floats, row 0 = bottom) scaled
+ * by `scale`; the sampling cache is built as in CalculateHdrCache. */
+RT_API rt_status rt_scene_set_env(rt_scene* s, const float* rgba, int32_t width, int32_t height, float scale);
+/* Scene::bounds, core/include/Scene.h:213 */
+RT_API rt_status rt_scene_get_bounds(const rt_scene* s, float lo[3], float hi[3]);
+RT_API rt_status rt_scene_counts(const rt_scene* s, int64_t* triangles, int32_t* meshes, int32_t* lights,
+                                 int32_t* media);
+/* SceneParser::LoadFromJson, core/src/SceneParser.cpp:3-23 and the schema of
+ * models/test.json.  Fills `opts`/`cam` (may be NULL) from the file. */
+RT_API rt_status rt_scene_load_json(rt_scene* s, const char* path, rt_options* opts, rt_camera* cam);
+RT_API rt_status rt_scene_load_json_string(rt_scene* s, const char* json, const char* base_dir,
+                                           rt_options* opts, rt_camera* cam);
+
+/* ---------------------------------------------------------------------- */
+/* Renderer: replaces class Renderer, core/include/Renderer.h:9-187        */
+/* ---------------------------------------------------------------------- */
+
+/* Renderer::Renderer(const Scene*), core/src/Renderer.cpp:39-93: builds the
+ * acceleration structure on the current CUDA device and uploads the scene. */
+RT_API rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_renderer** out);
+RT_API rt_status rt_renderer_destroy(rt_renderer* r);
+/* Public LaunchParams fields (numPixelSamples, maxBounce, filterType) and
+ * Renderer::progressive; changing them does not reset accumulation. */
+RT_API rt_status rt_renderer_set_options(rt_renderer* r, const rt_options* opts);
+RT_API rt_status rt_renderer_get_options(const rt_renderer* r, rt_options* opts);
+/* Renderer::Resize, core/src/Renderer.cpp:816-875 */
+RT_API rt_status rt_renderer_resize(rt_renderer* r, int32_t width, int32_t height);
+/* Renderer::SetCamera, core/src/Renderer.cpp:796-813 (resets accumulation) */
+RT_API rt_status rt_renderer_set_camera(rt_renderer* r, const rt_camera* cam);
+/* Use an external CUDA stream (cudaStream_t) for all work; NULL = own stream. */
+RT_API rt_status rt_renderer_set_stream(rt_renderer* r, void* cuda_stream);
+/* Renderer::Render, core/src/Renderer.cpp:635-793: one launch of `spp`
+ * samples per pixel, running-mean accumulation when progressive, and the
+ * tonemap of core/cuda/PostProcessing.cu:50-59.  Asynchronous. */
+RT_API rt_status rt_renderer_render(rt_renderer* r);
+RT_API rt_status rt_renderer_synchronize(rt_renderer* r);
+/* Renderer::DownloadPixels, core/src/Renderer.cpp:878-880 (RGBA8). */
+RT_API rt_status rt_renderer_download_rgba8(rt_renderer* r, uint32_t* pixels);
+/* Headless replacement of the GL blit: the float4 colour buffer. */
+RT_API rt_status rt_renderer_download_linear(rt_renderer* r, float* rgba);
+/* The albedo / normal AOVs the reference feeds its denoiser
+ * (core/cuda/devicePrograms.cu:518-531). */
+RT_API rt_status rt_renderer_download_aov(rt_renderer* r, int32_t kind, float* rgba);
+/* Device pointers of the float4 colour buffer and the RGBA8 buffer. */
+RT_API rt_status rt_renderer_device_buffers(rt_renderer* r, void** color_f32x4, void** rgba8);
+RT_API rt_status rt_renderer_get_stats(const rt_renderer* r, rt_render_stats* stats);
+/* Frame counter of progressive accumulation (LaunchParams::frame.frameID). */
+RT_API rt_status rt_renderer_frame_index(const rt_renderer* r, int32_t* frame);
+
+/* Ray queries against the renderer's scene: the equivalent of optixTrace,
+ * core/cuda/devicePrograms.cu:258-269 (closest hit) and :303-319 (shadow /
+ * any hit, terminate on first hit).  rays: n x 8 floats (ox oy oz tmin dx dy dz
+ * tmax).  hits: n x 4 floats (t, u, v, primitive id as float bits; id -1 on a
+ * miss).  For any-hit queries hits[i*4+3] holds 1 (occluded) or -1 bits.
+ * `device_ptrs` nonzero means both buffers are device memory. */
+RT_API rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
+                                   int32_t device_ptrs);
+
+/* ---------------------------------------------------------------------- */
+/* Shading verification: runs the renderer's device shading code on         */
+/* batches so it can be compared with a CPU oracle.                         */
+/* ---------------------------------------------------------------------- */
+
+enum {
+    /* EvaluateMaterial, core/cuda/Material.h:783-813.
+     * in: 16 floats/query: N[3] V[3] L[3] front_face material_index pad[5]
+     * out: 8 floats: f[3] pdf pad[4] */
+    RT_VERIFY_BSDF_EVAL = 0,
+    /* SampleMaterial, core/cuda/Material.h:815-845, random numbers taken
+     * from the query in order.
+     * in: 16 floats: N[3] V[3] u[6] front_face material_index pad[2]
+     * out: 8 floats: f[3] pdf L[3] used_randoms */
+    RT_VERIFY_BSDF_SAMPLE = 1,
+    /* SampleLight, core/cuda/Light.h:158-168 (+ point light).
+     * in: 16 floats: P[3] u[2] light_index pad[10]
+     * out: 8 floats: Li[3] pdf L[3] distance */
+    RT_VERIFY_LIGHT_SAMPLE = 2,
+    /* EvaluateLight, core/cuda/Light.h:145-156.
+     * in: 16 floats: O[3] D[3] max_distance light_index pad[8]
+     * out: 8 floats: Li[3] pdf distance pad[3] */
+    RT_VERIFY_LIGHT_EVAL = 3,
+    /* SampleMediumDistance, core/cuda/Medium.h:233-244 (homogeneous).
+     * in: 16 floats: max_distance u[2] medium_index pad[12]
+     * out: 8 floats: transmittance[3] trans_pdf distance scattered used pad */
+    RT_VERIFY_MEDIUM_SAMPLE = 4,
+    /* SamplePhase, core/cuda/Medium.h:96-108.
+     * in: 16 floats: V[3] u[4] medium_index pad[8]
+     * out: 8 floats: attenuation[3] pdf L[3] used_randoms */
+    RT_VERIFY_PHASE_SAMPLE = 5,
+    /* EvaluatePhase, core/cuda/Medium.h:83-94.
+     * in: 16 floats: V[3] L[3] medium_index pad[9]
+     * out: 8 floats: attenuation[3] pdf pad[4] */
+    RT_VERIFY_PHASE_EVAL = 6
+};
+
+/* Runs one verification op over n queries on the device.  `materials`,
+ * `lights` and `media` are host arrays indexed by the queries. */
+RT_API rt_status rt_verify_shading(int32_t op, const rt_material* materials, int32_t num_materials,
+                                   const rt_light* lights, int32_t num_lights, const rt_medium* media,
+                                   int32_t num_media, const float* in, int64_t n, float* out);
+/* ComputeKullaConty, core/cuda/Microfacet.h:231-291, as the renderer builds
+ * it: 64*64 floats of E(mu, alpha) and 64 floats of E_avg. */
+RT_API rt_status rt_kulla_conty_lut(float* bsdf_avg, float* albedo_avg);
+/* HdrTexture::CalculateHdrCache, core/src/Scene.cpp:217-313, as the renderer
+ * builds it: w*h*4 floats (sample x, sample y, pdf, 0). */
+RT_API rt_status rt_env_sampling_cache(const float* rgba, int32_t width, int32_t height, float* cache);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RT_CAPI_H */

@@ -1,0 +1,210 @@
+// rt_device.cuh - device-side data layout, vector math and random streams of
+// the B200 path tracer.
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rt_capi.h"
+
+#define RT_HD __host__ __device__ __forceinline__
+#define RT_D __device__ __forceinline__
+
+namespace rtd {
+
+// ------------------------------------------------------------------ vec3
+struct v3 {
+    float x, y, z;
+    RT_HD v3() : x(0.f), y(0.f), z(0.f) {}
+    RT_HD explicit v3(float s) : x(s), y(s), z(s) {}
+    RT_HD v3(float a, float b, float c) : x(a), y(b), z(c) {}
+    RT_HD float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+RT_HD v3 operator+(v3 a, v3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+RT_HD v3 operator-(v3 a, v3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+RT_HD v3 operator*(v3 a, v3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+RT_HD v3 operator/(v3 a, v3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+RT_HD v3 operator*(v3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+RT_HD v3 operator*(float s, v3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+RT_HD v3 operator/(v3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+RT_HD v3 operator+(v3 a, float s) { return v3(a.x + s, a.y + s, a.z + s); }
+RT_HD v3 operator-(float s, v3 a) { return v3(s - a.x, s - a.y, s - a.z); }
+RT_HD v3 operator-(v3 a, float s) { return v3(a.x - s, a.y - s, a.z - s); }
+RT_HD v3 operator-(v3 a) { return v3(-a.x, -a.y, -a.z); }
+RT_HD v3& operator+=(v3& a, v3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+RT_HD v3& operator*=(v3& a, v3 b) { a.x *= b.x; a.y *= b.y; a.z *= b.z; return a; }
+RT_HD v3& operator*=(v3& a, float s) { a.x *= s; a.y *= s; a.z *= s; return a; }
+RT_HD v3& operator/=(v3& a, float s) { a.x /= s; a.y /= s; a.z /= s; return a; }
+RT_HD float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+RT_HD v3 cross(v3 a, v3 b) { return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
+RT_HD float length(v3 v) { return sqrtf(dot(v, v)); }
+// Component-wise division by the length, as gdt's normalize (vec.h:306-310).
+RT_HD v3 normalize(v3 v) { return v / sqrtf(dot(v, v)); }
+RT_HD bool any_nan(v3 v) { return v.x != v.x || v.y != v.y || v.z != v.z; }
+RT_HD float sqr(float x) { return x * x; }
+RT_HD float mixf(float x, float y, float t) { return x * (1.0f - t) + y * t; }
+RT_HD v3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
+RT_HD float4 f4(v3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+RT_HD v3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
+
+// Depth limit of the per-thread traversal stack; a BVH deeper than this is
+// rejected at upload.
+constexpr int kStackSize = 32;
+
+constexpr float kEps = 1e-4f;                                  // core/cuda/Utils.h:10
+constexpr float kPi = 3.14159265358979323846f;                 // Utils.h:11
+constexpr float kTwoPi = 6.28318530717958647692f;              // Utils.h:14
+constexpr float kInvPi = 0.318309886183790671538f;             // Utils.h:13
+
+// ------------------------------------------------------------------ random
+// gdt::LCG<16> of the reference (common/gdt/gdt/random/random.h:54-87).
+RT_HD uint32_t lcg_seed(uint32_t v0, uint32_t v1) {
+    uint32_t s0 = 0;
+#pragma unroll
+    for (int n = 0; n < 16; n++) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return v0;
+}
+// PCG32 (pcg-random.org, pcg32_random_r); the increment is derived from the
+// path index so only the 64-bit state travels with a path.
+RT_HD uint64_t pcg_inc(uint64_t seq) { return (seq << 1u) | 1u; }
+RT_HD uint64_t pcg_seed(uint64_t initstate, uint64_t seq) {
+    uint64_t inc = pcg_inc(seq);
+    uint64_t s = inc;  // 0 * mult + inc
+    s += initstate;
+    s = s * 6364136223846793005ULL + inc;
+    return s;
+}
+RT_HD uint64_t pcg_frame_state(uint64_t seed, int frame) {
+    return seed ^ (uint64_t(uint32_t(frame)) * 0x9E3779B97F4A7C15ULL);
+}
+
+// One random stream: the reference LCG (24-bit floats) or PCG32.
+struct Rng {
+    uint64_t state;
+    uint64_t inc;  // 0 selects the LCG
+    RT_HD float next() {
+        if (inc == 0) {
+            uint32_t s = uint32_t(state) * 1664525u + 1013904223u;
+            state = s;
+            return float(s & 0x00FFFFFFu) / float(0x01000000);
+        }
+        uint64_t old = state;
+        state = old * 6364136223846793005ULL + inc;
+        uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+        uint32_t rot = uint32_t(old >> 59u);
+        uint32_t r = (xs >> rot) | (xs << ((32u - rot) & 31u));
+        return float(r >> 8) * (1.0f / 16777216.0f);
+    }
+};
+
+// ------------------------------------------------------------------ scene
+// Device copy of rt_material (core/include/Scene.h:70-116), 128 bytes.
+struct __align__(16) DevMaterial {
+    int type;
+    float albedo[3];
+    float roughness, anisotropy, int_ior, ext_ior;
+    float eta[3];
+    float metallic;
+    float k[3];
+    float coat_weight;
+    float specular[3];
+    int nonlinear;
+    float coat_roughness_u, coat_roughness_v;
+    float pad0, pad1;
+    int tex[8];
+};
+static_assert(sizeof(DevMaterial) == 128, "DevMaterial layout");
+
+// Device copy of rt_light (Scene.h:143-155), 64 bytes.
+struct __align__(16) DevLight {
+    int type;
+    int double_side;
+    float radius;
+    int medium;
+    float radiance[3];
+    float pad0;
+    float position[3];
+    float pad1;
+    float u[3];
+    float pad2;
+    float v[3];
+    float pad3;
+};
+
+// Device copy of rt_medium (Scene.h:48-55) plus the density grid.
+struct __align__(16) DevMedium {
+    int type, phase;
+    float scale;
+    int majorant_res;
+    float g[3];
+    float pad0;
+    float sigma_s[3];
+    float pad1;
+    float sigma_a[3];
+    float pad2;
+    float bmin[3];
+    float max_density;
+    float bmax[3];
+    float pad3;
+    int res[3];
+    int pad4;
+    const float* density;
+    const float* majorant;
+};
+
+// Per mesh: material index and medium interface (TriangleMeshSBTData,
+// core/include/LaunchParams.h:16-26).
+struct __align__(16) MeshInfo {
+    int material;
+    int in_medium;
+    int out_medium;
+    int pad;
+};
+
+// Compressed 8-wide BVH node (after Ylitie, Karras, Laine, HPG 2017):
+// 80 bytes, read as five 16-byte words.
+struct __align__(16) CwNode {
+    float px, py, pz;
+    uint8_t ex, ey, ez, imask;
+    uint32_t child_base;
+    uint32_t tri_base;
+    uint8_t meta[8];
+    uint8_t qlox[8], qloy[8], qloz[8];
+    uint8_t qhix[8], qhiy[8], qhiz[8];
+};
+static_assert(sizeof(CwNode) == 80, "CwNode layout");
+
+// Everything a kernel needs about one scene, all device pointers.
+struct SceneView {
+    const CwNode* nodes;
+    const float4* tri_v;   // 3 per triangle: v0 (w = original id bits), v1, v2
+    const float4* tri_a;   // 4 per triangle: normals, texcoords, mesh id
+    int num_nodes;
+    int num_tris;
+    const MeshInfo* meshes;
+    const DevMaterial* materials;
+    const DevLight* lights;
+    int num_lights;
+    int num_media;
+    const DevMedium* media;
+    const float4* env;
+    const float4* env_cache;
+    int env_w, env_h;
+    const float* lut;
+    const float* lut_avg;
+};
+
+// Camera vectors of Renderer::SetCamera (core/src/Renderer.cpp:796-813).
+struct CameraView {
+    float pos[3], dir[3], hor[3], ver[3];
+    int medium;
+};
+
+}  // namespace rtd

@@ -1,0 +1,787 @@
+// rt_kernels.cu - wavefront path-tracing kernels for sm_100a.
+//
+// The per-path control flow is the reference integrator
+// (core/cuda/devicePrograms.cu:170-532) cut at its optixTrace calls:
+//   raygen   devicePrograms.cu:220-253  camera ray, filter jitter, RNG state
+//   extend   devicePrograms.cu:258-269  closest hit through the wide BVH
+//   shade    devicePrograms.cu:71-132, 148-159, 270-497  hit attributes,
+//            analytic-light test, media, emission, NEE (shadow rays are queued
+//            with their contribution), BSDF sampling, Russian roulette
+//   shadow   devicePrograms.cu:303-319, 389-405, 437-453  any-hit; an occluded
+//            ray zeroes its pending contribution
+//   resolve  devicePrograms.cu:499-516  NaN handling and per-pixel sums
+//   finalize devicePrograms.cu:518-531 + PostProcessing.cu:26-48
+// Pending NEE contributions are folded into the path radiance at the start of
+// the next shade (or in resolve) in the reference's order: environment, then
+// light.  extend/shade/shadow are persistent kernels: each warp takes 32
+// queue entries at a time with one atomicAdd.
+#include <cstdio>
+
+#include "rt_kernels.cuh"
+#include "rt_shading.cuh"
+#include "rt_traverse.cuh"
+
+namespace rtd {
+
+constexpr int kBlock = 128;
+
+RT_D int find_segment(const Ctx& c, int slot) {
+    int s = c.num_seg - 1;
+    while (s > 0 && slot < __ldg(&c.seg[s].slot_begin)) s--;
+    return s;
+}
+
+RT_D int warp_fetch(int* counter, int lane) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// Appends `flag` lanes of a converged warp to a queue; returns the position.
+RT_D int warp_append(int* counter, bool flag, int lane) {
+    unsigned m = __ballot_sync(0xffffffffu, flag);
+    if (m == 0) return -1;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return flag ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+RT_D void warp_stat(unsigned long long* dst, unsigned v) {
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
+}
+
+// ------------------------------------------------------------------ begin
+__global__ void k_begin(const JobDesc* __restrict__ jd) {
+    const JobParams& j = jd->job;
+    int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= j.npix) return;
+    j.acc_color[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    j.acc_albedo[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    j.acc_normal[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (j.rng == RT_RNG_LCG) j.lcg_state[p] = lcg_seed(uint32_t(p), uint32_t(j.frame));  // devicePrograms.cu:179-180
+}
+
+// ------------------------------------------------------------------ raygen
+__global__ void k_raygen(Ctx c) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    WaveCtl* ctl = c.wb.ctl;
+    if (slot == 0) {
+        ctl->count[0] = c.wave_count;
+        ctl->count[1] = 0;
+        ctl->shadow_count = 0;
+        ctl->fetch_ext = 0;
+        ctl->fetch_shade = 0;
+        ctl->fetch_shadow = 0;
+    }
+    if (slot >= c.wave_count) return;
+    const Segment sg = c.seg[find_segment(c, slot)];
+    const JobDesc* jd = c.jobs + sg.job;
+    const JobParams& j = jd->job;
+    const CameraView& cam = jd->cam;
+    int64_t p = sg.path_begin + (slot - sg.slot_begin);
+    int pix = int(p % j.npix);
+    int ix = pix % j.width, iy = pix / j.width;
+    Rng rng;
+    if (j.rng == RT_RNG_LCG) {
+        rng.inc = 0;
+        rng.state = j.lcg_state[pix];
+    } else {
+        rng.inc = pcg_inc(uint64_t(p));
+        rng.state = pcg_seed(pcg_frame_state(j.seed, j.frame), uint64_t(p));
+    }
+    float u0 = rng.next(), u1 = rng.next();
+    float jx, jy;
+    filter_jitter(j.filter, u0, u1, jx, jy);
+    float sx = (float(ix) + 0.5f + jx) / float(j.width);
+    float sy = (float(iy) + 0.5f + jy) / float(j.height);
+    v3 dir = normalize(ld3(cam.dir) + (sx - 0.5f) * ld3(cam.hor) + (sy - 0.5f) * ld3(cam.ver));
+    const WaveBufs& b = c.wb;
+    b.ray_o[slot] = f4(ld3(cam.pos), 0.0f);
+    b.ray_d[slot] = f4(dir, 0.0f);
+    b.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+    b.rad[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    b.nee0[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    b.nee1[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    b.stale[slot] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    b.rng[slot] = make_uint2(uint32_t(rng.state), uint32_t(rng.state >> 32));
+    b.queue[0][slot] = slot;
+}
+
+// ------------------------------------------------------------------ extend
+template <bool Stats>
+__global__ void __launch_bounds__(kBlock) k_extend(Ctx c) {
+    WaveCtl* ctl = c.wb.ctl;
+    const int cur = c.bounce & 1, nxt = cur ^ 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->count[nxt] = 0;
+        ctl->shadow_count = 0;
+        ctl->fetch_shade = 0;
+    }
+    const int total = ctl->count[cur];
+    const int* __restrict__ q = c.wb.queue[cur];
+    const int lane = threadIdx.x & 31;
+    uint32_t nodes = 0, tris = 0, rays = 0;
+    while (true) {
+        int base = warp_fetch(&ctl->fetch_ext, lane);
+        if (base >= total) break;
+        int i = base + lane;
+        if (i < total) {
+            int slot = q[i];
+            const JobDesc* jd = c.jobs + c.seg[find_segment(c, slot)].job;
+            float4 o = c.wb.ray_o[slot], d = c.wb.ray_d[slot];
+            TravRay r;
+            r.o = xyz(o);
+            r.d = xyz(d);
+            r.tmin = kEps;
+            r.tmax = FLT_MAX;
+            prepare_ray(r);
+            float t = FLT_MAX, b1 = 0.f, b2 = 0.f;
+            int tri = traverse<false, Stats>(jd->sc, r, t, b1, b2, nodes, tris);
+            c.wb.hit[slot] = make_float4(t, b1, b2, __int_as_float(tri));
+            rays++;
+        }
+    }
+    if (Stats) {
+        warp_stat(&ctl->stats[0], rays);
+        warp_stat(&ctl->stats[2], nodes);
+        warp_stat(&ctl->stats[3], tris);
+    }
+}
+
+// lightTrace, devicePrograms.cu:192-211: the nearest analytic light closer
+// than `closest`; `lpdf` ends as the pdf of the last light evaluated.
+RT_D bool light_trace(const SceneView& sc, v3 o, v3 d, float& closest, v3& lrad, float& lpdf, int& medium) {
+    bool hit = false;
+    for (int i = 0; i < sc.num_lights; i++) {
+        LightParams l = load_light(sc.lights + i);
+        float ld = 0.0f;
+        v3 Li = evaluate_light(l, o, d, closest, lpdf, ld);
+        if (lpdf == 0.0f) continue;
+        hit = true;
+        lrad = Li;
+        closest = ld;
+        medium = l.medium;
+    }
+    return hit;
+}
+
+RT_D bool nee_pdf_ok(float p) { return p > 0.0f && p < FLT_MAX; }
+
+// ------------------------------------------------------------------ shade
+template <bool Stats>
+__global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
+    WaveCtl* ctl = c.wb.ctl;
+    const int cur = c.bounce & 1, nxt = cur ^ 1;
+    const int bounce = c.bounce;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->fetch_shadow = 0;
+        ctl->fetch_ext = 0;
+    }
+    const int total = ctl->count[cur];
+    const int* __restrict__ q = c.wb.queue[cur];
+    const WaveBufs& B = c.wb;
+    const int lane = threadIdx.x & 31;
+    uint32_t nan_paths = 0;
+    while (true) {
+        int base = warp_fetch(&ctl->fetch_shade, lane);
+        if (base >= total) break;
+        int i = base + lane;
+        bool cont = false;
+        bool sh0 = false, sh1 = false;
+        int slot = 0;
+        v3 s0o, s0d, s1o, s1d;
+        float s0t = 0.f, s1t = 0.f;
+        if (i < total) {
+            slot = q[i];
+            const JobDesc* jd = c.jobs + c.seg[find_segment(c, slot)].job;
+            const SceneView& sc = jd->sc;
+            const JobParams& jp = jd->job;
+            float4 o4 = B.ray_o[slot], d4 = B.ray_d[slot], th = B.thr[slot], h4 = B.hit[slot];
+            float4 r4 = B.rad[slot];
+            float4 n0 = B.nee0[slot], n1 = B.nee1[slot];
+            uint2 rs = B.rng[slot];
+            Rng rng;
+            rng.state = uint64_t(rs.x) | (uint64_t(rs.y) << 32);
+            if (jp.rng == RT_RNG_LCG) {
+                rng.inc = 0;
+            } else {
+                const Segment& sg = c.seg[find_segment(c, slot)];
+                rng.inc = pcg_inc(uint64_t(sg.path_begin + (slot - sg.slot_begin)));
+            }
+            v3 o = xyz(o4), d = xyz(d4);
+            v3 history = xyz(th);
+            float pre_pdf = th.w;
+            v3 radiance = xyz(r4);
+            radiance += xyz(n0);
+            radiance += xyz(n1);
+            v3 V = -d, L = d;
+            // ---- closest hit / miss programs (devicePrograms.cu:71-132, 148-159)
+            int tri = __float_as_int(h4.w);
+            Surf s;
+            v3 pos = o;
+            float closest;
+            int in_m, out_m;
+            if (tri >= 0) {
+                const float4* tv = sc.tri_v + size_t(tri) * 3;
+                const float4* ta = sc.tri_a + size_t(tri) * 4;
+                float4 p0 = __ldg(tv), p1 = __ldg(tv + 1), p2 = __ldg(tv + 2);
+                float4 a0 = __ldg(ta), a1 = __ldg(ta + 1), a2 = __ldg(ta + 2), a3 = __ldg(ta + 3);
+                float u = h4.y, v = h4.z;
+                float w0 = 1.0f - u - v;
+                v3 Ns = normalize(w0 * xyz(a0) + u * xyz(a1) + v * xyz(a2));
+                v3 P = w0 * xyz(p0) + u * xyz(p1) + v * xyz(p2);
+                int mesh = __float_as_int(a3.w);
+                MeshInfo mi = sc.meshes[mesh];
+                s.front = dot(d, Ns) < 0.0f;
+                s.sn = s.front ? Ns : -Ns;
+                s.mat = sc.materials + mi.material;
+                closest = length(P - o);
+                pos = P;
+                in_m = mi.in_medium;
+                out_m = mi.out_medium;
+                B.stale[slot] = make_float4(s.sn.x, s.sn.y, s.sn.z, __int_as_float(mesh));
+                if (bounce == 0) {
+                    B.aov_a[slot] = make_float4(s.mat->albedo[0], s.mat->albedo[1], s.mat->albedo[2], Ns.x);
+                    B.aov_n[slot] = make_float2(Ns.y, Ns.z);
+                }
+            } else {
+                float4 st = B.stale[slot];
+                int mesh = __float_as_int(st.w);
+                s.sn = xyz(st);
+                s.front = true;
+                s.mat = mesh >= 0 ? sc.materials + sc.meshes[mesh].material : nullptr;
+                closest = FLT_MAX;
+                in_m = out_m = jd->cam.medium;
+                if (bounce == 0) {
+                    B.aov_a[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    B.aov_n[slot] = make_float2(0.f, 0.f);
+                }
+            }
+            // ---- analytic lights (devicePrograms.cu:270-271)
+            v3 light_rad(0.0f);
+            float light_pdf = 0.0f;
+            int lm = 0;
+            bool hit_light = light_trace(sc, o, d, closest, light_rad, light_pdf, lm);
+            if (hit_light) in_m = out_m = lm;
+
+            bool alive = true;
+            bool scattered = false;
+            int medium_index = -1;
+            float mult_trans_pdf = 1.0f;
+            v3 nee_e(0.0f), nee_l(0.0f);
+            // ---- media (devicePrograms.cu:274-338)
+            if (sc.num_media != 0) {
+                medium_index = (hit_light || s.front) ? out_m : in_m;
+                if (medium_index != -1) {
+                    const MedParams med = load_medium(sc.media + medium_index);
+                    float distance = 0.0f, trans_pdf = 0.0f;
+                    v3 tr;
+                    scattered = sample_medium_distance(med, closest, distance, trans_pdf, tr, rng);
+                    history *= (tr / trans_pdf);
+                    mult_trans_pdf *= trans_pdf;
+                    if (scattered) {
+                        pos = o + distance * d;
+                        const int nl = sc.num_lights;
+                        if (nl != 0) {
+                            int idx = min(max(int(float(nl) * rng.next()), 0), nl - 1);
+                            LightParams l = load_light(sc.lights + idx);
+                            float ld = 0.0f, lp = 0.0f;
+                            v3 sd;
+                            float u0 = rng.next(), u1 = rng.next();
+                            v3 lr = sample_light(l, pos, u0, u1, sd, ld, lp);
+                            lp *= (1.0f / float(nl));
+                            float cl = ld - kEps;
+                            v3 tvv;
+                            float tpdf;
+                            int tm;
+                            if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
+                                float tp2, phase_pdf;
+                                v3 tr2 = eval_medium_distance(med, false, cl, tp2);
+                                v3 att = evaluate_phase(med, V, sd, phase_pdf);
+                                float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, phase_pdf * tp2);
+                                nee_l = w * (tr2 / tp2) * lr * att * history / lp;
+                                sh1 = true;
+                                s1o = pos;
+                                s1d = sd;
+                                s1t = ld - kEps;
+                            }
+                        }
+                        float phase_pdf = 0.0f;
+                        v3 att = sample_phase(med, rng, V, L, phase_pdf);
+                        history *= (att / phase_pdf);
+                        pre_pdf = phase_pdf;
+                    }
+                }
+            }
+            if (!scattered) {
+                if (hit_light) {  // devicePrograms.cu:342-351
+                    float w = 1.0f;
+                    if (bounce != 0) {
+                        pre_pdf *= mult_trans_pdf;
+                        w = power_heuristic(pre_pdf, light_pdf);
+                    }
+                    radiance += w * history * light_rad;
+                    alive = false;
+                } else if (closest == FLT_MAX && medium_index == -1) {  // devicePrograms.cu:354-373
+                    if (sc.env_w > 0) {
+                        float u, v;
+                        sphere_to_plane(d, u, v);
+                        float lp = float(sc.env_w * sc.env_h) / (2.0f * sqr(kPi));
+                        float4 e = tex_bilinear(sc.env, sc.env_w, sc.env_h, u, v);
+                        lp *= tex_bilinear(sc.env_cache, sc.env_w, sc.env_h, u, v).z;
+                        float w = 1.0f;
+                        if (bounce != 0) {
+                            pre_pdf *= mult_trans_pdf;
+                            w = power_heuristic(pre_pdf, lp);
+                        }
+                        radiance += w * history * xyz(e);
+                    }
+                    alive = false;
+                } else {
+                    if (sc.env_w > 0) {  // environment NEE, devicePrograms.cu:376-424
+                        float r0 = rng.next(), r1 = rng.next();
+                        float4 cs = tex_bilinear(sc.env_cache, sc.env_w, sc.env_h, r0, r1);
+                        v3 sd = plane_to_sphere(cs.x, cs.y);
+                        float lp = float(sc.env_w * sc.env_h) / (2.0f * sqr(kPi));
+                        lp *= tex_bilinear(sc.env_cache, sc.env_w, sc.env_h, cs.x, cs.y).z;
+                        v3 lr = xyz(tex_bilinear(sc.env, sc.env_w, sc.env_h, cs.x, cs.y));
+                        float cl = FLT_MAX;
+                        v3 tvv;
+                        float tpdf;
+                        int tm;
+                        if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
+                            float bpdf;
+                            v3 f = eval_material(sc, s, V, sd, bpdf);
+                            float ct = fabsf(dot(s.sn, sd));
+                            float w = power_heuristic(lp, bpdf);
+                            v3 thh(1.0f);
+                            if (medium_index != -1) {
+                                const MedParams med = load_medium(sc.media + medium_index);
+                                float tp2;
+                                v3 tr2 = eval_medium_distance(med, false, cl, tp2);
+                                thh = tr2 / tp2;
+                                w = power_heuristic(lp, bpdf * tp2);
+                            }
+                            nee_e = w * thh * lr * f * ct * history / lp;
+                            sh0 = true;
+                            s0o = pos;
+                            s0d = sd;
+                            s0t = FLT_MAX;
+                        }
+                    }
+                    const int nl = sc.num_lights;
+                    if (nl != 0) {  // light NEE, devicePrograms.cu:426-471
+                        int idx = min(max(int(float(nl) * rng.next()), 0), nl - 1);
+                        LightParams l = load_light(sc.lights + idx);
+                        float ld = 0.0f, lp = 0.0f;
+                        v3 sd;
+                        float u0 = rng.next(), u1 = rng.next();
+                        v3 lr = sample_light(l, pos, u0, u1, sd, ld, lp);
+                        lp *= (1.0f / float(nl));
+                        float cl = ld - kEps;
+                        v3 tvv;
+                        float tpdf;
+                        int tm;
+                        if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
+                            float bpdf;
+                            v3 f = eval_material(sc, s, V, sd, bpdf);
+                            float ct = fabsf(dot(s.sn, sd));
+                            float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, bpdf);
+                            v3 thh(1.0f);
+                            if (medium_index != -1) {
+                                const MedParams med = load_medium(sc.media + medium_index);
+                                float tp2;
+                                v3 tr2 = eval_medium_distance(med, false, cl, tp2);
+                                thh = tr2 / tp2;
+                                if (l.type != RT_LIGHT_POINT) w = power_heuristic(lp, bpdf * tp2);
+                            }
+                            nee_l = w * thh * lr * f * ct * history / lp;
+                            sh1 = true;
+                            s1o = pos;
+                            s1d = sd;
+                            s1t = ld - kEps;
+                        }
+                    }
+                    // BSDF sampling, devicePrograms.cu:474-477
+                    float bpdf = 0.0f;
+                    v3 f = sample_material(sc, s, rng, V, L, bpdf);
+                    float ct = fabsf(dot(s.sn, L));
+                    history *= (f * ct / bpdf);
+                    pre_pdf = bpdf;
+                }
+            }
+            if (alive) {
+                // Russian roulette, devicePrograms.cu:480-489
+                if (bounce >= jp.rr_depth) {
+                    float prr = fminf((history.x + history.y + history.z) / 3.0f, 0.95f);
+                    if (rng.next() > prr) {
+                        alive = false;
+                    } else {
+                        history /= prr;
+                    }
+                }
+                if (alive && any_nan(history)) {
+                    alive = false;
+                    nan_paths++;
+                }
+            }
+            cont = alive && (bounce + 1 < jp.max_depth);
+            B.rad[slot] = f4(radiance, 0.0f);
+            B.nee0[slot] = f4(nee_e, 0.0f);
+            B.nee1[slot] = f4(nee_l, 0.0f);
+            B.rng[slot] = make_uint2(uint32_t(rng.state), uint32_t(rng.state >> 32));
+            if (cont) {
+                B.ray_o[slot] = f4(pos, 0.0f);
+                B.ray_d[slot] = f4(L, 0.0f);
+                B.thr[slot] = f4(history, pre_pdf);
+            }
+        }
+        int qp = warp_append(&ctl->count[nxt], cont, lane);
+        if (cont) B.queue[nxt][qp] = slot;
+        int p0 = warp_append(&ctl->shadow_count, sh0, lane);
+        if (sh0) {
+            B.sh_o[p0] = f4(s0o, s0t);
+            B.sh_d[p0] = f4(s0d, __int_as_float(slot * 2 + 0));
+        }
+        int p1 = warp_append(&ctl->shadow_count, sh1, lane);
+        if (sh1) {
+            B.sh_o[p1] = f4(s1o, s1t);
+            B.sh_d[p1] = f4(s1d, __int_as_float(slot * 2 + 1));
+        }
+    }
+    if (Stats) warp_stat(&ctl->stats[6], nan_paths);
+}
+
+// ------------------------------------------------------------------ shadow
+template <bool Stats>
+__global__ void __launch_bounds__(kBlock) k_shadow(Ctx c) {
+    WaveCtl* ctl = c.wb.ctl;
+    const int total = ctl->shadow_count;
+    const int lane = threadIdx.x & 31;
+    uint32_t nodes = 0, tris = 0, rays = 0;
+    while (true) {
+        int base = warp_fetch(&ctl->fetch_shadow, lane);
+        if (base >= total) break;
+        int i = base + lane;
+        if (i < total) {
+            float4 o = c.wb.sh_o[i], d = c.wb.sh_d[i];
+            int code = __float_as_int(d.w);
+            int slot = code >> 1, ch = code & 1;
+            rays++;
+            if (o.w > kEps) {
+                const JobDesc* jd = c.jobs + c.seg[find_segment(c, slot)].job;
+                TravRay r;
+                r.o = xyz(o);
+                r.d = xyz(d);
+                r.tmin = kEps;
+                r.tmax = o.w;
+                prepare_ray(r);
+                float t, b1, b2;
+                int tri = traverse<true, Stats>(jd->sc, r, t, b1, b2, nodes, tris);
+                if (tri >= 0) (ch ? c.wb.nee1 : c.wb.nee0)[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    }
+    if (Stats) {
+        warp_stat(&ctl->stats[1], rays);
+        warp_stat(&ctl->stats[4], nodes);
+        warp_stat(&ctl->stats[5], tris);
+    }
+}
+
+// ------------------------------------------------------------------ resolve
+// Folds the last pending NEE and adds each path to its pixel's sum in sample
+// order.  With RT_RNG_LCG a wave holds at most one sample per pixel and a NaN
+// sample ends the pixel's launch (devicePrograms.cu:499-501); with PCG32 the
+// first sample of a pixel in the wave sums all of them and a NaN sample is
+// dropped alone.
+__global__ void k_resolve(Ctx c) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= c.wave_count) return;
+    const Segment& sg = c.seg[find_segment(c, slot)];
+    const JobDesc* jd = c.jobs + sg.job;
+    const JobParams& j = jd->job;
+    const WaveBufs& B = c.wb;
+    int64_t p = sg.path_begin + (slot - sg.slot_begin);
+    int pix = int(p % j.npix);
+    if (j.rng == RT_RNG_LCG) {
+        uint2 rs = B.rng[slot];
+        j.lcg_state[pix] = rs.x;
+        float4 acc = j.acc_color[pix];
+        if (acc.w != 0.0f) return;
+        v3 r = xyz(B.rad[slot]);
+        r += xyz(B.nee0[slot]);
+        r += xyz(B.nee1[slot]);
+        if (any_nan(r)) {
+            j.acc_color[pix].w = 1.0f;
+            atomicAdd(&B.ctl->stats[6], 1ull);
+            return;
+        }
+        float4 a = B.aov_a[slot];
+        float2 n = B.aov_n[slot];
+        j.acc_color[pix] = make_float4(acc.x + r.x, acc.y + r.y, acc.z + r.z, 0.0f);
+        float4 aa = j.acc_albedo[pix], an = j.acc_normal[pix];
+        j.acc_albedo[pix] = make_float4(aa.x + a.x, aa.y + a.y, aa.z + a.z, 0.f);
+        j.acc_normal[pix] = make_float4(an.x + a.w, an.y + n.x, an.z + n.y, 0.f);
+        return;
+    }
+    // PCG32: is this the first sample of `pix` inside the segment?
+    int64_t first = sg.path_begin;
+    if (p - j.npix >= first) return;
+    float4 acc = j.acc_color[pix], aa = j.acc_albedo[pix], an = j.acc_normal[pix];
+    int64_t end = sg.path_begin + sg.count;
+    unsigned nans = 0;
+    for (int64_t q = p; q < end; q += j.npix) {
+        int sl = sg.slot_begin + int(q - sg.path_begin);
+        v3 r = xyz(B.rad[sl]);
+        r += xyz(B.nee0[sl]);
+        r += xyz(B.nee1[sl]);
+        if (any_nan(r)) {
+            nans++;
+            continue;
+        }
+        float4 a = B.aov_a[sl];
+        float2 n = B.aov_n[sl];
+        acc.x += r.x;
+        acc.y += r.y;
+        acc.z += r.z;
+        aa.x += a.x;
+        aa.y += a.y;
+        aa.z += a.z;
+        an.x += a.w;
+        an.y += n.x;
+        an.z += n.y;
+    }
+    j.acc_color[pix] = acc;
+    j.acc_albedo[pix] = aa;
+    j.acc_normal[pix] = an;
+    if (nans) atomicAdd(&B.ctl->stats[6], (unsigned long long)nans);
+}
+
+// ------------------------------------------------------------------ finalize
+RT_D uint32_t tonemap_pixel(float4 c, int mode, float exposure) {
+    float x = c.x * exposure, y = c.y * exposure, z = c.z * exposure;
+    if (mode == RT_TONEMAP_REINHARD) {  // PostProcessing.cu:18-48
+        float lum = 0.299f * x + 0.587f * y + 0.114f * z;
+        float f = 1.0f / (1.0f + lum / 1.5f);
+        float v0 = powf(x * f, 1.0f / 2.2f), v1 = powf(y * f, 1.0f / 2.2f), v2 = powf(z * f, 1.0f / 2.2f);
+        v0 = fminf(1.0f, fmaxf(0.0f, v0));
+        v1 = fminf(1.0f, fmaxf(0.0f, v1));
+        v2 = fminf(1.0f, fmaxf(0.0f, v2));
+        return uint32_t(v0 * 255.9f) | (uint32_t(v1 * 255.9f) << 8) | (uint32_t(v2 * 255.9f) << 16) | (255u << 24);
+    }
+    float v[3] = {x, y, z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float t = v[k];
+        if (mode == RT_TONEMAP_ACES_SRGB) {  // ACES filmic fit (Narkowicz 2015), then sRGB encoding
+            t = (t * (2.51f * t + 0.03f)) / (t * (2.43f * t + 0.59f) + 0.14f);
+            t = fminf(1.0f, fmaxf(0.0f, t));
+            t = t <= 0.0031308f ? 12.92f * t : 1.055f * powf(t, 1.0f / 2.4f) - 0.055f;
+        }
+        v[k] = fminf(1.0f, fmaxf(0.0f, t));
+    }
+    return uint32_t(v[0] * 255.0f + 0.5f) | (uint32_t(v[1] * 255.0f + 0.5f) << 8) |
+           (uint32_t(v[2] * 255.0f + 0.5f) << 16) | (255u << 24);
+}
+
+__global__ void k_finalize(const JobDesc* __restrict__ jd) {
+    const JobParams& j = jd->job;
+    int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= j.npix) return;
+    float spp = float(j.spp);
+    float4 a = j.acc_color[p];
+    float4 rgba = make_float4(a.x / spp, a.y / spp, a.z / spp, 1.0f);
+    if (j.frame > 0) {  // devicePrograms.cu:524-528
+        float fr = float(j.frame);
+        float4 old = j.color[p];
+        rgba.x = (rgba.x + fr * old.x) / (fr + 1.0f);
+        rgba.y = (rgba.y + fr * old.y) / (fr + 1.0f);
+        rgba.z = (rgba.z + fr * old.z) / (fr + 1.0f);
+        rgba.w = (rgba.w + fr * old.w) / (fr + 1.0f);
+    }
+    j.color[p] = rgba;
+    float4 al = j.acc_albedo[p], nm = j.acc_normal[p];
+    j.albedo[p] = make_float4(al.x / spp, al.y / spp, al.z / spp, 1.0f);
+    j.normal[p] = make_float4(nm.x / spp, nm.y / spp, nm.z / spp, 1.0f);
+    j.rgba8[p] = tonemap_pixel(rgba, j.tonemap, j.exposure);
+}
+
+// ------------------------------------------------------------------ ray queries
+template <bool AnyHit>
+__global__ void __launch_bounds__(kBlock) k_trace(SceneView sc, const float* __restrict__ rays, int64_t n,
+                                                  float* __restrict__ hits) {
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* rr = reinterpret_cast<const float4*>(rays) + i * 2;
+    float4 a = rr[0], b = rr[1];
+    TravRay r;
+    r.o = xyz(a);
+    r.d = xyz(b);
+    r.tmin = a.w;
+    r.tmax = b.w;
+    prepare_ray(r);
+    float t = FLT_MAX, b1 = 0.f, b2 = 0.f;
+    uint32_t nv = 0, nt = 0;
+    int tri = traverse<AnyHit, false>(sc, r, t, b1, b2, nv, nt);
+    float4 out;
+    if (tri < 0) {
+        out = make_float4(FLT_MAX, 0.f, 0.f, __int_as_float(-1));
+    } else if (AnyHit) {
+        out = make_float4(t, b1, b2, __int_as_float(1));
+    } else {
+        int orig = __float_as_int(__ldg(sc.tri_v + size_t(tri) * 3).w);
+        out = make_float4(t, b1, b2, __int_as_float(orig));
+    }
+    reinterpret_cast<float4*>(hits)[i] = out;
+}
+
+// ------------------------------------------------------------------ verification
+struct ListRng {
+    const float* u;
+    int n, used;
+    RT_D float next() {
+        used++;
+        return (used - 1) < n ? u[used - 1] : 0.5f;
+    }
+};
+
+__global__ void k_verify(int op, SceneView sc, const DevLight* lights, const DevMedium* media,
+                         const float* __restrict__ in, int64_t n, float* __restrict__ out) {
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* x = in + i * 16;
+    float* y = out + i * 8;
+    float r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    ListRng rng;
+    rng.used = 0;
+    if (op == RT_VERIFY_BSDF_EVAL || op == RT_VERIFY_BSDF_SAMPLE) {
+        bool sample = op == RT_VERIFY_BSDF_SAMPLE;
+        Surf s;
+        s.sn = ld3(x);
+        s.front = (sample ? x[12] : x[9]) != 0.0f;
+        s.mat = sc.materials + int(sample ? x[13] : x[10]);
+        v3 V = ld3(x + 3);
+        float pdf = 0.0f;
+        v3 f;
+        if (!sample) {
+            f = eval_material(sc, s, V, ld3(x + 6), pdf);
+        } else {
+            rng.u = x + 6;
+            rng.n = 6;
+            v3 L(0.0f);
+            f = sample_material(sc, s, rng, V, L, pdf);
+            r[4] = L.x;
+            r[5] = L.y;
+            r[6] = L.z;
+            r[7] = float(rng.used);
+        }
+        r[0] = f.x;
+        r[1] = f.y;
+        r[2] = f.z;
+        r[3] = pdf;
+    } else if (op == RT_VERIFY_LIGHT_SAMPLE) {
+        LightParams l = load_light(lights + int(x[5]));
+        v3 L(0.0f);
+        float dist = 0.0f, pdf = 0.0f;
+        v3 Li = sample_light(l, ld3(x), x[3], x[4], L, dist, pdf);
+        r[0] = Li.x; r[1] = Li.y; r[2] = Li.z; r[3] = pdf;
+        r[4] = L.x; r[5] = L.y; r[6] = L.z; r[7] = dist;
+    } else if (op == RT_VERIFY_LIGHT_EVAL) {
+        LightParams l = load_light(lights + int(x[7]));
+        float pdf = 0.0f, ld = 0.0f;
+        v3 Li = evaluate_light(l, ld3(x), ld3(x + 3), x[6], pdf, ld);
+        r[0] = Li.x; r[1] = Li.y; r[2] = Li.z; r[3] = pdf; r[4] = ld;
+    } else if (op == RT_VERIFY_MEDIUM_SAMPLE) {
+        MedParams m = load_medium(media + int(x[3]));
+        rng.u = x + 1;
+        rng.n = 2;
+        float dist = 0.0f, tp = 0.0f;
+        v3 tr;
+        bool sc_ = sample_medium_distance(m, x[0], dist, tp, tr, rng);
+        r[0] = tr.x; r[1] = tr.y; r[2] = tr.z; r[3] = tp; r[4] = dist; r[5] = sc_ ? 1.0f : 0.0f;
+        r[6] = float(rng.used);
+    } else if (op == RT_VERIFY_PHASE_SAMPLE) {
+        MedParams m = load_medium(media + int(x[7]));
+        rng.u = x + 3;
+        rng.n = 4;
+        v3 L(0.0f);
+        float pdf = 0.0f;
+        v3 a = sample_phase(m, rng, ld3(x), L, pdf);
+        r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = pdf;
+        r[4] = L.x; r[5] = L.y; r[6] = L.z; r[7] = float(rng.used);
+    } else if (op == RT_VERIFY_PHASE_EVAL) {
+        MedParams m = load_medium(media + int(x[6]));
+        float pdf = 0.0f;
+        v3 a = evaluate_phase(m, ld3(x), ld3(x + 3), pdf);
+        r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = pdf;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) y[k] = r[k];
+}
+
+}  // namespace rtd
+
+// ====================================================================== host
+namespace rth {
+using namespace rtd;
+
+void query_shape(LaunchShape& s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev);
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend<false>, kBlock, 0);
+    s.blocks_extend = s.sms * (b > 0 ? b : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false>, kBlock, 0);
+    s.blocks_shade = s.sms * (b > 0 ? b : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shadow<false>, kBlock, 0);
+    s.blocks_shadow = s.sms * (b > 0 ? b : 1);
+}
+
+static unsigned grid_for(int64_t n, int block) { return unsigned((n + block - 1) / block); }
+
+void launch_begin(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
+    k_begin<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
+}
+void launch_raygen(const Ctx& c, cudaStream_t st) { k_raygen<<<grid_for(c.wave_count, 256), 256, 0, st>>>(c); }
+void launch_extend(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
+    if (stats)
+        k_extend<true><<<s.blocks_extend, kBlock, 0, st>>>(c);
+    else
+        k_extend<false><<<s.blocks_extend, kBlock, 0, st>>>(c);
+}
+void launch_shade(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
+    if (stats)
+        k_shade<true><<<s.blocks_shade, kBlock, 0, st>>>(c);
+    else
+        k_shade<false><<<s.blocks_shade, kBlock, 0, st>>>(c);
+}
+void launch_shadow(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
+    if (stats)
+        k_shadow<true><<<s.blocks_shadow, kBlock, 0, st>>>(c);
+    else
+        k_shadow<false><<<s.blocks_shadow, kBlock, 0, st>>>(c);
+}
+void launch_resolve(const Ctx& c, cudaStream_t st) { k_resolve<<<grid_for(c.wave_count, 256), 256, 0, st>>>(c); }
+void launch_finalize(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
+    k_finalize<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
+}
+void launch_trace(const SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st) {
+    if (n <= 0) return;
+    if (any_hit)
+        k_trace<true><<<grid_for(n, kBlock), kBlock, 0, st>>>(sc, rays, n, hits);
+    else
+        k_trace<false><<<grid_for(n, kBlock), kBlock, 0, st>>>(sc, rays, n, hits);
+}
+void launch_verify(int op, const SceneView& sc, const DevLight* lights, const DevMedium* media, const float* in,
+                   int64_t n, float* out, cudaStream_t st) {
+    if (n <= 0) return;
+    k_verify<<<grid_for(n, 128), 128, 0, st>>>(op, sc, lights, media, in, n, out);
+}
+}  // namespace rth

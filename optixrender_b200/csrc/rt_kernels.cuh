@@ -1,0 +1,108 @@
+// rt_kernels.cuh - host-visible declarations of the wavefront pipeline.
+//
+// One Renderer::Render() (core/src/Renderer.cpp:635-793) becomes, per wave of
+// paths: raygen -> [extend -> shade -> shadow] x max_depth -> resolve, and
+// finally finalize (running mean, AOVs, tonemap).  The megakernel loop of
+// core/cuda/devicePrograms.cu:213-516 is split at every optixTrace call.
+#pragma once
+
+#include "rt_device.cuh"
+
+namespace rtd {
+
+constexpr int kMaxSegments = 16;
+
+// Per-render parameters and per-pixel buffers of one job.
+struct JobParams {
+    int width, height, spp, max_depth;
+    int filter, rng, rr_depth, frame;
+    uint64_t seed;
+    int64_t npix;
+    int tonemap;
+    float exposure;
+    float4* acc_color;   // per pixel: running sum of the launch (w: aborted flag)
+    float4* acc_albedo;
+    float4* acc_normal;
+    uint32_t* lcg_state; // per pixel (RT_RNG_LCG)
+    float4* color;       // running mean across Render() calls
+    float4* albedo;
+    float4* normal;
+    uint32_t* rgba8;
+};
+
+struct JobDesc {
+    SceneView sc;
+    CameraView cam;
+    JobParams job;
+};
+
+// A contiguous run of one job's paths inside a wave.
+struct Segment {
+    int job;
+    int slot_begin;
+    int count;
+    int pad;
+    int64_t path_begin;
+};
+
+struct WaveCtl {
+    int count[2];
+    int shadow_count;
+    int fetch_ext;
+    int fetch_shade;
+    int fetch_shadow;
+    int error;
+    int pad;
+    unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris, nan, spare
+};
+
+// Structure-of-arrays path state, one entry per slot of a wave.
+struct WaveBufs {
+    float4* ray_o;   // origin
+    float4* ray_d;   // direction
+    float4* hit;     // t, b1, b2, triangle (bits; -1 = miss)
+    float4* thr;     // throughput (history), pre_pdf
+    float4* rad;     // radiance
+    float4* nee0;    // pending environment NEE contribution
+    float4* nee1;    // pending light NEE contribution
+    float4* stale;   // shading normal and mesh of the last hit
+    float4* aov_a;   // albedo, normal.x
+    float2* aov_n;   // normal.y, normal.z
+    uint2* rng;      // random state
+    int* queue[2];   // active slots
+    float4* sh_o;    // shadow ray origin, tmax
+    float4* sh_d;    // shadow ray direction, slot * 2 + channel (bits)
+    WaveCtl* ctl;
+    int capacity;
+};
+
+struct Ctx {
+    const JobDesc* jobs;
+    WaveBufs wb;
+    const Segment* seg;  // device array of num_seg entries
+    int num_seg;
+    int wave_count;
+    int bounce;
+    int max_depth;  // largest max_depth of the jobs in the wave
+};
+
+}  // namespace rtd
+
+// Host launchers (rt_kernels.cu).
+namespace rth {
+struct LaunchShape {
+    int sms;
+    int blocks_extend, blocks_shade, blocks_shadow;
+};
+void query_shape(LaunchShape& s);
+void launch_begin(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);
+void launch_raygen(const rtd::Ctx& c, cudaStream_t st);
+void launch_extend(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
+void launch_shade(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
+void launch_shadow(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
+void launch_resolve(const rtd::Ctx& c, cudaStream_t st);
+void launch_finalize(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);
+void launch_trace(const rtd::SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st);
+void launch_verify(int op, const rtd::SceneView& sc, const rtd::DevLight* lights, const rtd::DevMedium* media,
+                   const float* in, int64_t n, float* out, cudaStream_t st);
+}  // namespace rth

@@ -1,0 +1,604 @@
+// rt_renderer.cpp - the Renderer handle: scene upload, per-pixel and per-wave
+// buffers, and the host loop that issues the wavefront kernels for one
+// Renderer::Render() (core/src/Renderer.cpp:635-793).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "rt_bvh.h"
+#include "rt_internal.h"
+
+using namespace rtd;
+using namespace rti;
+
+namespace rti {
+
+DeviceScene::~DeviceScene() {
+    for (DevBuf* g : grids) delete g;
+}
+
+#define RT_CUDA(call, what)                        \
+    do {                                           \
+        cudaError_t e_ = (call);                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
+    const int64_t nt = int64_t(s.tri_mesh.size());
+    rth::BuiltBvh bvh;
+    std::string err;
+    if (!rth::build_cwbvh(s.tv.data(), nt, bvh, err)) return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
+    if (bvh.depth > kStackSize)
+        return fail(RT_ERR_UNSUPPORTED, "BVH too deep for the traversal stack (" + std::to_string(bvh.depth) + " levels)");
+    ds.bvh_depth = bvh.depth;
+    std::vector<float4> tv(size_t(nt) * 3), ta(size_t(nt) * 4);
+    for (int64_t t = 0; t < nt; t++) {
+        int o = bvh.order[size_t(t)];
+        const float* p = &s.tv[size_t(o) * 9];
+        const float* n = &s.tn[size_t(o) * 9];
+        const float* uv = &s.tuv[size_t(o) * 6];
+        float4 id;
+        std::memcpy(&id.x, &o, 4);
+        tv[size_t(t) * 3 + 0] = make_float4(p[0], p[1], p[2], id.x);
+        tv[size_t(t) * 3 + 1] = make_float4(p[3], p[4], p[5], 0.0f);
+        tv[size_t(t) * 3 + 2] = make_float4(p[6], p[7], p[8], 0.0f);
+        int mesh = s.tri_mesh[size_t(o)];
+        float mf;
+        std::memcpy(&mf, &mesh, 4);
+        ta[size_t(t) * 4 + 0] = make_float4(n[0], n[1], n[2], uv[0]);
+        ta[size_t(t) * 4 + 1] = make_float4(n[3], n[4], n[5], uv[1]);
+        ta[size_t(t) * 4 + 2] = make_float4(n[6], n[7], n[8], uv[2]);
+        ta[size_t(t) * 4 + 3] = make_float4(uv[3], uv[4], uv[5], mf);
+    }
+    std::vector<MeshInfo> meshes(s.mesh_mat.size());
+    std::vector<DevMaterial> mats(s.mesh_mat.size());
+    for (size_t i = 0; i < meshes.size(); i++) {
+        meshes[i].material = int(i);
+        meshes[i].in_medium = s.mesh_in[i];
+        meshes[i].out_medium = s.mesh_out[i];
+        meshes[i].pad = 0;
+        mats[i] = to_dev(s.mesh_mat[i]);
+    }
+    std::vector<DevLight> lights;
+    for (auto& l : s.lights) lights.push_back(to_dev(l));
+    std::vector<DevMedium> media;
+    for (size_t i = 0; i < s.media.size(); i++) media.push_back(to_dev(s.media[i]));
+    RT_CUDA(ds.nodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(CwNode), st), "upload BVH nodes");
+    RT_CUDA(ds.tri_v.upload(tv.data(), tv.size() * sizeof(float4), st), "upload triangles");
+    RT_CUDA(ds.tri_a.upload(ta.data(), ta.size() * sizeof(float4), st), "upload triangle attributes");
+    RT_CUDA(ds.meshes.upload(meshes.data(), meshes.size() * sizeof(MeshInfo), st), "upload meshes");
+    RT_CUDA(ds.materials.upload(mats.data(), mats.size() * sizeof(DevMaterial), st), "upload materials");
+    RT_CUDA(ds.lights.upload(lights.data(), lights.size() * sizeof(DevLight), st), "upload lights");
+    const float* avg = nullptr;
+    const float* lut = kc_tables(&avg);
+    RT_CUDA(ds.lut.upload(lut, 64 * 64 * sizeof(float), st), "upload LUT");
+    RT_CUDA(ds.lut_avg.upload(avg, 64 * sizeof(float), st), "upload LUT");
+    if (s.env_w > 0) {
+        std::vector<float> cache(s.env.size());
+        rth::env_sampling_cache(s.env.data(), s.env_w, s.env_h, cache.data());
+        RT_CUDA(ds.env.upload(s.env.data(), s.env.size() * sizeof(float), st), "upload environment");
+        RT_CUDA(ds.env_cache.upload(cache.data(), cache.size() * sizeof(float), st), "upload environment cache");
+    }
+    for (size_t i = 0; i < media.size(); i++) {
+        if (s.media[i].type != RT_MEDIUM_GRID) continue;
+        const std::vector<float>& d = s.media_density[i];
+        DevBuf* g = new DevBuf();
+        ds.grids.push_back(g);
+        RT_CUDA(g->upload(d.data(), d.size() * sizeof(float), st), "upload density grid");
+        media[i].density = g->as<float>();
+        float mx = 0.0f;
+        for (float v : d) mx = std::max(mx, v);
+        media[i].max_density = mx;
+    }
+    RT_CUDA(ds.media.upload(media.data(), media.size() * sizeof(DevMedium), st), "upload media");
+    SceneView& v = ds.view;
+    v.nodes = ds.nodes.as<CwNode>();
+    v.tri_v = ds.tri_v.as<float4>();
+    v.tri_a = ds.tri_a.as<float4>();
+    v.num_nodes = int(bvh.nodes.size());
+    v.num_tris = int(nt);
+    v.meshes = ds.meshes.as<MeshInfo>();
+    v.materials = ds.materials.as<DevMaterial>();
+    v.lights = ds.lights.as<DevLight>();
+    v.num_lights = int(lights.size());
+    v.media = ds.media.as<DevMedium>();
+    v.num_media = int(media.size());
+    v.env = ds.env.as<float4>();
+    v.env_cache = ds.env_cache.as<float4>();
+    v.env_w = s.env_w;
+    v.env_h = s.env_h;
+    v.lut = ds.lut.as<float>();
+    v.lut_avg = ds.lut_avg.as<float>();
+    ds.bytes = ds.nodes.bytes + ds.tri_v.bytes + ds.tri_a.bytes + ds.env.bytes + ds.env_cache.bytes;
+    return RT_OK;
+}
+
+}  // namespace rti
+
+struct KernelTimer {
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<std::pair<int, size_t>> marks;  // (class, event index of the start)
+    cudaEvent_t next() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    void reset() {
+        used = 0;
+        marks.clear();
+    }
+    ~KernelTimer() {
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+};
+
+struct rt_renderer {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DeviceScene ds;
+    rt_options opt{};
+    rt_camera cam{};
+    int frame = 0;
+    int pw = 0, ph = 0;
+    DevBuf acc_color, acc_albedo, acc_normal, lcg_state, color, albedo, normal, rgba8;
+    int capacity = 0;
+    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, ctl, segs, job;
+    rth::LaunchShape shape{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    KernelTimer timer;
+    bool rendered = false;
+    int launches = 0;
+    int waves = 0;
+    int extend_launches = 0;
+    int64_t paths = 0;
+};
+
+namespace {
+
+rt_status ensure_pixels(rt_renderer* r, int w, int h) {
+    if (r->pw == w && r->ph == h) return RT_OK;
+    size_t n = size_t(w) * h;
+    DevBuf* f4s[] = {&r->acc_color, &r->acc_albedo, &r->acc_normal, &r->color, &r->albedo, &r->normal};
+    for (DevBuf* b : f4s) {
+        b->release();
+        RT_CUDA(b->alloc(n * sizeof(float4)), "allocate frame buffers");
+        RT_CUDA(cudaMemsetAsync(b->ptr, 0, n * sizeof(float4), r->stream), "clear frame buffers");
+    }
+    r->lcg_state.release();
+    r->rgba8.release();
+    RT_CUDA(r->lcg_state.alloc(n * 4), "allocate frame buffers");
+    RT_CUDA(r->rgba8.alloc(n * 4), "allocate frame buffers");
+    RT_CUDA(cudaMemsetAsync(r->rgba8.ptr, 0, n * 4, r->stream), "clear frame buffers");
+    r->pw = w;
+    r->ph = h;
+    return RT_OK;
+}
+
+rt_status ensure_waves(rt_renderer* r, int cap) {
+    if (cap <= r->capacity) return RT_OK;
+    size_t n = size_t(cap);
+    DevBuf* f4s[] = {&r->ray_o, &r->ray_d, &r->hit, &r->thr, &r->rad, &r->nee0, &r->nee1, &r->stale, &r->aov_a};
+    for (DevBuf* b : f4s) RT_CUDA(b->alloc(n * sizeof(float4)), "allocate path state");
+    RT_CUDA(r->aov_n.alloc(n * sizeof(float2)), "allocate path state");
+    RT_CUDA(r->rng.alloc(n * sizeof(uint2)), "allocate path state");
+    RT_CUDA(r->q0.alloc(n * sizeof(int)), "allocate queues");
+    RT_CUDA(r->q1.alloc(n * sizeof(int)), "allocate queues");
+    RT_CUDA(r->sh_o.alloc(2 * n * sizeof(float4)), "allocate shadow queue");
+    RT_CUDA(r->sh_d.alloc(2 * n * sizeof(float4)), "allocate shadow queue");
+    r->capacity = cap;
+    return RT_OK;
+}
+
+int auto_capacity(const rt_options& o, int64_t npix, int64_t total) {
+    int64_t cap = o.wave_paths > 0 ? int64_t(o.wave_paths) : std::max<int64_t>(npix, int64_t(1) << 21);
+    cap = std::min<int64_t>(cap, int64_t(1) << 24);
+    if (o.rng == RT_RNG_LCG) cap = std::min<int64_t>(cap, npix);
+    cap = std::min<int64_t>(cap, total);
+    return int(std::max<int64_t>(cap, 1));
+}
+
+rt_status check_options(const rt_options* o) {
+    if (o->spp < 1 || o->max_depth < 1) return fail(RT_ERR_INVALID_ARG, "spp and max_depth must be >= 1");
+    if (o->width < 0 || o->height < 0) return fail(RT_ERR_INVALID_ARG, "negative frame size");
+    if (int64_t(o->width) * o->height > (int64_t(1) << 28)) return fail(RT_ERR_INVALID_ARG, "frame too large");
+    if (o->rng != RT_RNG_LCG && o->rng != RT_RNG_PCG32) return fail(RT_ERR_INVALID_ARG, "unknown rng");
+    if (o->filter < RT_FILTER_BOX || o->filter > RT_FILTER_GAUSSIAN) return fail(RT_ERR_INVALID_ARG, "unknown filter");
+    return RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_renderer** out) {
+    if (!s || !out) return fail(RT_ERR_INVALID_ARG, "rt_renderer_create: NULL argument");
+    rt_options o;
+    rt_options_default(&o);
+    if (opts) o = *opts;
+    rt_status st = check_options(&o);
+    if (st) return st;
+    rt_renderer* r = new (std::nothrow) rt_renderer();
+    if (!r) return fail(RT_ERR_OUT_OF_MEMORY, "rt_renderer_create: out of host memory");
+    cudaError_t e = cudaGetDevice(&r->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete r;
+        return cuda_fail(e, "rt_renderer_create");
+    }
+    r->own_stream = true;
+    r->opt = o;
+    rt_camera_default(&r->cam);
+    st = upload_scene(*s, r->ds, r->stream);
+    if (st == RT_OK) {
+        e = cudaEventCreate(&r->ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&r->ev1);
+        if (e == cudaSuccess) e = cudaMalloc(&r->ctl.ptr, sizeof(WaveCtl));
+        if (e == cudaSuccess) {
+            r->ctl.bytes = sizeof(WaveCtl);
+            e = cudaMemset(r->ctl.ptr, 0, sizeof(WaveCtl));
+        }
+        if (e == cudaSuccess) e = r->job.alloc(sizeof(JobDesc));
+        if (e != cudaSuccess) st = cuda_fail(e, "rt_renderer_create");
+    }
+    if (st == RT_OK) rth::query_shape(r->shape);
+    if (st == RT_OK && o.width > 0 && o.height > 0) st = ensure_pixels(r, o.width, o.height);
+    if (st) {
+        rt_renderer_destroy(r);
+        return st;
+    }
+    *out = r;
+    return RT_OK;
+}
+
+rt_status rt_renderer_destroy(rt_renderer* r) {
+    if (!r) return RT_OK;
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    if (r->ev0) cudaEventDestroy(r->ev0);
+    if (r->ev1) cudaEventDestroy(r->ev1);
+    if (r->own_stream && r->stream) cudaStreamDestroy(r->stream);
+    delete r;
+    return RT_OK;
+}
+
+rt_status rt_renderer_set_options(rt_renderer* r, const rt_options* o) {
+    if (!r || !o) return fail(RT_ERR_INVALID_ARG, "rt_renderer_set_options: NULL argument");
+    rt_status st = check_options(o);
+    if (st) return st;
+    int w = r->opt.width, h = r->opt.height;
+    r->opt = *o;
+    if (o->width != w || o->height != h) return rt_renderer_resize(r, o->width, o->height);
+    return RT_OK;
+}
+
+rt_status rt_renderer_get_options(const rt_renderer* r, rt_options* o) {
+    if (!r || !o) return fail(RT_ERR_INVALID_ARG, "rt_renderer_get_options: NULL argument");
+    *o = r->opt;
+    return RT_OK;
+}
+
+rt_status rt_renderer_resize(rt_renderer* r, int32_t w, int32_t h) {
+    if (!r || w < 0 || h < 0) return fail(RT_ERR_INVALID_ARG, "rt_renderer_resize: bad argument");
+    r->opt.width = w;
+    r->opt.height = h;
+    if (w > 0 && h > 0) {
+        rt_status st = ensure_pixels(r, w, h);
+        if (st) return st;
+    }
+    r->frame = 0;  // SetCamera(lastSetCamera), Renderer.cpp:874
+    return RT_OK;
+}
+
+rt_status rt_renderer_set_camera(rt_renderer* r, const rt_camera* c) {
+    if (!r || !c) return fail(RT_ERR_INVALID_ARG, "rt_renderer_set_camera: NULL argument");
+    r->cam = *c;
+    r->frame = 0;  // Renderer.cpp:799
+    return RT_OK;
+}
+
+rt_status rt_renderer_set_stream(rt_renderer* r, void* s) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_set_stream: NULL renderer");
+    cudaStreamSynchronize(r->stream);
+    if (r->own_stream) cudaStreamDestroy(r->stream);
+    if (s) {
+        r->stream = static_cast<cudaStream_t>(s);
+        r->own_stream = false;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e, "rt_renderer_set_stream");
+        r->own_stream = true;
+    }
+    return RT_OK;
+}
+
+rt_status rt_renderer_render(rt_renderer* r) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_render: NULL renderer");
+    const rt_options& o = r->opt;
+    if (o.width <= 0 || o.height <= 0) return RT_OK;  // Renderer.cpp:638-640
+    rt_status st = ensure_pixels(r, o.width, o.height);
+    if (st) return st;
+    const int64_t npix = int64_t(o.width) * o.height;
+    const int64_t total = npix * o.spp;
+    const int cap = auto_capacity(o, npix, total);
+    st = ensure_waves(r, cap);
+    if (st) return st;
+    if (!o.progressive) r->frame = 0;  // Renderer.cpp:642-644
+    JobDesc hj;
+    std::memset(&hj, 0, sizeof(hj));
+    hj.sc = r->ds.view;
+    hj.cam = camera_view(r->cam, o.width, o.height);
+    JobParams& j = hj.job;
+    j.width = o.width;
+    j.height = o.height;
+    j.spp = o.spp;
+    j.max_depth = o.max_depth;
+    j.filter = o.filter;
+    j.rng = o.rng;
+    j.rr_depth = o.rr_depth;
+    j.frame = r->frame;
+    j.seed = o.seed;
+    j.npix = npix;
+    j.tonemap = o.tonemap;
+    j.exposure = o.exposure;
+    j.acc_color = r->acc_color.as<float4>();
+    j.acc_albedo = r->acc_albedo.as<float4>();
+    j.acc_normal = r->acc_normal.as<float4>();
+    j.lcg_state = r->lcg_state.as<uint32_t>();
+    j.color = r->color.as<float4>();
+    j.albedo = r->albedo.as<float4>();
+    j.normal = r->normal.as<float4>();
+    j.rgba8 = r->rgba8.as<uint32_t>();
+    r->frame++;
+    cudaStream_t s = r->stream;
+    RT_CUDA(cudaMemcpyAsync(r->job.ptr, &hj, sizeof(hj), cudaMemcpyHostToDevice, s), "upload launch parameters");
+    const int64_t nwaves = (total + cap - 1) / cap;
+    std::vector<Segment> segs(static_cast<size_t>(nwaves));
+    for (int64_t w = 0; w < nwaves; w++) {
+        Segment& g = segs[size_t(w)];
+        g.job = 0;
+        g.slot_begin = 0;
+        g.path_begin = w * cap;
+        g.count = int(std::min<int64_t>(cap, total - w * cap));
+        g.pad = 0;
+    }
+    RT_CUDA(r->segs.alloc(segs.size() * sizeof(Segment)), "allocate wave table");
+    RT_CUDA(cudaMemcpyAsync(r->segs.ptr, segs.data(), segs.size() * sizeof(Segment), cudaMemcpyHostToDevice, s),
+            "upload wave table");
+    RT_CUDA(cudaMemsetAsync(r->ctl.ptr, 0, sizeof(WaveCtl), s), "clear counters");
+    const bool stats = o.collect_stats != 0;
+    r->timer.reset();
+    RT_CUDA(cudaEventRecord(r->ev0, s), "record event");
+    const JobDesc* dj = r->job.as<JobDesc>();
+    rth::launch_begin(hj, dj, s);
+    int launches = 1;
+    int ext = 0;
+    Ctx c;
+    std::memset(&c, 0, sizeof(c));
+    c.jobs = dj;
+    WaveBufs& b = c.wb;
+    b.ray_o = r->ray_o.as<float4>();
+    b.ray_d = r->ray_d.as<float4>();
+    b.hit = r->hit.as<float4>();
+    b.thr = r->thr.as<float4>();
+    b.rad = r->rad.as<float4>();
+    b.nee0 = r->nee0.as<float4>();
+    b.nee1 = r->nee1.as<float4>();
+    b.stale = r->stale.as<float4>();
+    b.aov_a = r->aov_a.as<float4>();
+    b.aov_n = r->aov_n.as<float2>();
+    b.rng = r->rng.as<uint2>();
+    b.queue[0] = r->q0.as<int>();
+    b.queue[1] = r->q1.as<int>();
+    b.sh_o = r->sh_o.as<float4>();
+    b.sh_d = r->sh_d.as<float4>();
+    b.ctl = r->ctl.as<WaveCtl>();
+    b.capacity = cap;
+    c.num_seg = 1;
+    c.max_depth = o.max_depth;
+    for (int64_t w = 0; w < nwaves; w++) {
+        c.seg = r->segs.as<Segment>() + w;
+        c.wave_count = segs[size_t(w)].count;
+        c.bounce = 0;
+        rth::launch_raygen(c, s);
+        launches++;
+        for (int bnc = 0; bnc < o.max_depth; bnc++) {
+            c.bounce = bnc;
+            cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+            if (stats) {
+                e0 = r->timer.next();
+                cudaEventRecord(e0, s);
+            }
+            rth::launch_extend(c, r->shape, stats, s);
+            if (stats) {
+                e1 = r->timer.next();
+                cudaEventRecord(e1, s);
+            }
+            rth::launch_shade(c, r->shape, stats, s);
+            if (stats) {
+                e2 = r->timer.next();
+                cudaEventRecord(e2, s);
+            }
+            rth::launch_shadow(c, r->shape, stats, s);
+            if (stats) {
+                e3 = r->timer.next();
+                cudaEventRecord(e3, s);
+                size_t i0 = r->timer.used - 4;
+                r->timer.marks.push_back({0, i0});
+                r->timer.marks.push_back({1, i0 + 1});
+                r->timer.marks.push_back({2, i0 + 2});
+            }
+            launches += 3;
+            ext++;
+        }
+        rth::launch_resolve(c, s);
+        launches++;
+    }
+    rth::launch_finalize(hj, dj, s);
+    launches++;
+    RT_CUDA(cudaEventRecord(r->ev1, s), "record event");
+    RT_CUDA(cudaGetLastError(), "launch");
+    r->rendered = true;
+    r->launches = launches;
+    r->waves = int(nwaves);
+    r->extend_launches = ext;
+    r->paths = total;
+    return RT_OK;
+}
+
+rt_status rt_renderer_synchronize(rt_renderer* r) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_synchronize: NULL renderer");
+    RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_synchronize");
+    return RT_OK;
+}
+
+static rt_status download(rt_renderer* r, const DevBuf& b, void* dst, size_t bytes) {
+    if (!r || !dst) return fail(RT_ERR_INVALID_ARG, "download: NULL argument");
+    if (!b.ptr) return fail(RT_ERR_STATE, "download: nothing rendered at this size");
+    RT_CUDA(cudaMemcpyAsync(dst, b.ptr, bytes, cudaMemcpyDeviceToHost, r->stream), "download");
+    RT_CUDA(cudaStreamSynchronize(r->stream), "download");
+    return RT_OK;
+}
+
+rt_status rt_renderer_download_rgba8(rt_renderer* r, uint32_t* px) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "NULL renderer");
+    return download(r, r->rgba8, px, size_t(r->pw) * r->ph * 4);
+}
+
+rt_status rt_renderer_download_linear(rt_renderer* r, float* rgba) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "NULL renderer");
+    return download(r, r->color, rgba, size_t(r->pw) * r->ph * 16);
+}
+
+rt_status rt_renderer_download_aov(rt_renderer* r, int32_t kind, float* rgba) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "NULL renderer");
+    size_t n = size_t(r->pw) * r->ph * 16;
+    if (kind == RT_AOV_COLOR) return download(r, r->color, rgba, n);
+    if (kind == RT_AOV_ALBEDO) return download(r, r->albedo, rgba, n);
+    if (kind == RT_AOV_NORMAL) return download(r, r->normal, rgba, n);
+    return fail(RT_ERR_INVALID_ARG, "rt_renderer_download_aov: unknown kind");
+}
+
+rt_status rt_renderer_device_buffers(rt_renderer* r, void** color, void** rgba8) {
+    if (!r) return fail(RT_ERR_INVALID_ARG, "NULL renderer");
+    if (color) *color = r->color.ptr;
+    if (rgba8) *rgba8 = r->rgba8.ptr;
+    return RT_OK;
+}
+
+rt_status rt_renderer_frame_index(const rt_renderer* r, int32_t* f) {
+    if (!r || !f) return fail(RT_ERR_INVALID_ARG, "NULL argument");
+    *f = r->frame;
+    return RT_OK;
+}
+
+rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
+    rt_renderer* r = const_cast<rt_renderer*>(rc);
+    if (!r || !out) return fail(RT_ERR_INVALID_ARG, "rt_renderer_get_stats: NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    if (!r->rendered) return RT_OK;
+    RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_get_stats");
+    WaveCtl ctl;
+    RT_CUDA(cudaMemcpy(&ctl, r->ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost), "read counters");
+    out->paths = r->paths;
+    out->extend_rays = int64_t(ctl.stats[0]);
+    out->shadow_rays = int64_t(ctl.stats[1]);
+    out->extend_nodes = int64_t(ctl.stats[2]);
+    out->extend_tris = int64_t(ctl.stats[3]);
+    out->nodes_visited = int64_t(ctl.stats[2] + ctl.stats[4]);
+    out->tris_tested = int64_t(ctl.stats[3] + ctl.stats[5]);
+    out->nan_samples = int64_t(ctl.stats[6]);
+    out->waves = r->waves;
+    out->launches = r->launches;
+    out->extend_launches = r->extend_launches;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    out->ms_total = ms;
+    float cls[3] = {0.f, 0.f, 0.f};
+    for (auto& m : r->timer.marks) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, r->timer.pool[m.second], r->timer.pool[m.second + 1]);
+        cls[m.first] += t;
+    }
+    out->ms_extend = cls[0];
+    out->ms_shade = cls[1];
+    out->ms_shadow = cls[2];
+    out->ms_other = r->timer.marks.empty() ? 0.0f : ms - cls[0] - cls[1] - cls[2];
+    return RT_OK;
+}
+
+rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
+                            int32_t device_ptrs) {
+    if (!r || (n > 0 && (!rays || !hits)) || n < 0) return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace: bad argument");
+    if (n == 0) return RT_OK;
+    if (device_ptrs) {
+        rth::launch_trace(r->ds.view, any_hit != 0, rays, n, hits, r->stream);
+        RT_CUDA(cudaGetLastError(), "rt_renderer_trace");
+        RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace");
+        return RT_OK;
+    }
+    DevBuf dr, dh;
+    RT_CUDA(dr.alloc(size_t(n) * 32), "rt_renderer_trace: allocate");
+    RT_CUDA(dh.alloc(size_t(n) * 16), "rt_renderer_trace: allocate");
+    RT_CUDA(cudaMemcpyAsync(dr.ptr, rays, size_t(n) * 32, cudaMemcpyHostToDevice, r->stream), "rt_renderer_trace");
+    rth::launch_trace(r->ds.view, any_hit != 0, dr.as<float>(), n, dh.as<float>(), r->stream);
+    RT_CUDA(cudaGetLastError(), "rt_renderer_trace");
+    RT_CUDA(cudaMemcpyAsync(hits, dh.ptr, size_t(n) * 16, cudaMemcpyDeviceToHost, r->stream), "rt_renderer_trace");
+    RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace");
+    return RT_OK;
+}
+
+rt_status rt_verify_shading(int32_t op, const rt_material* materials, int32_t nmat, const rt_light* lights, int32_t nl,
+                            const rt_medium* media, int32_t nm, const float* in, int64_t n, float* out) {
+    if (!in || !out || n < 0) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: bad argument");
+    if (op < RT_VERIFY_BSDF_EVAL || op > RT_VERIFY_PHASE_EVAL) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: unknown op");
+    for (int64_t i = 0; i < n; i++) {
+        const float* x = in + i * 16;
+        int idx = op == RT_VERIFY_BSDF_EVAL ? int(x[10])
+                  : op == RT_VERIFY_BSDF_SAMPLE ? int(x[13])
+                  : op == RT_VERIFY_LIGHT_SAMPLE ? int(x[5])
+                  : op == RT_VERIFY_LIGHT_EVAL ? int(x[7])
+                  : op == RT_VERIFY_MEDIUM_SAMPLE ? int(x[3])
+                  : op == RT_VERIFY_PHASE_SAMPLE ? int(x[7])
+                                                  : int(x[6]);
+        int lim = (op <= RT_VERIFY_BSDF_SAMPLE) ? nmat : (op <= RT_VERIFY_LIGHT_EVAL ? nl : nm);
+        if (idx < 0 || idx >= lim) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: index out of range");
+    }
+    if (n == 0) return RT_OK;
+    cudaStream_t s = nullptr;
+    DevBuf dm, dl, dmed, dlut, davg, din, dout;
+    std::vector<DevMaterial> m;
+    for (int i = 0; i < nmat; i++) m.push_back(to_dev(materials[i]));
+    std::vector<DevLight> l;
+    for (int i = 0; i < nl; i++) l.push_back(to_dev(lights[i]));
+    std::vector<DevMedium> md;
+    for (int i = 0; i < nm; i++) md.push_back(to_dev(media[i]));
+    const float* avg = nullptr;
+    const float* lut = kc_tables(&avg);
+    RT_CUDA(dm.upload(m.data(), m.size() * sizeof(DevMaterial), s), "rt_verify_shading");
+    RT_CUDA(dl.upload(l.data(), l.size() * sizeof(DevLight), s), "rt_verify_shading");
+    RT_CUDA(dmed.upload(md.data(), md.size() * sizeof(DevMedium), s), "rt_verify_shading");
+    RT_CUDA(dlut.upload(lut, 64 * 64 * 4, s), "rt_verify_shading");
+    RT_CUDA(davg.upload(avg, 64 * 4, s), "rt_verify_shading");
+    RT_CUDA(din.upload(in, size_t(n) * 64, s), "rt_verify_shading");
+    RT_CUDA(dout.alloc(size_t(n) * 32), "rt_verify_shading");
+    SceneView v;
+    std::memset(&v, 0, sizeof(v));
+    v.materials = dm.as<DevMaterial>();
+    v.lut = dlut.as<float>();
+    v.lut_avg = davg.as<float>();
+    rth::launch_verify(op, v, dl.as<DevLight>(), dmed.as<DevMedium>(), din.as<float>(), n, dout.as<float>(), s);
+    RT_CUDA(cudaGetLastError(), "rt_verify_shading");
+    RT_CUDA(cudaMemcpy(out, dout.ptr, size_t(n) * 32, cudaMemcpyDeviceToHost), "rt_verify_shading");
+    return RT_OK;
+}
+
+}  // extern "C"

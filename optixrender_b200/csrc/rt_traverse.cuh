@@ -1,0 +1,192 @@
+// rt_traverse.cuh - ray traversal of the compressed 8-wide BVH.
+//
+// Replaces optixTrace (core/cuda/devicePrograms.cu:258-269 closest hit,
+// :303-319 terminate-on-first-hit shadow rays).  Traversal follows Ylitie,
+// Karras and Laine, "Efficient Incoherent Ray Traversal on GPUs Through
+// Compressed Wide BVHs" (HPG 2017): a node is read as five 16-byte loads, its
+// eight quantised child boxes are tested at once, and the hits become a
+// 32-bit group mask (bits 24..31 internal children in near-to-far order,
+// bits 0..23 triangles) kept on a short per-thread stack.  Triangles use the
+// watertight test of Woop, Benthin and Wald (JCGT 2013).
+#pragma once
+
+#include "rt_device.cuh"
+
+namespace rtd {
+
+struct TravRay {
+    v3 o, d;
+    float tmin, tmax;
+    v3 idir;        // 1 / d with tiny components clamped
+    uint32_t oct;   // bit a set when d[a] < 0: slot index of the nearest child
+    int kx, ky, kz; // watertight shear axes
+    float Sx, Sy, Sz;
+};
+
+RT_D void prepare_ray(TravRay& r) {
+    const float tiny = 1e-20f;
+    float dx = fabsf(r.d.x) > tiny ? r.d.x : copysignf(tiny, r.d.x);
+    float dy = fabsf(r.d.y) > tiny ? r.d.y : copysignf(tiny, r.d.y);
+    float dz = fabsf(r.d.z) > tiny ? r.d.z : copysignf(tiny, r.d.z);
+    r.idir = v3(1.0f / dx, 1.0f / dy, 1.0f / dz);
+    r.oct = (r.d.x < 0.0f ? 1u : 0u) | (r.d.y < 0.0f ? 2u : 0u) | (r.d.z < 0.0f ? 4u : 0u);
+    float ax = fabsf(r.d.x), ay = fabsf(r.d.y), az = fabsf(r.d.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    float dkz = r.d[kz];
+    if (dkz < 0.0f) {
+        int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.Sx = __fdiv_rn(r.d[kx], dkz);
+    r.Sy = __fdiv_rn(r.d[ky], dkz);
+    r.Sz = __fdiv_rn(1.0f, dkz);
+}
+
+RT_D float comp(v3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Watertight ray/triangle test.  Products are rounded individually (no FMA
+// contraction) so the edge functions match a plain FP32 evaluation.
+RT_D bool intersect_tri(const TravRay& r, float4 a, float4 b, float4 c, float tmax, float& t, float& b1, float& b2) {
+    v3 A = v3(a.x, a.y, a.z) - r.o, B = v3(b.x, b.y, b.z) - r.o, C = v3(c.x, c.y, c.z) - r.o;
+    float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+    float Ax = __fsub_rn(comp(A, r.kx), __fmul_rn(r.Sx, Akz)), Ay = __fsub_rn(comp(A, r.ky), __fmul_rn(r.Sy, Akz));
+    float Bx = __fsub_rn(comp(B, r.kx), __fmul_rn(r.Sx, Bkz)), By = __fsub_rn(comp(B, r.ky), __fmul_rn(r.Sy, Bkz));
+    float Cx = __fsub_rn(comp(C, r.kx), __fmul_rn(r.Sx, Ckz)), Cy = __fsub_rn(comp(C, r.ky), __fmul_rn(r.Sy, Ckz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.0f) return false;
+    float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
+    float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+    float inv = __fdiv_rn(1.0f, det);
+    float tt = __fmul_rn(T, inv);
+    if (!(tt > r.tmin && tt < tmax)) return false;
+    t = tt;
+    b1 = __fmul_rn(V, inv);
+    b2 = __fmul_rn(W, inv);
+    return true;
+}
+
+RT_D float u8f(uint32_t w, int byte) { return float((w >> (8 * byte)) & 0xFFu); }
+
+// Tests the eight children of `node`; returns the hit mask of internal
+// children (bits 24..31, near-to-far) with the node's imask in bits 0..7,
+// and the triangle hit mask (bits 0..23) in `tri_bits`.
+RT_D uint32_t intersect_children(const CwNode* nodes, uint32_t idx, const TravRay& r, float tmax, uint32_t& child_base,
+                                 uint32_t& tri_base, uint32_t& tri_bits) {
+    const float4* q = reinterpret_cast<const float4*>(nodes + idx);
+    float4 n0 = __ldg(q + 0), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3), n4 = __ldg(q + 4);
+    uint32_t e = __float_as_uint(n0.w);
+    uint32_t ex = e & 0xFFu, ey = (e >> 8) & 0xFFu, ez = (e >> 16) & 0xFFu, imask = e >> 24;
+    child_base = __float_as_uint(n1.x);
+    tri_base = __float_as_uint(n1.y);
+    uint32_t meta_lo = __float_as_uint(n1.z), meta_hi = __float_as_uint(n1.w);
+    // per axis: t = q * (2^e * idir) + (p - o) * idir
+    float sx = __uint_as_float(ex << 23) * r.idir.x, sy = __uint_as_float(ey << 23) * r.idir.y,
+          sz = __uint_as_float(ez << 23) * r.idir.z;
+    float ox = (n0.x - r.o.x) * r.idir.x, oy = (n0.y - r.o.y) * r.idir.y, oz = (n0.z - r.o.z) * r.idir.z;
+    // lo / hi planes per axis packed as bytes: qlox n2.xy, qloy n2.zw, qloz n3.xy, qhix n3.zw, qhiy n4.xy, qhiz n4.zw
+    uint32_t lox[2] = {__float_as_uint(n2.x), __float_as_uint(n2.y)};
+    uint32_t loy[2] = {__float_as_uint(n2.z), __float_as_uint(n2.w)};
+    uint32_t loz[2] = {__float_as_uint(n3.x), __float_as_uint(n3.y)};
+    uint32_t hix[2] = {__float_as_uint(n3.z), __float_as_uint(n3.w)};
+    uint32_t hiy[2] = {__float_as_uint(n4.x), __float_as_uint(n4.y)};
+    uint32_t hiz[2] = {__float_as_uint(n4.z), __float_as_uint(n4.w)};
+    // near plane = lo when the direction is positive
+    const bool nx = r.idir.x >= 0.0f, ny = r.idir.y >= 0.0f, nz = r.idir.z >= 0.0f;
+    uint32_t node_bits = 0, tbits = 0;
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        uint32_t mlo = half == 0 ? meta_lo : meta_hi;
+        uint32_t xn = nx ? lox[half] : hix[half], xf = nx ? hix[half] : lox[half];
+        uint32_t yn = ny ? loy[half] : hiy[half], yf = ny ? hiy[half] : loy[half];
+        uint32_t zn = nz ? loz[half] : hiz[half], zf = nz ? hiz[half] : loz[half];
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            uint32_t meta = (mlo >> (8 * b)) & 0xFFu;
+            float tx0 = fmaf(u8f(xn, b), sx, ox), tx1 = fmaf(u8f(xf, b), sx, ox);
+            float ty0 = fmaf(u8f(yn, b), sy, oy), ty1 = fmaf(u8f(yf, b), sy, oy);
+            float tz0 = fmaf(u8f(zn, b), sz, oz), tz1 = fmaf(u8f(zf, b), sz, oz);
+            float tn = fmaxf(fmaxf(tx0, ty0), fmaxf(tz0, r.tmin));
+            float tf = fminf(fminf(tx1, ty1), fminf(tz1, tmax));
+            bool hit = meta != 0u && tn * 0.9999992f <= tf * 1.0000008f;
+            if (hit) {
+                const int slot = half * 4 + b;
+                if ((imask >> slot) & 1u) {
+                    node_bits |= 1u << (24 + (uint32_t(slot) ^ r.oct));
+                } else {
+                    tbits |= (meta >> 5) << (meta & 31u);
+                }
+            }
+        }
+    }
+    tri_bits = tbits;
+    return node_bits | imask;
+}
+
+// Returns the index of the closest hit triangle (or -1) in [tmin, tmax).
+// `nodes_visited` / `tris_tested` are only updated when Stats is true.
+template <bool AnyHit, bool Stats>
+RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, float& b2, uint32_t& nodes_visited,
+                  uint32_t& tris_tested) {
+    int hit_tri = -1;
+    float tmax = r.tmax;
+    if (sc.num_nodes <= 0) return -1;
+    uint2 stack[kStackSize];
+    int sp = 0;
+    // node group: x = base node index, y = internal hit bits (24..31) | parent imask (0..7)
+    uint2 g = make_uint2(0u, 1u << (24 + r.oct));
+    uint2 tg = make_uint2(0u, 0u);
+    while (true) {
+        if (g.y & 0xFF000000u) {
+            uint32_t bits = g.y >> 24;
+            uint32_t bit = __ffs(bits) - 1u;
+            g.y &= ~(1u << (24 + bit));
+            uint32_t slot = bit ^ r.oct;
+            uint32_t idx = g.x + __popc((g.y & 0xFFu) & ((1u << slot) - 1u));
+            if (g.y & 0xFF000000u) {
+                if (sp < kStackSize) stack[sp++] = g;
+            }
+            uint32_t cb, tb, tbits;
+            uint32_t nb = intersect_children(sc.nodes, idx, r, tmax, cb, tb, tbits);
+            if (Stats) nodes_visited++;
+            g = make_uint2(cb, nb);
+            tg = make_uint2(tb, tbits);
+        } else {
+            tg = g;
+            g = make_uint2(0u, 0u);
+        }
+        while (tg.y & 0x00FFFFFFu) {
+            uint32_t b = __ffs(tg.y) - 1u;
+            tg.y &= ~(1u << b);
+            uint32_t ti = tg.x + b;
+            const float4* tv = sc.tri_v + size_t(ti) * 3;
+            float4 a = __ldg(tv), bb = __ldg(tv + 1), c = __ldg(tv + 2);
+            if (Stats) tris_tested++;
+            float t, u, v;
+            if (intersect_tri(r, a, bb, c, tmax, t, u, v)) {
+                hit_tri = int(ti);
+                tmax = t;
+                t_hit = t;
+                b1 = u;
+                b2 = v;
+                if (AnyHit) return hit_tri;
+            }
+        }
+        if (!(g.y & 0xFF000000u)) {
+            if (sp == 0) break;
+            g = stack[--sp];
+        }
+    }
+    return hit_tri;
+}
+
+}  // namespace rtd

@@ -1,0 +1,280 @@
+"""Seeded procedural scenes of the benchmark configurations.
+
+Each generator returns a ``SceneSpec``: meshes, lights, media, an optional
+equirectangular environment, a camera and render settings.  ``build_scene``
+turns a spec into a ``Scene`` of the CUDA library; the CPU oracle builds its
+own scene from the same arrays.  All randomness comes from
+``numpy.random.default_rng(seed)``.
+
+* ``cornell``  - 256x256, 16 spp, depth 8: five wall quads and two boxes
+  (34 triangles), Lambert walls, a GGX conductor box, a ceiling quad light.
+* ``spheres``  - 1920x1080, 64 spp, depth 16: a level-8 icosphere
+  (1,310,720 triangles) displaced by fBm, 64 spheres of 20,000 triangles each
+  (conductor / dielectric / plastic), and a 2048x1024 sky with a 0.5-degree
+  sun of peak radiance 5e3.
+* ``media``    - 1280x720, 256 spp, depth 32: a 128^3 fBm density grid inside
+  an IOR-1.33 dielectric sphere, a homogeneous fog slab, an area light and the
+  same sky.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import (FILTER_GAUSSIAN, LIGHT_QUAD, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_DIFFUSE, MAT_PLASTIC,
+               MEDIUM_GRID, MEDIUM_HOMOGENEOUS, PHASE_HG, PHASE_ISOTROPIC, RNG_PCG32, Renderer, Scene, camera,
+               light, material, medium, options)
+
+
+@dataclass
+class MeshSpec:
+    positions: np.ndarray            # (n, 3) float32
+    indices: Optional[np.ndarray]    # (m, 3) int32 or None (de-indexed)
+    material: dict
+    out_medium: int = -1
+    in_medium: int = -1
+
+    def triangles(self) -> np.ndarray:
+        """(m, 9) float32 de-indexed vertex positions."""
+        if self.indices is None:
+            return np.ascontiguousarray(self.positions.reshape(-1, 9), dtype=np.float32)
+        return np.ascontiguousarray(self.positions[self.indices].reshape(-1, 9), dtype=np.float32)
+
+
+@dataclass
+class SceneSpec:
+    name: str
+    meshes: list
+    lights: list = field(default_factory=list)      # dicts for light()
+    media: list = field(default_factory=list)       # dicts for medium()
+    env: Optional[np.ndarray] = None                # (h, w, 4) float32
+    camera: dict = field(default_factory=dict)
+    settings: dict = field(default_factory=dict)    # options() keywords
+
+    @property
+    def num_triangles(self):
+        return int(sum(m.triangles().shape[0] if m.indices is None else m.indices.shape[0] for m in self.meshes))
+
+
+# ------------------------------------------------------------------ geometry
+def box(lo, hi):
+    """Axis-aligned box: 8 vertices, 12 outward-wound triangles."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], np.float32)
+    f = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                  [3, 6, 2], [3, 7, 6], [0, 4, 7], [0, 7, 3], [1, 2, 6], [1, 6, 5]], np.int32)
+    return v, f
+
+
+def quad(p, u, v):
+    p, u, v = (np.asarray(a, np.float32) for a in (p, u, v))
+    verts = np.stack([p, p + u, p + u + v, p + v])
+    return verts, np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+
+
+def icosphere(level):
+    """Unit icosphere of 20 * 4^level triangles (shared vertices)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (len(v) + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a = uniq // (len(v) + 1)
+        b = uniq % (len(v) + 1)
+        mid = v[a] + v[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = len(v)
+        v = np.concatenate([v, mid])
+        nf = len(f)
+        m01 = base + inv[:nf]
+        m12 = base + inv[nf:2 * nf]
+        m20 = base + inv[2 * nf:]
+        f = np.concatenate([np.stack([f[:, 0], m01, m20], 1), np.stack([f[:, 1], m12, m01], 1),
+                            np.stack([f[:, 2], m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    return v, f
+
+
+def uv_sphere(n_lat=101, n_lon=100):
+    """UV sphere with 2 * n_lon * (n_lat - 1) triangles (20,000 by default)."""
+    th = np.linspace(0.0, np.pi, n_lat)
+    ph = np.linspace(0.0, 2 * np.pi, n_lon, endpoint=False)
+    st, ct = np.sin(th)[:, None], np.cos(th)[:, None]
+    v = np.stack([st * np.cos(ph)[None], ct * np.ones_like(ph)[None], st * np.sin(ph)[None]], -1).reshape(-1, 3)
+    idx = np.arange(n_lat * n_lon).reshape(n_lat, n_lon)
+    a = idx[:-1]
+    b = np.roll(idx[:-1], -1, axis=1)
+    c = idx[1:]
+    d = np.roll(idx[1:], -1, axis=1)
+    f = np.concatenate([np.stack([a, c, b], -1).reshape(-1, 3), np.stack([b, c, d], -1).reshape(-1, 3)])
+    return v, f
+
+
+def _hash3(ix, iy, iz, seed):
+    h = (ix.astype(np.uint64) * np.uint64(0x8da6b343) ^ iy.astype(np.uint64) * np.uint64(0xd8163841) ^
+         iz.astype(np.uint64) * np.uint64(0xcb1ab31f) ^ np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15))
+    h ^= h >> np.uint64(33)
+    h *= np.uint64(0xff51afd7ed558ccd)
+    h ^= h >> np.uint64(33)
+    h *= np.uint64(0xc4ceb9fe1a85ec53)
+    h ^= h >> np.uint64(33)
+    return (h >> np.uint64(40)).astype(np.float64) / float(1 << 24)
+
+
+def value_noise(p, seed):
+    """Trilinear value noise in [-1, 1] with smoothstep weights."""
+    p = np.asarray(p, np.float64)
+    i = np.floor(p).astype(np.int64)
+    f = p - i
+    w = f * f * (3 - 2 * f)
+    out = np.zeros(p.shape[:-1])
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                h = _hash3(i[..., 0] + dx, i[..., 1] + dy, i[..., 2] + dz, seed)
+                wx = w[..., 0] if dx else 1 - w[..., 0]
+                wy = w[..., 1] if dy else 1 - w[..., 1]
+                wz = w[..., 2] if dz else 1 - w[..., 2]
+                out += wx * wy * wz * (2 * h - 1)
+    return out
+
+
+def fbm(p, seed, octaves=5, freq=2.0, lacunarity=2.0, gain=0.5):
+    amp, total, norm = 1.0, 0.0, 0.0
+    p = np.asarray(p, np.float64) * freq
+    for o in range(octaves):
+        total = total + amp * value_noise(p, seed + 7919 * o)
+        norm += amp
+        amp *= gain
+        p = p * lacunarity
+    return total / norm
+
+
+def sky(width=2048, height=1024, sun_elev_deg=35.0, sun_azim_deg=40.0, sun_peak=5e3, sun_diam_deg=0.5):
+    """Equirectangular RGBA sky: a gradient and a sun lobe.  Row r holds
+    v = (r + 0.5) / height and column c holds u = (c + 0.5) / width in the
+    reference's mapping (core/cuda/Sampling.h:12-33)."""
+    u = (np.arange(width) + 0.5) / width
+    v = (np.arange(height) + 0.5) / height
+    phi = 2 * np.pi * (u - 0.5)
+    th = np.pi * (v - 0.5)
+    d = np.stack([np.cos(th)[:, None] * np.cos(phi)[None], np.sin(th)[:, None] * np.ones_like(phi)[None],
+                  np.cos(th)[:, None] * np.sin(phi)[None]], -1)
+    y = d[..., 1]
+    t = np.clip(y, 0, 1)[..., None]
+    horizon = np.array([0.85, 0.9, 1.0])
+    zenith = np.array([0.15, 0.3, 0.75])
+    ground = np.array([0.25, 0.22, 0.2])
+    col = np.where((y >= 0)[..., None], horizon * (1 - t) + zenith * t, ground * (0.5 + 0.5 * (1 + y[..., None])))
+    se, sa = np.radians(sun_elev_deg), np.radians(sun_azim_deg)
+    s = np.array([np.cos(se) * np.cos(sa), np.sin(se), np.cos(se) * np.sin(sa)])
+    ang = np.degrees(np.arccos(np.clip(d @ s, -1, 1)))
+    r = sun_diam_deg / 2
+    lobe = np.clip(1 - (ang / r) ** 2, 0, 1)
+    col = col + sun_peak * lobe[..., None] * np.array([1.0, 0.95, 0.85])
+    img = np.concatenate([col, np.ones(col.shape[:2] + (1,))], -1).astype(np.float32)
+    return img
+
+
+# ------------------------------------------------------------------ scenes
+def cornell(width=256, height=256, spp=16, seed=1):
+    white = dict(type=MAT_DIFFUSE, albedo=(0.73, 0.73, 0.73), roughness=0.0)
+    red = dict(type=MAT_DIFFUSE, albedo=(0.65, 0.05, 0.05), roughness=0.0)
+    green = dict(type=MAT_DIFFUSE, albedo=(0.12, 0.45, 0.15), roughness=0.0)
+    copper = dict(type=MAT_CONDUCTOR, albedo=(1.0, 1.0, 1.0), roughness=0.2)
+    meshes = []
+    for p, u, v, m in [((0, 0, 0), (1, 0, 0), (0, 0, 1), white),     # floor
+                       ((0, 1, 0), (0, 0, 1), (1, 0, 0), white),     # ceiling
+                       ((0, 0, 1), (1, 0, 0), (0, 1, 0), white),     # back
+                       ((0, 0, 0), (0, 0, 1), (0, 1, 0), red),       # left
+                       ((1, 0, 0), (0, 1, 0), (0, 0, 1), green)]:    # right
+        verts, f = quad(p, u, v)
+        meshes.append(MeshSpec(verts, f, m))
+    v, f = box((0.13, 0.0, 0.2), (0.43, 0.3, 0.5))
+    meshes.append(MeshSpec(v, f, white))
+    v, f = box((0.55, 0.0, 0.45), (0.85, 0.6, 0.75))
+    meshes.append(MeshSpec(v, f, copper))
+    # Quad light just below the ceiling, emitting downwards (-cross(u, v)).
+    lights = [dict(type=LIGHT_QUAD, position=(0.375, 0.999, 0.375), u=(0.0, 0.0, 0.25), v=(0.25, 0.0, 0.0),
+                   radiance=(17.0, 12.0, 4.0), double_side=0)]
+    cam = dict(from_=(0.5, 0.5, -1.6), at=(0.5, 0.5, 0.5), up=(0, 1, 0))
+    settings = dict(width=width, height=height, spp=spp, max_depth=8, rr_depth=3, rng=RNG_PCG32, seed=seed,
+                    filter=FILTER_GAUSSIAN)
+    return SceneSpec("cornell", meshes, lights, [], None, cam, settings)
+
+
+def spheres(width=1920, height=1080, spp=64, seed=1, ico_level=8, sphere_tris=True, env_size=(2048, 1024)):
+    rng = np.random.default_rng(seed)
+    v, f = icosphere(ico_level)
+    disp = fbm(v * 1.5, seed, octaves=6)
+    v = v * (1.0 + 0.05 * disp)[:, None]
+    base = dict(type=MAT_PLASTIC, albedo=(0.55, 0.55, 0.6), roughness=0.3, int_ior=1.5, ext_ior=1.0)
+    meshes = [MeshSpec(v.astype(np.float32), f.astype(np.int32), base)]
+    sv, sf = uv_sphere() if sphere_tris else uv_sphere(9, 10)
+    centers = []
+    while len(centers) < 64:
+        r = rng.uniform(0.12, 0.28)
+        ang = rng.uniform(0, 2 * np.pi)
+        dist = rng.uniform(1.35, 2.6)
+        y = rng.uniform(-1.1, 1.1)
+        c = np.array([dist * np.cos(ang), y, dist * np.sin(ang)])
+        if all(np.linalg.norm(c - c2) > r + r2 + 0.02 for c2, r2 in centers):
+            centers.append((c, r))
+    for c, r in centers:
+        kind = rng.integers(0, 3)
+        if kind == 0:
+            m = dict(type=MAT_CONDUCTOR, albedo=(1, 1, 1), roughness=float(rng.uniform(0.05, 0.8)),
+                     eta=tuple(rng.uniform(0.2, 1.5, 3)), k=tuple(rng.uniform(2.0, 4.0, 3)))
+        elif kind == 1:
+            # roughness 0 makes the reference's GGX density 0/0; 0.02 is the defined minimum
+            m = dict(type=MAT_DIELECTRIC, albedo=(1, 1, 1), roughness=float(max(rng.uniform(0.0, 0.3), 0.02)),
+                     int_ior=1.5, ext_ior=1.0)
+        else:
+            m = dict(type=MAT_PLASTIC, albedo=tuple(rng.uniform(0.1, 0.9, 3)), int_ior=1.5, ext_ior=1.0)
+        meshes.append(MeshSpec((sv * r + c).astype(np.float32), sf.astype(np.int32), m))
+    env = sky(*env_size)
+    cam = dict(from_=(0.0, 0.9, -5.2), at=(0.0, 0.0, 0.0), up=(0, 1, 0))
+    settings = dict(width=width, height=height, spp=spp, max_depth=16, rr_depth=0, rng=RNG_PCG32, seed=seed,
+                    filter=FILTER_GAUSSIAN)
+    return SceneSpec("spheres", meshes, [], [], env, cam, settings)
+
+
+def _material_obj(d):
+    return material(**d)
+
+
+def build_scene(spec: SceneSpec) -> Scene:
+    """A CUDA-library Scene holding the spec's meshes, lights, media and sky."""
+    s = Scene()
+    for m in spec.meshes:
+        s.add_mesh(m.positions, _material_obj(m.material), indices=m.indices, out_medium=m.out_medium,
+                   in_medium=m.in_medium)
+    for l in spec.lights:
+        s.add_light(light(**l))
+    for md in spec.media:
+        s.add_medium(medium(**md))
+    if spec.env is not None:
+        s.add_env(spec.env)
+    return s
+
+
+def build_renderer(spec: SceneSpec, **overrides) -> tuple:
+    s = build_scene(spec)
+    st = dict(spec.settings)
+    st.update(overrides)
+    r = Renderer(s, options(**st))
+    r.set_camera(camera(**spec.camera))
+    return s, r
+
+
+SCENES = {"cornell": cornell, "spheres": spheres}

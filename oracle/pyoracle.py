@@ -1,0 +1,170 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
+bench.py's CPU-baseline leg, always as the checker of the CUDA library.  It
+also loads the host build of the reference's own shading code
+(oracle/_ref/*.so) when that was built, for pinning the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+REF_DIR = HERE / "_ref"
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            raise ImportError(f"{LIB} missing: run `make -C oracle`")
+        _lib = C.CDLL(str(LIB))
+        P, VP, I32, I64, F = C.POINTER, C.c_void_p, C.c_int32, C.c_int64, C.c_float
+        _lib.orc_scene_new.restype = VP
+        _lib.orc_scene_new.argtypes = [P(F), P(F), P(F), P(I32), I64, VP, P(I32), I32, VP, I32, VP, I32, P(F), I32,
+                                       I32]
+        _lib.orc_scene_free.argtypes = [VP]
+        _lib.orc_render.restype = I32
+        _lib.orc_render.argtypes = [VP, I32, VP, VP, I32, P(F), P(F), P(F), P(I64), I32, I32, I32]
+        _lib.orc_camera.argtypes = [VP, I32, I32, P(F)]
+        _lib.orc_trace.restype = I32
+        _lib.orc_trace.argtypes = [VP, I32, I32, P(F), I64, P(C.c_double)]
+        _lib.orc_shading.restype = I32
+        _lib.orc_shading.argtypes = [I32, I32, VP, I32, VP, I32, VP, I32, P(F), I64, P(F)]
+        _lib.orc_kulla_conty.argtypes = [P(F), P(F)]
+        _lib.orc_env_cache.argtypes = [P(F), I32, I32, P(F)]
+        _lib.orc_tonemap.argtypes = [P(F), I64, I32, F, P(C.c_uint32)]
+    return _lib
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class OracleScene:
+    """The oracle's copy of a SceneSpec (optixrender_b200.scenes)."""
+
+    def __init__(self, spec):
+        import optixrender_b200 as rt
+        lib = load()
+        tris, tmesh = [], []
+        mats = []
+        media_pairs = []
+        for i, m in enumerate(spec.meshes):
+            t = m.triangles()
+            tris.append(t)
+            tmesh.append(np.full(t.shape[0], i, np.int32))
+            mats.append(rt.material(**m.material))
+            media_pairs += [m.out_medium, m.in_medium]
+        self.tv = np.ascontiguousarray(np.concatenate(tris), np.float32)
+        self.tmesh = np.ascontiguousarray(np.concatenate(tmesh), np.int32)
+        self.mats = (rt.Material * len(mats))(*mats)
+        self.mm = np.asarray(media_pairs, np.int32)
+        self.lights = (rt.Light * max(1, len(spec.lights)))(*[rt.light(**l) for l in spec.lights])
+        self.media = (rt.Medium * max(1, len(spec.media)))(*[rt.medium(**m) for m in spec.media])
+        env = spec.env
+        self.env = None if env is None else np.ascontiguousarray(env, np.float32)
+        eh, ew = (0, 0) if env is None else env.shape[:2]
+        self.h = lib.orc_scene_new(_f(self.tv), None, None, self.tmesh.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   self.tv.shape[0], C.cast(self.mats, C.c_void_p),
+                                   self.mm.ctypes.data_as(C.POINTER(C.c_int32)), len(mats),
+                                   C.cast(self.lights, C.c_void_p), len(spec.lights), C.cast(self.media, C.c_void_p),
+                                   len(spec.media), None if env is None else _f(self.env), ew, eh)
+        self.spec = spec
+
+    def close(self):
+        if self.h:
+            load().orc_scene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, opts, cam, frame=0, color=None, precision=32, threads=0, rows=None, want_aov=True):
+        """One Renderer::Render of the reference integrator on the CPU.
+        Returns (color, albedo, normal, nan_count) as (h, w, 4) arrays."""
+        lib = load()
+        w, h = opts.width, opts.height
+        if color is None:
+            color = np.zeros((h, w, 4), np.float32)
+        alb = np.zeros((h, w, 4), np.float32) if want_aov else None
+        nrm = np.zeros((h, w, 4), np.float32) if want_aov else None
+        nan = C.c_int64()
+        r0, r1 = rows if rows is not None else (0, 0)
+        rc = lib.orc_render(self.h, precision, C.byref(opts), C.byref(cam), frame, _f(color),
+                            None if alb is None else _f(alb), None if nrm is None else _f(nrm), C.byref(nan),
+                            threads, r0, r1)
+        if rc:
+            raise RuntimeError("orc_render failed")
+        return color, alb, nrm, nan.value
+
+    def trace(self, rays, any_hit=False, precision=64):
+        lib = load()
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.zeros((r.shape[0], 8), np.float64)
+        lib.orc_trace(self.h, precision, 1 if any_hit else 0, _f(r), r.shape[0],
+                      out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+
+def shading(op, inputs, materials=(), lights=(), media=(), precision=64):
+    import optixrender_b200 as rt
+    lib = load()
+    x = np.ascontiguousarray(inputs, np.float32).reshape(-1, 16)
+    out = np.zeros((x.shape[0], 8), np.float32)
+    M = (rt.Material * max(1, len(materials)))(*materials)
+    L = (rt.Light * max(1, len(lights)))(*lights)
+    D = (rt.Medium * max(1, len(media)))(*media)
+    lib.orc_shading(precision, op, C.cast(M, C.c_void_p), len(materials), C.cast(L, C.c_void_p), len(lights),
+                    C.cast(D, C.c_void_p), len(media), _f(x), x.shape[0], _f(out))
+    return out
+
+
+def kulla_conty():
+    lib = load()
+    a = np.zeros(4096, np.float32)
+    b = np.zeros(64, np.float32)
+    lib.orc_kulla_conty(_f(a), _f(b))
+    return a.reshape(64, 64), b
+
+
+def env_cache(rgba):
+    lib = load()
+    img = np.ascontiguousarray(rgba, np.float32)
+    h, w = img.shape[:2]
+    out = np.zeros_like(img)
+    lib.orc_env_cache(_f(img), w, h, _f(out))
+    return out
+
+
+def tonemap(color, mode=0, exposure=1.0):
+    lib = load()
+    c = np.ascontiguousarray(color, np.float32).reshape(-1, 4)
+    out = np.zeros(c.shape[0], np.uint32)
+    lib.orc_tonemap(_f(c), c.shape[0], mode, exposure, out.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return out.reshape(color.shape[:-1])
+
+
+def camera_vectors(cam, w, h):
+    lib = load()
+    out = np.zeros(12, np.float32)
+    lib.orc_camera(C.byref(cam), w, h, _f(out))
+    return out.reshape(4, 3)
+
+
+# ---------------------------------------------------------------- reference host build
+def ref_libs():
+    """(shading, scene, rng) libraries built from the reference sources, or None."""
+    paths = [REF_DIR / n for n in ("libref_shading.so", "libref_scene.so", "libref_rng.so")]
+    if not all(p.exists() for p in paths):
+        return None
+    return tuple(C.CDLL(str(p)) for p in paths)
