@@ -186,7 +186,7 @@ typedef struct rt_render_stats {
     int64_t tris_tested;
     int64_t extend_nodes;
     int64_t extend_tris;
-    int64_t nan_samples;
+    int64_t nan_samples;       /* samples dropped for a NaN radiance */
     int32_t waves;
     int32_t launches;          /* kernels launched by the last Render() */
     float ms_total;            /* device time of the last Render() */
@@ -195,6 +195,7 @@ typedef struct rt_render_stats {
     float ms_shadow;
     float ms_other;
     int64_t extend_launches;
+    int64_t nan_throughput_paths; /* paths ended by IsNan(history), devicePrograms.cu:487-489 */
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */
@@ -245,6 +246,11 @@ RT_API rt_status rt_scene_set_env(rt_scene* s, const float* rgba, int32_t width,
 RT_API rt_status rt_scene_get_bounds(const rt_scene* s, float lo[3], float hi[3]);
 RT_API rt_status rt_scene_counts(const rt_scene* s, int64_t* triangles, int32_t* meshes, int32_t* lights,
                                  int32_t* media);
+/* Builds the acceleration structure (the work of optixAccelBuild,
+ * core/src/Renderer.cpp:146-285) on the host and validates it: every child and
+ * triangle index in range, every quantised box containing what it bounds.
+ * Needs no device. */
+RT_API rt_status rt_scene_build_bvh(const rt_scene* s, int64_t* num_nodes, int32_t* depth);
 /* SceneParser::LoadFromJson, core/src/SceneParser.cpp:3-23 and the schema of
  * models/test.json.  Fills `opts`/`cam` (may be NULL) from the file. */
 RT_API rt_status rt_scene_load_json(rt_scene* s, const char* path, rt_options* opts, rt_camera* cam);

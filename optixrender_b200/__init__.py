@@ -82,7 +82,7 @@ class RenderStats(C.Structure):
                 ("extend_tris", C.c_int64), ("nan_samples", C.c_int64), ("waves", C.c_int32),
                 ("launches", C.c_int32), ("ms_total", C.c_float), ("ms_extend", C.c_float),
                 ("ms_shade", C.c_float), ("ms_shadow", C.c_float), ("ms_other", C.c_float),
-                ("extend_launches", C.c_int64)]
+                ("extend_launches", C.c_int64), ("nan_throughput_paths", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -124,6 +124,7 @@ def load_library():
         "rt_scene_get_bounds": (I32, [VP, P(F), P(F)]),
         "rt_scene_counts": (I32, [VP, P(I64), P(I32), P(I32), P(I32)]),
         "rt_scene_load_json": (I32, [VP, C.c_char_p, P(Options), P(Camera)]),
+        "rt_scene_build_bvh": (I32, [VP, P(I64), P(I32)]),
         "rt_scene_load_json_string": (I32, [VP, C.c_char_p, C.c_char_p, P(Options), P(Camera)]),
         "rt_renderer_create": (I32, [VP, P(Options), P(VP)]),
         "rt_renderer_destroy": (I32, [VP]),
@@ -312,6 +313,12 @@ class Scene:
         _check(self._lib.rt_scene_load_json_string(self._h, text.encode(), str(base_dir).encode(), C.byref(o),
                                                    C.byref(c)))
         return o, c
+
+    def build_bvh(self):
+        """Host build and validation of the acceleration structure: (nodes, depth)."""
+        n, d = C.c_int64(), C.c_int32()
+        _check(self._lib.rt_scene_build_bvh(self._h, C.byref(n), C.byref(d)))
+        return n.value, d.value
 
     def bounds(self):
         lo = (C.c_float * 3)()

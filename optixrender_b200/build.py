@@ -22,7 +22,7 @@ BUILD = PKG / "_build"
 LIBNAME = "liboptixrender_b200.so"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-CXX = os.environ.get("CXX", "g++")
+CXX = os.environ.get("RT_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-ftz=true", "-prec-div=false", "-prec-sqrt=false",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]

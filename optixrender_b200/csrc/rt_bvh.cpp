@@ -199,6 +199,7 @@ struct Collapser {
     const Builder& b;
     std::vector<rtd::CwNode>& out;
     std::vector<int>& order;
+    std::vector<Box> wbox;  // true bounds of each wide node
     int max_depth = 0;
 
     Collapser(const Builder& bb, std::vector<rtd::CwNode>& o, std::vector<int>& ord) : b(bb), out(o), order(ord) {}
@@ -331,8 +332,83 @@ struct Collapser {
             }
         }
         out[size_t(wi)] = node;
+        if (wbox.size() < out.size()) wbox.resize(out.size());
+        wbox[size_t(wi)] = nb;
+        for (int s = 0; s < 8; s++) {
+            int c = child_at[s];
+            if (c >= 0 && ((node.imask >> s) & 1u)) {
+                int rank = 0;
+                for (int q = 0; q < s; q++) rank += (node.imask >> q) & 1u;
+                wbox[size_t(node.child_base) + size_t(rank)] = b.nodes[size_t(c)].box;
+            }
+        }
     }
 };
+
+// Checks that every index a traversal can form stays in range and that each
+// quantised child box contains the child it stands for.
+bool validate(const std::vector<rtd::CwNode>& nodes, const std::vector<int>& order, const std::vector<Box>& wbox,
+              const float* tv, std::string& err) {
+    const size_t nn = nodes.size(), nt = order.size();
+    for (size_t i = 0; i < nn; i++) {
+        const rtd::CwNode& n = nodes[i];
+        const float p[3] = {n.px, n.py, n.pz};
+        const int e[3] = {int(n.ex) - 127, int(n.ey) - 127, int(n.ez) - 127};
+        const uint8_t* qlo[3] = {n.qlox, n.qloy, n.qloz};
+        const uint8_t* qhi[3] = {n.qhix, n.qhiy, n.qhiz};
+        int rank = 0;
+        for (int s = 0; s < 8; s++) {
+            if (n.meta[s] == 0) {
+                if ((n.imask >> s) & 1u) {
+                    err = "internal slot without meta";
+                    return false;
+                }
+                continue;
+            }
+            double lo[3], hi[3];
+            for (int a = 0; a < 3; a++) {
+                lo[a] = double(p[a]) + std::ldexp(double(qlo[a][s]), e[a]);
+                hi[a] = double(p[a]) + std::ldexp(double(qhi[a][s]), e[a]);
+            }
+            auto inside = [&](const float* v) {
+                for (int a = 0; a < 3; a++)
+                    if (double(v[a]) < lo[a] || double(v[a]) > hi[a]) return false;
+                return true;
+            };
+            if ((n.imask >> s) & 1u) {
+                size_t c = size_t(n.child_base) + size_t(rank++);
+                if (c >= nn || c == i) {
+                    err = "child index out of range";
+                    return false;
+                }
+                const Box& cb = wbox[c];
+                if (!inside(cb.lo) || !inside(cb.hi)) {
+                    err = "quantised box does not contain its child node";
+                    return false;
+                }
+                if ((n.meta[s] & 31u) != uint32_t(24 + s) || (n.meta[s] >> 5) != 1u) {
+                    err = "bad internal meta";
+                    return false;
+                }
+            } else {
+                uint32_t unary = n.meta[s] >> 5, off = n.meta[s] & 31u;
+                int cnt = unary == 1 ? 1 : unary == 3 ? 2 : unary == 7 ? 3 : 0;
+                if (cnt == 0 || off + uint32_t(cnt) > 24 || size_t(n.tri_base) + off + size_t(cnt) > nt) {
+                    err = "leaf triangle range out of bounds";
+                    return false;
+                }
+                for (int k = 0; k < cnt; k++) {
+                    const float* t = tv + size_t(order[size_t(n.tri_base) + off + size_t(k)]) * 9;
+                    if (!inside(t) || !inside(t + 3) || !inside(t + 6)) {
+                        err = "quantised box does not contain its triangles";
+                        return false;
+                    }
+                }
+            }
+        }
+    }
+    return true;
+}
 
 }  // namespace
 
@@ -383,7 +459,15 @@ bool build_cwbvh(const float* tv, int64_t ntri, BuiltBvh& res, std::string& err)
         err = "internal error: triangle count mismatch after collapse";
         return false;
     }
-    return true;
+    std::vector<char> seen(size_t(ntri), 0);
+    for (int t : res.order) {
+        if (t < 0 || t >= ntri || seen[size_t(t)]) {
+            err = "internal error: triangle order is not a permutation";
+            return false;
+        }
+        seen[size_t(t)] = 1;
+    }
+    return validate(res.nodes, res.order, c.wbox, tv, err);
 }
 
 }  // namespace rth

@@ -384,6 +384,17 @@ rt_status rt_scene_counts(const rt_scene* s, int64_t* tris, int32_t* meshes, int
     return RT_OK;
 }
 
+rt_status rt_scene_build_bvh(const rt_scene* s, int64_t* num_nodes, int32_t* depth) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_scene_build_bvh: NULL scene");
+    rth::BuiltBvh bvh;
+    std::string err;
+    if (!rth::build_cwbvh(s->tv.data(), int64_t(s->tri_mesh.size()), bvh, err))
+        return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
+    if (num_nodes) *num_nodes = int64_t(bvh.nodes.size());
+    if (depth) *depth = bvh.depth;
+    return RT_OK;
+}
+
 // ====================================================================== tables
 rt_status rt_kulla_conty_lut(float* bsdf, float* avg) {
     if (!bsdf || !avg) return fail(RT_ERR_INVALID_ARG, "rt_kulla_conty_lut: NULL argument");

@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
             B.sh_d[p1] = f4(s1d, __int_as_float(slot * 2 + 1));
         }
     }
-    if (Stats) warp_stat(&ctl->stats[6], nan_paths);
+    if (Stats) warp_stat(&ctl->stats[7], nan_paths);
 }
 
 // ------------------------------------------------------------------ shadow

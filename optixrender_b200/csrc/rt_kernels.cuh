@@ -53,7 +53,8 @@ struct WaveCtl {
     int fetch_shadow;
     int error;
     int pad;
-    unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris, nan, spare
+    unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris,
+                                  // NaN samples, paths ended by a NaN throughput
 };
 
 // Structure-of-arrays path state, one entry per slot of a wave.

@@ -516,6 +516,7 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     out->nodes_visited = int64_t(ctl.stats[2] + ctl.stats[4]);
     out->tris_tested = int64_t(ctl.stats[3] + ctl.stats[5]);
     out->nan_samples = int64_t(ctl.stats[6]);
+    out->nan_throughput_paths = int64_t(ctl.stats[7]);
     out->waves = r->waves;
     out->launches = r->launches;
     out->extend_launches = r->extend_launches;

@@ -144,30 +144,21 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
     int sp = 0;
     // node group: x = base node index, y = internal hit bits (24..31) | parent imask (0..7)
     uint2 g = make_uint2(0u, 1u << (24 + r.oct));
-    uint2 tg = make_uint2(0u, 0u);
+    // Invariant at the top of the loop: g holds at least one internal-child bit.
     while (true) {
-        if (g.y & 0xFF000000u) {
-            uint32_t bits = g.y >> 24;
-            uint32_t bit = __ffs(bits) - 1u;
-            g.y &= ~(1u << (24 + bit));
-            uint32_t slot = bit ^ r.oct;
-            uint32_t idx = g.x + __popc((g.y & 0xFFu) & ((1u << slot) - 1u));
-            if (g.y & 0xFF000000u) {
-                if (sp < kStackSize) stack[sp++] = g;
-            }
-            uint32_t cb, tb, tbits;
-            uint32_t nb = intersect_children(sc.nodes, idx, r, tmax, cb, tb, tbits);
-            if (Stats) nodes_visited++;
-            g = make_uint2(cb, nb);
-            tg = make_uint2(tb, tbits);
-        } else {
-            tg = g;
-            g = make_uint2(0u, 0u);
-        }
-        while (tg.y & 0x00FFFFFFu) {
-            uint32_t b = __ffs(tg.y) - 1u;
-            tg.y &= ~(1u << b);
-            uint32_t ti = tg.x + b;
+        uint32_t bit = __ffs(g.y >> 24) - 1u;
+        g.y &= ~(1u << (24 + bit));
+        uint32_t slot = bit ^ r.oct;
+        uint32_t idx = g.x + __popc((g.y & 0xFFu) & ((1u << slot) - 1u));
+        if ((g.y & 0xFF000000u) && sp < kStackSize) stack[sp++] = g;
+        uint32_t cb, tb, tbits;
+        uint32_t nb = intersect_children(sc.nodes, idx, r, tmax, cb, tb, tbits);
+        if (Stats) nodes_visited++;
+        g = make_uint2(cb, nb);
+        while (tbits) {
+            uint32_t b = __ffs(tbits) - 1u;
+            tbits &= ~(1u << b);
+            uint32_t ti = tb + b;
             const float4* tv = sc.tri_v + size_t(ti) * 3;
             float4 a = __ldg(tv), bb = __ldg(tv + 1), c = __ldg(tv + 2);
             if (Stats) tris_tested++;
@@ -181,8 +172,8 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
                 if (AnyHit) return hit_tri;
             }
         }
-        if (!(g.y & 0xFF000000u)) {
-            if (sp == 0) break;
+        while (!(g.y & 0xFF000000u)) {
+            if (sp == 0) return hit_tri;
             g = stack[--sp];
         }
     }

@@ -121,6 +121,11 @@ def uv_sphere(n_lat=101, n_lon=100):
 
 
 def _hash3(ix, iy, iz, seed):
+    with np.errstate(over="ignore"):
+        return _hash3_impl(ix, iy, iz, seed)
+
+
+def _hash3_impl(ix, iy, iz, seed):
     h = (ix.astype(np.uint64) * np.uint64(0x8da6b343) ^ iy.astype(np.uint64) * np.uint64(0xd8163841) ^
          iz.astype(np.uint64) * np.uint64(0xcb1ab31f) ^ np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15))
     h ^= h >> np.uint64(33)
