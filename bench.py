@@ -209,8 +209,8 @@ def main():
     from optixrender_b200 import scenes
     torch.cuda.set_device(local)
     spec = scenes.spheres(spp=args.spp, seed=1 + rank)
-    s, r = scenes.build_renderer(spec, collect_stats=1)
-    stream = torch.cuda.current_stream()
+    s, r = scenes.build_renderer(spec, collect_stats=0)
+    stream = torch.cuda.Stream()
     r.set_stream(stream.cuda_stream)
     W, H = spec.settings["width"], spec.settings["height"]
     paths_per_step = W * H * args.spp
@@ -220,37 +220,50 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kern = {"extend": 0.0, "shade": 0.0, "shadow": 0.0, "other": 0.0}
-    counters = {"extend_rays": 0, "extend_nodes": 0, "extend_tris": 0, "shadow_rays": 0, "nodes": 0, "tris": 0,
-                "launches": 0, "extend_launches": 0, "nan": 0,
-                "nan_history": 0}
+    # timed region A: the production path (one captured graph per wave)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
             r.render()
-            st = r.stats()  # per-kernel events of this step (synchronizes)
-            for k in kern:
-                kern[k] += st["ms_" + k]
-            counters["extend_rays"] += st["extend_rays"]
-            counters["extend_nodes"] += st["extend_nodes"]
-            counters["extend_tris"] += st["extend_tris"]
-            counters["shadow_rays"] += st["shadow_rays"]
-            counters["nodes"] += st["nodes_visited"]
-            counters["tris"] += st["tris_tested"]
-            counters["launches"] += st["launches"]
-            counters["extend_launches"] += st["extend_launches"]
-            counters["nan"] += st["nan_samples"]
-            counters["nan_history"] += st["nan_throughput_paths"]
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
+    launches_per_step = r.stats()["launches"]
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     ms_step = ms / args.steps
     value = paths_per_step * world / (ms_step / 1e3) / 1e6
+
+    # timed region B: the same steps with a CUDA event pair around every kernel
+    # and device counters of nodes / triangles / rays, for the roofline
+    o = r.options
+    o.collect_stats = 1
+    r.set_options(o)
+    kern = {"extend": 0.0, "shade": 0.0, "shadow": 0.0, "other": 0.0}
+    counters = {"extend_rays": 0, "extend_nodes": 0, "extend_tris": 0, "shadow_rays": 0, "nodes": 0, "tris": 0,
+                "extend_launches": 0, "nan": 0, "nan_history": 0, "ms": 0.0}
+    r.render()  # warm the per-kernel path once
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        r.render()
+        st = r.stats()
+        for k in kern:
+            kern[k] += st["ms_" + k]
+        counters["ms"] += st["ms_total"]
+        counters["extend_rays"] += st["extend_rays"]
+        counters["extend_nodes"] += st["extend_nodes"]
+        counters["extend_tris"] += st["extend_tris"]
+        counters["shadow_rays"] += st["shadow_rays"]
+        counters["nodes"] += st["nodes_visited"]
+        counters["tris"] += st["tris_tested"]
+        counters["extend_launches"] += st["extend_launches"]
+        counters["nan"] += st["nan_samples"]
+        counters["nan_history"] += st["nan_throughput_paths"]
+    o.collect_stats = 0
+    r.set_options(o)
 
     # end to end through the C ABI: render + RGBA8 download to pinned host memory
     host = torch.empty((H, W), dtype=torch.int32, pin_memory=True)
@@ -278,7 +291,6 @@ def main():
                  counters["extend_rays"] * RAY_BYTES)
     ext_ms = kern["extend"]
     achieved = ext_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
-    launches_per_step = counters["launches"] / args.steps
     traffic = None
     prof = ROOT / "profiles" / "extend_traffic.json"
     if prof.exists():
@@ -293,13 +305,14 @@ def main():
         "config": {"workload": "spheres-1080p", **dict(WORKLOAD, spp=args.spp), "triangles": spec.num_triangles,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (scene + BVH ~0.3 GB)"},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": W * H * 4},
-        "gpu_launches": int(counters["launches"]),
+        "gpu_launches": int(launches_per_step * args.steps),
         "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak if peak else None,
                      "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": ext_bytes / max(1, counters["extend_launches"]),
                      "ms_extend_per_launch": ext_ms / max(1, counters["extend_launches"])},
         "kernel_ms_per_step": {k: v / args.steps for k, v in kern.items()},
+        "instrumented_ms_per_step": counters["ms"] / args.steps,
         "rays_per_step": {"extend": counters["extend_rays"] / args.steps,
                           "shadow": counters["shadow_rays"] / args.steps},
         "nan_samples": counters["nan"], "paths_ended_by_nan_throughput": counters["nan_history"],

@@ -87,6 +87,11 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     if force or jobs or not _newer(lib, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", str(lib)] + [str(o) for o in objs] +
              ["-Xcompiler", "-fopenmp", "-lgomp", "-cudart", "static"])
+    cli = LIBDIR / "render_json"
+    src = PKG / "cpp" / "render_json.cpp"
+    if src.exists() and (force or not _newer(cli, [src, lib, ROOT / "include" / "optixrender.hpp"])):
+        _run([CXX, "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(src), "-o", str(cli), "-L", str(LIBDIR),
+              "-loptixrender_b200", "-Wl,-rpath,$ORIGIN"])
     return lib
 
 

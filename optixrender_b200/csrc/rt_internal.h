@@ -66,5 +66,6 @@ struct DeviceScene {
     ~DeviceScene();
 };
 rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st);
+void grid_majorants(const float* dens, const int res[3], int mres, std::vector<float>& out);
 
 }  // namespace rti

@@ -18,6 +18,7 @@
 #include <cstdio>
 
 #include "rt_kernels.cuh"
+#include "rt_media.cuh"
 #include "rt_shading.cuh"
 #include "rt_traverse.cuh"
 
@@ -25,9 +26,11 @@ namespace rtd {
 
 constexpr int kBlock = 128;
 
-RT_D int find_segment(const Ctx& c, int slot) {
-    int s = c.num_seg - 1;
-    while (s > 0 && slot < __ldg(&c.seg[s].slot_begin)) s--;
+RT_D const WaveParams& wave_of(const Ctx& c) { return c.waves[*c.wave_index]; }
+
+RT_D int find_segment(const WaveParams& w, int slot) {
+    int s = w.num_seg - 1;
+    while (s > 0 && slot < w.seg[s].slot_begin) s--;
     return s;
 }
 
@@ -70,16 +73,17 @@ __global__ void k_begin(const JobDesc* __restrict__ jd) {
 __global__ void k_raygen(Ctx c) {
     int slot = blockIdx.x * blockDim.x + threadIdx.x;
     WaveCtl* ctl = c.wb.ctl;
+    const WaveParams& W = wave_of(c);
     if (slot == 0) {
-        ctl->count[0] = c.wave_count;
+        ctl->count[0] = W.wave_count;
         ctl->count[1] = 0;
         ctl->shadow_count = 0;
         ctl->fetch_ext = 0;
         ctl->fetch_shade = 0;
         ctl->fetch_shadow = 0;
     }
-    if (slot >= c.wave_count) return;
-    const Segment sg = c.seg[find_segment(c, slot)];
+    if (slot >= W.wave_count) return;
+    const Segment sg = W.seg[find_segment(W, slot)];
     const JobDesc* jd = c.jobs + sg.job;
     const JobParams& j = jd->job;
     const CameraView& cam = jd->cam;
@@ -113,8 +117,26 @@ __global__ void k_raygen(Ctx c) {
 }
 
 // ------------------------------------------------------------------ extend
+struct ExtendSrc {
+    const Ctx* c;
+    const int* q;
+    RT_D void load(int i, TravRay& r, const SceneView*& sc) {
+        int slot = q[i];
+        const WaveParams& W = wave_of(*c);
+        sc = &c->jobs[W.seg[find_segment(W, slot)].job].sc;
+        float4 o = c->wb.ray_o[slot], d = c->wb.ray_d[slot];
+        r.o = xyz(o);
+        r.d = xyz(d);
+        r.tmin = kEps;
+        r.tmax = FLT_MAX;
+    }
+    RT_D void finish(int i, int tri, float t, float b1, float b2) {
+        c->wb.hit[q[i]] = make_float4(tri >= 0 ? t : FLT_MAX, b1, b2, __int_as_float(tri));
+    }
+};
+
 template <bool Stats>
-__global__ void __launch_bounds__(kBlock) k_extend(Ctx c) {
+__global__ void __launch_bounds__(kBlock, 8) k_extend(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     const int cur = c.bounce & 1, nxt = cur ^ 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -123,29 +145,9 @@ __global__ void __launch_bounds__(kBlock) k_extend(Ctx c) {
         ctl->fetch_shade = 0;
     }
     const int total = ctl->count[cur];
-    const int* __restrict__ q = c.wb.queue[cur];
-    const int lane = threadIdx.x & 31;
     uint32_t nodes = 0, tris = 0, rays = 0;
-    while (true) {
-        int base = warp_fetch(&ctl->fetch_ext, lane);
-        if (base >= total) break;
-        int i = base + lane;
-        if (i < total) {
-            int slot = q[i];
-            const JobDesc* jd = c.jobs + c.seg[find_segment(c, slot)].job;
-            float4 o = c.wb.ray_o[slot], d = c.wb.ray_d[slot];
-            TravRay r;
-            r.o = xyz(o);
-            r.d = xyz(d);
-            r.tmin = kEps;
-            r.tmax = FLT_MAX;
-            prepare_ray(r);
-            float t = FLT_MAX, b1 = 0.f, b2 = 0.f;
-            int tri = traverse<false, Stats>(jd->sc, r, t, b1, b2, nodes, tris);
-            c.wb.hit[slot] = make_float4(t, b1, b2, __int_as_float(tri));
-            rays++;
-        }
-    }
+    ExtendSrc src{&c, c.wb.queue[cur]};
+    traverse_queue<false, Stats>(src, &ctl->fetch_ext, total, nodes, tris, rays);
     if (Stats) {
         warp_stat(&ctl->stats[0], rays);
         warp_stat(&ctl->stats[2], nodes);
@@ -172,6 +174,27 @@ RT_D bool light_trace(const SceneView& sc, v3 o, v3 d, float& closest, v3& lrad,
 
 RT_D bool nee_pdf_ok(float p) { return p > 0.0f && p < FLT_MAX; }
 
+// SampleMediumDistance (Medium.h:233-244) for either medium type.
+template <class RNG>
+RT_D bool medium_sample(const DevMedium* mp, const MedParams& med, v3 o, v3 d, float maxd, float& dist, float& tp,
+                        v3& tr, RNG& rng) {
+    if (med.type == RT_MEDIUM_GRID) {
+        tp = 1.0f;
+        return grid_sample_distance(load_grid(mp), o, d, maxd, rng, dist, tr);
+    }
+    return sample_medium_distance(med, maxd, dist, tp, tr, rng);
+}
+// EvaluateMediumDistance(medium, false, ...) (Medium.h:222-231): the
+// transmittance of a next-event segment; ratio tracking for a grid.
+template <class RNG>
+RT_D v3 medium_transmittance(const DevMedium* mp, const MedParams& med, v3 o, v3 d, float dist, float& tp, RNG& rng) {
+    if (med.type == RT_MEDIUM_GRID) {
+        tp = 1.0f;
+        return v3(grid_transmittance(load_grid(mp), o, d, dist, rng));
+    }
+    return eval_medium_distance(med, false, dist, tp);
+}
+
 // ------------------------------------------------------------------ shade
 template <bool Stats>
 __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
@@ -185,6 +208,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
     const int total = ctl->count[cur];
     const int* __restrict__ q = c.wb.queue[cur];
     const WaveBufs& B = c.wb;
+    const WaveParams& W = wave_of(c);
     const int lane = threadIdx.x & 31;
     uint32_t nan_paths = 0;
     while (true) {
@@ -198,7 +222,8 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
         float s0t = 0.f, s1t = 0.f;
         if (i < total) {
             slot = q[i];
-            const JobDesc* jd = c.jobs + c.seg[find_segment(c, slot)].job;
+            const Segment& sgm = W.seg[find_segment(W, slot)];
+            const JobDesc* jd = c.jobs + sgm.job;
             const SceneView& sc = jd->sc;
             const JobParams& jp = jd->job;
             float4 o4 = B.ray_o[slot], d4 = B.ray_d[slot], th = B.thr[slot], h4 = B.hit[slot];
@@ -210,8 +235,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
             if (jp.rng == RT_RNG_LCG) {
                 rng.inc = 0;
             } else {
-                const Segment& sg = c.seg[find_segment(c, slot)];
-                rng.inc = pcg_inc(uint64_t(sg.path_begin + (slot - sg.slot_begin)));
+                rng.inc = pcg_inc(uint64_t(sgm.path_begin + (slot - sgm.slot_begin)));
             }
             v3 o = xyz(o4), d = xyz(d4);
             v3 history = xyz(th);
@@ -278,10 +302,11 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
             if (sc.num_media != 0) {
                 medium_index = (hit_light || s.front) ? out_m : in_m;
                 if (medium_index != -1) {
-                    const MedParams med = load_medium(sc.media + medium_index);
+                    const DevMedium* mp = sc.media + medium_index;
+                    const MedParams med = load_medium(mp);
                     float distance = 0.0f, trans_pdf = 0.0f;
                     v3 tr;
-                    scattered = sample_medium_distance(med, closest, distance, trans_pdf, tr, rng);
+                    scattered = medium_sample(mp, med, o, d, closest, distance, trans_pdf, tr, rng);
                     history *= (tr / trans_pdf);
                     mult_trans_pdf *= trans_pdf;
                     if (scattered) {
@@ -301,7 +326,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                             int tm;
                             if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
                                 float tp2, phase_pdf;
-                                v3 tr2 = eval_medium_distance(med, false, cl, tp2);
+                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng);
                                 v3 att = evaluate_phase(med, V, sd, phase_pdf);
                                 float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, phase_pdf * tp2);
                                 nee_l = w * (tr2 / tp2) * lr * att * history / lp;
@@ -361,9 +386,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                             float w = power_heuristic(lp, bpdf);
                             v3 thh(1.0f);
                             if (medium_index != -1) {
-                                const MedParams med = load_medium(sc.media + medium_index);
+                                const DevMedium* mp = sc.media + medium_index;
+                                const MedParams med = load_medium(mp);
                                 float tp2;
-                                v3 tr2 = eval_medium_distance(med, false, cl, tp2);
+                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng);
                                 thh = tr2 / tp2;
                                 w = power_heuristic(lp, bpdf * tp2);
                             }
@@ -394,9 +420,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                             float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, bpdf);
                             v3 thh(1.0f);
                             if (medium_index != -1) {
-                                const MedParams med = load_medium(sc.media + medium_index);
+                                const DevMedium* mp = sc.media + medium_index;
+                                const MedParams med = load_medium(mp);
                                 float tp2;
-                                v3 tr2 = eval_medium_distance(med, false, cl, tp2);
+                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng);
                                 thh = tr2 / tp2;
                                 if (l.type != RT_LIGHT_POINT) w = power_heuristic(lp, bpdf * tp2);
                             }
@@ -458,35 +485,35 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
 }
 
 // ------------------------------------------------------------------ shadow
+// Shadow rays whose tmax is not above tmin cannot hit anything (the reference
+// traces [EPS, light_distance - EPS]); they keep their contribution.
+struct ShadowSrc {
+    const Ctx* c;
+    RT_D void load(int i, TravRay& r, const SceneView*& sc) {
+        float4 o = c->wb.sh_o[i], d = c->wb.sh_d[i];
+        int slot = __float_as_int(d.w) >> 1;
+        const WaveParams& W = wave_of(*c);
+        sc = &c->jobs[W.seg[find_segment(W, slot)].job].sc;
+        r.o = xyz(o);
+        r.d = xyz(d);
+        r.tmin = kEps;
+        r.tmax = o.w;
+    }
+    RT_D void finish(int i, int tri, float, float, float) {
+        if (tri < 0) return;
+        int code = __float_as_int(c->wb.sh_d[i].w);
+        int slot = code >> 1;
+        (code & 1 ? c->wb.nee1 : c->wb.nee0)[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+};
+
 template <bool Stats>
-__global__ void __launch_bounds__(kBlock) k_shadow(Ctx c) {
+__global__ void __launch_bounds__(kBlock, 8) k_shadow(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     const int total = ctl->shadow_count;
-    const int lane = threadIdx.x & 31;
     uint32_t nodes = 0, tris = 0, rays = 0;
-    while (true) {
-        int base = warp_fetch(&ctl->fetch_shadow, lane);
-        if (base >= total) break;
-        int i = base + lane;
-        if (i < total) {
-            float4 o = c.wb.sh_o[i], d = c.wb.sh_d[i];
-            int code = __float_as_int(d.w);
-            int slot = code >> 1, ch = code & 1;
-            rays++;
-            if (o.w > kEps) {
-                const JobDesc* jd = c.jobs + c.seg[find_segment(c, slot)].job;
-                TravRay r;
-                r.o = xyz(o);
-                r.d = xyz(d);
-                r.tmin = kEps;
-                r.tmax = o.w;
-                prepare_ray(r);
-                float t, b1, b2;
-                int tri = traverse<true, Stats>(jd->sc, r, t, b1, b2, nodes, tris);
-                if (tri >= 0) (ch ? c.wb.nee1 : c.wb.nee0)[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-        }
-    }
+    ShadowSrc src{&c};
+    traverse_queue<true, Stats>(src, &ctl->fetch_shadow, total, nodes, tris, rays);
     if (Stats) {
         warp_stat(&ctl->stats[1], rays);
         warp_stat(&ctl->stats[4], nodes);
@@ -502,8 +529,9 @@ __global__ void __launch_bounds__(kBlock) k_shadow(Ctx c) {
 // dropped alone.
 __global__ void k_resolve(Ctx c) {
     int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= c.wave_count) return;
-    const Segment& sg = c.seg[find_segment(c, slot)];
+    const WaveParams& W = wave_of(c);
+    if (slot >= W.wave_count) return;
+    const Segment& sg = W.seg[find_segment(W, slot)];
     const JobDesc* jd = c.jobs + sg.job;
     const JobParams& j = jd->job;
     const WaveBufs& B = c.wb;
@@ -562,6 +590,8 @@ __global__ void k_resolve(Ctx c) {
     j.acc_normal[pix] = an;
     if (nans) atomicAdd(&B.ctl->stats[6], (unsigned long long)nans);
 }
+
+__global__ void k_next_wave(int* wave_index) { *wave_index += 1; }
 
 // ------------------------------------------------------------------ finalize
 RT_D uint32_t tonemap_pixel(float4 c, int mode, float exposure) {
@@ -749,7 +779,7 @@ static unsigned grid_for(int64_t n, int block) { return unsigned((n + block - 1)
 void launch_begin(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_begin<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
 }
-void launch_raygen(const Ctx& c, cudaStream_t st) { k_raygen<<<grid_for(c.wave_count, 256), 256, 0, st>>>(c); }
+void launch_raygen(const Ctx& c, cudaStream_t st) { k_raygen<<<grid_for(c.wb.capacity, 256), 256, 0, st>>>(c); }
 void launch_extend(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
     if (stats)
         k_extend<true><<<s.blocks_extend, kBlock, 0, st>>>(c);
@@ -768,7 +798,8 @@ void launch_shadow(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t 
     else
         k_shadow<false><<<s.blocks_shadow, kBlock, 0, st>>>(c);
 }
-void launch_resolve(const Ctx& c, cudaStream_t st) { k_resolve<<<grid_for(c.wave_count, 256), 256, 0, st>>>(c); }
+void launch_resolve(const Ctx& c, cudaStream_t st) { k_resolve<<<grid_for(c.wb.capacity, 256), 256, 0, st>>>(c); }
+void launch_next_wave(const Ctx& c, cudaStream_t st) { k_next_wave<<<1, 1, 0, st>>>(c.wave_index); }
 void launch_finalize(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_finalize<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
 }

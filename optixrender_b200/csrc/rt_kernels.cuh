@@ -77,12 +77,20 @@ struct WaveBufs {
     int capacity;
 };
 
+// The per-wave part of a launch, in device memory so that one captured graph
+// serves every wave: kernels read waves[*wave_index].
+struct WaveParams {
+    Segment seg[kMaxSegments];
+    int num_seg;
+    int wave_count;
+    int pad[2];
+};
+
 struct Ctx {
     const JobDesc* jobs;
     WaveBufs wb;
-    const Segment* seg;  // device array of num_seg entries
-    int num_seg;
-    int wave_count;
+    const WaveParams* waves;
+    int* wave_index;  // advanced by k_next_wave at the end of each wave
     int bounce;
     int max_depth;  // largest max_depth of the jobs in the wave
 };
@@ -102,6 +110,7 @@ void launch_extend(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStre
 void launch_shade(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
 void launch_shadow(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
 void launch_resolve(const rtd::Ctx& c, cudaStream_t st);
+void launch_next_wave(const rtd::Ctx& c, cudaStream_t st);
 void launch_finalize(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);
 void launch_trace(const rtd::SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st);
 void launch_verify(int op, const rtd::SceneView& sc, const rtd::DevLight* lights, const rtd::DevMedium* media,

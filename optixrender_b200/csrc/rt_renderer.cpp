@@ -28,6 +28,27 @@ DeviceScene::~DeviceScene() {
         if (e_ != cudaSuccess) return cuda_fail(e_, what); \
     } while (0)
 
+// Per majorant cell, the largest density any trilinear lookup inside the cell
+// can return: the maximum over the voxels within one voxel of the cell.
+void grid_majorants(const float* dens, const int res[3], int mres, std::vector<float>& out) {
+    out.assign(size_t(mres) * mres * mres, 0.0f);
+    for (int cz = 0; cz < mres; cz++)
+        for (int cy = 0; cy < mres; cy++)
+            for (int cx = 0; cx < mres; cx++) {
+                int c[3] = {cx, cy, cz}, lo[3], hi[3];
+                for (int a = 0; a < 3; a++) {
+                    lo[a] = std::max(0, int(std::floor(double(c[a]) * res[a] / mres)) - 1);
+                    hi[a] = std::min(res[a] - 1, int(std::ceil(double(c[a] + 1) * res[a] / mres)) + 1);
+                }
+                float m = 0.0f;
+                for (int z = lo[2]; z <= hi[2]; z++)
+                    for (int y = lo[1]; y <= hi[1]; y++)
+                        for (int x = lo[0]; x <= hi[0]; x++)
+                            m = std::max(m, dens[(size_t(z) * res[1] + y) * res[0] + x]);
+                out[(size_t(cz) * mres + cy) * mres + cx] = m;
+            }
+}
+
 rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
     const int64_t nt = int64_t(s.tri_mesh.size());
     rth::BuiltBvh bvh;
@@ -94,6 +115,12 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
         float mx = 0.0f;
         for (float v : d) mx = std::max(mx, v);
         media[i].max_density = mx;
+        std::vector<float> maj;
+        grid_majorants(d.data(), s.media[i].grid_res, media[i].majorant_res, maj);
+        DevBuf* mb = new DevBuf();
+        ds.grids.push_back(mb);
+        RT_CUDA(mb->upload(maj.data(), maj.size() * sizeof(float), st), "upload majorant grid");
+        media[i].majorant = mb->as<float>();
     }
     RT_CUDA(ds.media.upload(media.data(), media.size() * sizeof(DevMedium), st), "upload media");
     SceneView& v = ds.view;
@@ -153,6 +180,11 @@ struct rt_renderer {
     DevBuf acc_color, acc_albedo, acc_normal, lcg_state, color, albedo, normal, rgba8;
     int capacity = 0;
     DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, ctl, segs, job;
+    DevBuf wave_index;
+    // one captured wave (raygen, (extend, shade, shadow) x depth, resolve, advance)
+    cudaGraphExec_t graph = nullptr;
+    int graph_capacity = -1, graph_depth = -1;
+    const void* graph_waves = nullptr;
     rth::LaunchShape shape{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     KernelTimer timer;
@@ -263,6 +295,7 @@ rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_rende
 rt_status rt_renderer_destroy(rt_renderer* r) {
     if (!r) return RT_OK;
     if (r->stream) cudaStreamSynchronize(r->stream);
+    if (r->graph) cudaGraphExecDestroy(r->graph);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
     if (r->own_stream && r->stream) cudaStreamDestroy(r->stream);
@@ -361,18 +394,22 @@ rt_status rt_renderer_render(rt_renderer* r) {
     cudaStream_t s = r->stream;
     RT_CUDA(cudaMemcpyAsync(r->job.ptr, &hj, sizeof(hj), cudaMemcpyHostToDevice, s), "upload launch parameters");
     const int64_t nwaves = (total + cap - 1) / cap;
-    std::vector<Segment> segs(static_cast<size_t>(nwaves));
+    std::vector<WaveParams> waves(static_cast<size_t>(nwaves));
     for (int64_t w = 0; w < nwaves; w++) {
-        Segment& g = segs[size_t(w)];
-        g.job = 0;
-        g.slot_begin = 0;
-        g.path_begin = w * cap;
-        g.count = int(std::min<int64_t>(cap, total - w * cap));
-        g.pad = 0;
+        WaveParams& wp = waves[size_t(w)];
+        std::memset(&wp, 0, sizeof(wp));
+        wp.num_seg = 1;
+        wp.wave_count = int(std::min<int64_t>(cap, total - w * cap));
+        wp.seg[0].job = 0;
+        wp.seg[0].slot_begin = 0;
+        wp.seg[0].count = wp.wave_count;
+        wp.seg[0].path_begin = w * cap;
     }
-    RT_CUDA(r->segs.alloc(segs.size() * sizeof(Segment)), "allocate wave table");
-    RT_CUDA(cudaMemcpyAsync(r->segs.ptr, segs.data(), segs.size() * sizeof(Segment), cudaMemcpyHostToDevice, s),
+    RT_CUDA(r->segs.alloc(waves.size() * sizeof(WaveParams)), "allocate wave table");
+    RT_CUDA(cudaMemcpyAsync(r->segs.ptr, waves.data(), waves.size() * sizeof(WaveParams), cudaMemcpyHostToDevice, s),
             "upload wave table");
+    if (!r->wave_index.ptr) RT_CUDA(r->wave_index.alloc(sizeof(int)), "allocate wave counter");
+    RT_CUDA(cudaMemsetAsync(r->wave_index.ptr, 0, sizeof(int), s), "clear wave counter");
     RT_CUDA(cudaMemsetAsync(r->ctl.ptr, 0, sizeof(WaveCtl), s), "clear counters");
     const bool stats = o.collect_stats != 0;
     r->timer.reset();
@@ -401,47 +438,55 @@ rt_status rt_renderer_render(rt_renderer* r) {
     b.sh_o = r->sh_o.as<float4>();
     b.sh_d = r->sh_d.as<float4>();
     b.ctl = r->ctl.as<WaveCtl>();
-    b.capacity = cap;
-    c.num_seg = 1;
+    b.capacity = r->capacity;
+    c.waves = r->segs.as<WaveParams>();
+    c.wave_index = r->wave_index.as<int>();
     c.max_depth = o.max_depth;
-    for (int64_t w = 0; w < nwaves; w++) {
-        c.seg = r->segs.as<Segment>() + w;
-        c.wave_count = segs[size_t(w)].count;
+    auto issue_wave = [&](bool timed) {
         c.bounce = 0;
         rth::launch_raygen(c, s);
-        launches++;
         for (int bnc = 0; bnc < o.max_depth; bnc++) {
             c.bounce = bnc;
-            cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
-            if (stats) {
-                e0 = r->timer.next();
-                cudaEventRecord(e0, s);
-            }
-            rth::launch_extend(c, r->shape, stats, s);
-            if (stats) {
-                e1 = r->timer.next();
-                cudaEventRecord(e1, s);
-            }
-            rth::launch_shade(c, r->shape, stats, s);
-            if (stats) {
-                e2 = r->timer.next();
-                cudaEventRecord(e2, s);
-            }
-            rth::launch_shadow(c, r->shape, stats, s);
-            if (stats) {
-                e3 = r->timer.next();
-                cudaEventRecord(e3, s);
-                size_t i0 = r->timer.used - 4;
+            size_t i0 = r->timer.used;
+            if (timed) cudaEventRecord(r->timer.next(), s);
+            rth::launch_extend(c, r->shape, timed, s);
+            if (timed) cudaEventRecord(r->timer.next(), s);
+            rth::launch_shade(c, r->shape, timed, s);
+            if (timed) cudaEventRecord(r->timer.next(), s);
+            rth::launch_shadow(c, r->shape, timed, s);
+            if (timed) {
+                cudaEventRecord(r->timer.next(), s);
                 r->timer.marks.push_back({0, i0});
                 r->timer.marks.push_back({1, i0 + 1});
                 r->timer.marks.push_back({2, i0 + 2});
             }
-            launches += 3;
-            ext++;
         }
         rth::launch_resolve(c, s);
-        launches++;
+        rth::launch_next_wave(c, s);
+    };
+    // graph capture is not possible on the legacy default stream
+    if (stats || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+        for (int64_t w = 0; w < nwaves; w++) issue_wave(stats);
+    } else {
+        if (!r->graph || r->graph_capacity != r->capacity || r->graph_depth != o.max_depth ||
+            r->graph_waves != r->segs.ptr) {
+            if (r->graph) cudaGraphExecDestroy(r->graph);
+            r->graph = nullptr;
+            cudaGraph_t g = nullptr;
+            RT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+            issue_wave(false);
+            RT_CUDA(cudaStreamEndCapture(s, &g), "end graph capture");
+            cudaError_t e = cudaGraphInstantiate(&r->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(e, "instantiate wave graph");
+            r->graph_capacity = r->capacity;
+            r->graph_depth = o.max_depth;
+            r->graph_waves = r->segs.ptr;
+        }
+        for (int64_t w = 0; w < nwaves; w++) RT_CUDA(cudaGraphLaunch(r->graph, s), "launch wave graph");
     }
+    launches += int(nwaves) * (3 * o.max_depth + 3);
+    ext = int(nwaves) * o.max_depth;
     rth::launch_finalize(hj, dj, s);
     launches++;
     RT_CUDA(cudaEventRecord(r->ev1, s), "record event");

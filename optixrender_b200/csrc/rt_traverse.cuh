@@ -51,7 +51,9 @@ RT_D void prepare_ray(TravRay& r) {
 RT_D float comp(v3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 
 // Watertight ray/triangle test.  Products are rounded individually (no FMA
-// contraction) so the edge functions match a plain FP32 evaluation.
+// contraction) so the edge functions match a plain FP32 evaluation.  The
+// distance range is tested on the unnormalised T against tmin/tmax * |det|;
+// the one division happens only for an accepted hit.
 RT_D bool intersect_tri(const TravRay& r, float4 a, float4 b, float4 c, float tmax, float& t, float& b1, float& b2) {
     v3 A = v3(a.x, a.y, a.z) - r.o, B = v3(b.x, b.y, b.z) - r.o, C = v3(c.x, c.y, c.z) - r.o;
     float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
@@ -66,6 +68,9 @@ RT_D bool intersect_tri(const TravRay& r, float4 a, float4 b, float4 c, float tm
     if (det == 0.0f) return false;
     float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
     float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+    const float adet = fabsf(det);
+    const float sT = det < 0.0f ? -T : T;
+    if (!(sT > 0.99999f * r.tmin * adet && sT < 1.00001f * tmax * adet)) return false;
     float inv = __fdiv_rn(1.0f, det);
     float tt = __fmul_rn(T, inv);
     if (!(tt > r.tmin && tt < tmax)) return false;
@@ -75,7 +80,12 @@ RT_D bool intersect_tri(const TravRay& r, float4 a, float4 b, float4 c, float tm
     return true;
 }
 
-RT_D float u8f(uint32_t w, int byte) { return float((w >> (8 * byte)) & 0xFFu); }
+// Byte `byte` of w as a float, without an int-to-float conversion: the byte is
+// placed in the mantissa of 2^23 by a byte permute and 2^23 subtracted (exact).
+RT_D float u8f(uint32_t w, int byte) {
+    const uint32_t sel = uint32_t(byte) | (4u << 4) | (5u << 8) | (7u << 12);
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, sel)) - 8388608.0f;
+}
 
 // Tests the eight children of `node`; returns the hit mask of internal
 // children (bits 24..31, near-to-far) with the node's imask in bits 0..7,
@@ -178,6 +188,111 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
         }
     }
     return hit_tri;
+}
+
+// ------------------------------------------------------------------ persistent traversal
+// Lane-refill ("while-while with dynamic fetch", Aila and Laine, HPG 2009):
+// every lane traverses its own ray one wide node at a time; when enough lanes
+// of a warp have finished, they take new rays from the queue with a single
+// warp-aggregated atomicAdd, so a warp never waits for its slowest ray while
+// work remains.  `src.load(i, ray, scene)` fetches queue entry i and
+// `src.finish(i, tri, t, b1, b2)` stores its result.
+constexpr int kRefillLanes = 12;
+
+struct TravState {
+    TravRay r;
+    const CwNode* nodes;
+    const float4* tri_v;
+    uint2 g;
+    float tmax;
+    float t, b1, b2;
+    int hit;
+    int sp;
+};
+
+// One wide node and its triangles; returns true when the ray is finished.
+template <bool AnyHit, bool Stats>
+RT_D bool trav_step(TravState& s, uint2* stack, uint32_t& nodes_visited, uint32_t& tris_tested) {
+    uint32_t bit = __ffs(s.g.y >> 24) - 1u;
+    s.g.y &= ~(1u << (24 + bit));
+    uint32_t slot = bit ^ s.r.oct;
+    uint32_t idx = s.g.x + __popc((s.g.y & 0xFFu) & ((1u << slot) - 1u));
+    if ((s.g.y & 0xFF000000u) && s.sp < kStackSize) stack[s.sp++] = s.g;
+    uint32_t cb, tb, tbits;
+    uint32_t nb = intersect_children(s.nodes, idx, s.r, s.tmax, cb, tb, tbits);
+    if (Stats) nodes_visited++;
+    s.g = make_uint2(cb, nb);
+    while (tbits) {
+        uint32_t b = __ffs(tbits) - 1u;
+        tbits &= ~(1u << b);
+        uint32_t ti = tb + b;
+        const float4* tv = s.tri_v + size_t(ti) * 3;
+        float4 a = __ldg(tv), bb = __ldg(tv + 1), c = __ldg(tv + 2);
+        if (Stats) tris_tested++;
+        float t, u, v;
+        if (intersect_tri(s.r, a, bb, c, s.tmax, t, u, v)) {
+            s.hit = int(ti);
+            s.tmax = t;
+            s.t = t;
+            s.b1 = u;
+            s.b2 = v;
+            if (AnyHit) return true;
+        }
+    }
+    while (!(s.g.y & 0xFF000000u)) {
+        if (s.sp == 0) return true;
+        s.g = stack[--s.sp];
+    }
+    return false;
+}
+
+template <bool AnyHit, bool Stats, class Src>
+RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& nodes_visited, uint32_t& tris_tested,
+                         uint32_t& rays) {
+    const int lane = threadIdx.x & 31;
+    uint2 stack[kStackSize];
+    TravState s;
+    int item = -1;
+    bool active = false, exhausted = false;
+    while (true) {
+        unsigned idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && idle && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            int leader = __ffs(idle) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(fetch_counter, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= total) exhausted = true;
+            if (!active) {
+                int my = base + __popc(idle & ((1u << lane) - 1u));
+                if (my < total) {
+                    item = my;
+                    const SceneView* sc = nullptr;
+                    src.load(item, s.r, sc);
+                    prepare_ray(s.r);
+                    s.nodes = sc->nodes;
+                    s.tri_v = sc->tri_v;
+                    s.tmax = s.r.tmax;
+                    s.hit = -1;
+                    s.sp = 0;
+                    s.g = make_uint2(0u, 1u << (24 + s.r.oct));
+                    rays++;
+                    if (sc->num_nodes > 0) {
+                        active = true;
+                    } else {
+                        src.finish(item, -1, 0.0f, 0.0f, 0.0f);
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        if (active && trav_step<AnyHit, Stats>(s, stack, nodes_visited, tris_tested)) {
+            src.finish(item, s.hit, s.t, s.b1, s.b2);
+            active = false;
+        }
+    }
 }
 
 }  // namespace rtd

@@ -254,6 +254,52 @@ def spheres(width=1920, height=1080, spp=64, seed=1, ico_level=8, sphere_tris=Tr
     return SceneSpec("spheres", meshes, [], [], env, cam, settings)
 
 
+def density_grid(res=128, seed=1, sigma_max=5.0):
+    """A res^3 fBm density in [0, sigma_max] shaped to a ball (x fastest)."""
+    ax = (np.arange(res) + 0.5) / res * 2.0 - 1.0
+    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    p = np.stack([x, y, z], -1)
+    n = fbm(p * 1.3, seed + 17, octaves=5)
+    r = np.sqrt(x * x + y * y + z * z)
+    ball = np.clip((1.0 - r) / 0.15, 0.0, 1.0)
+    d = np.clip(0.5 + 1.2 * n, 0.0, 1.0) * ball
+    return (d * sigma_max).astype(np.float32)
+
+
+def media(width=1280, height=720, spp=256, seed=1, grid_res=128, env_size=(2048, 1024)):
+    """A 128^3 fBm grid medium (sigma_t 0-5, albedo 0.9, HG g=0.6) inside an
+    IOR-1.33 dielectric sphere; a homogeneous fog box (sigma_t 0.05, albedo
+    0.9) bounded by an index-matched thin dielectric; a diffuse floor and a
+    quad light inside the fog; the sky outside."""
+    FOG, GRID = 0, 1
+    meshes = []
+    sv, sf = uv_sphere(61, 60)
+    meshes.append(MeshSpec(sv.astype(np.float32), sf.astype(np.int32),
+                           dict(type=MAT_DIELECTRIC, albedo=(1, 1, 1), roughness=0.05, int_ior=1.33, ext_ior=1.0),
+                           out_medium=FOG, in_medium=GRID))
+    lo, hi = (-3.0, -1.2, -3.0), (3.0, 2.6, 3.0)
+    v, f = box(lo, hi)
+    boundary = dict(type=5, albedo=(1, 1, 1), roughness=0.01, int_ior=1.0, ext_ior=1.0)  # thin dielectric, IOR 1
+    keep = np.array([i for i in range(12) if i not in (4, 5)])  # faces 4,5 are the y = lo floor
+    meshes.append(MeshSpec(v, f[keep], boundary, out_medium=-1, in_medium=FOG))
+    fv, ff = quad((lo[0], lo[1], lo[2]), (hi[0] - lo[0], 0, 0), (0, 0, hi[2] - lo[2]))
+    meshes.append(MeshSpec(fv, ff, dict(type=MAT_DIFFUSE, albedo=(0.6, 0.6, 0.6), roughness=0.0),
+                           out_medium=FOG, in_medium=FOG))
+    lights = [dict(type=LIGHT_QUAD, position=(-0.75, 2.4, -0.75), u=(0.0, 0.0, 1.5), v=(1.5, 0.0, 0.0),
+                   radiance=(12.0, 11.0, 9.0), double_side=0, medium=FOG)]
+    dens = density_grid(grid_res, seed)
+    med = [dict(type=MEDIUM_HOMOGENEOUS, phase=PHASE_ISOTROPIC, sigma_s=(0.045, 0.045, 0.045),
+                sigma_a=(0.005, 0.005, 0.005), scale=1.0),
+           dict(type=MEDIUM_GRID, density=dens, phase=PHASE_HG, g=(0.6, 0.6, 0.6), sigma_s=(0.9, 0.9, 0.9),
+                sigma_a=(0.1, 0.1, 0.1), scale=1.0, bounds_min=(-1, -1, -1), bounds_max=(1, 1, 1),
+                majorant_res=8)]
+    env = sky(*env_size)
+    cam = dict(from_=(0.0, 0.6, -7.5), at=(0.0, 0.2, 0.0), up=(0, 1, 0), medium=-1)
+    settings = dict(width=width, height=height, spp=spp, max_depth=32, rr_depth=0, rng=RNG_PCG32, seed=seed,
+                    filter=FILTER_GAUSSIAN)
+    return SceneSpec("media", meshes, lights, med, env, cam, settings)
+
+
 def _material_obj(d):
     return material(**d)
 
@@ -282,4 +328,4 @@ def build_renderer(spec: SceneSpec, **overrides) -> tuple:
     return s, r
 
 
-SCENES = {"cornell": cornell, "spheres": spheres}
+SCENES = {"cornell": cornell, "spheres": spheres, "media": media}

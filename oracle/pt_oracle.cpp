@@ -27,6 +27,7 @@ struct Scene {
     std::vector<int> mesh_in, mesh_out;
     std::vector<Lt<R>> lights;
     std::vector<Med<R>> media;
+    std::vector<Grid<R>> grids;
     const float* env = nullptr;
     const float* cache = nullptr;
     int env_w = 0, env_h = 0;
@@ -43,6 +44,7 @@ struct SceneHandle {
     std::vector<int32_t> mesh_media;
     std::vector<rt_light> lights;
     std::vector<rt_medium> media;
+    std::vector<std::vector<float>> dens, maj;
     std::vector<float> env, cache;
     int env_w = 0, env_h = 0;
     Bvh2 bvh;
@@ -65,7 +67,25 @@ Scene<R>* make_scene(SceneHandle* h) {
     s->lights.resize(h->lights.size());
     for (size_t i = 0; i < h->lights.size(); i++) s->lights[i].set(h->lights[i]);
     s->media.resize(h->media.size());
-    for (size_t i = 0; i < h->media.size(); i++) s->media[i].set(h->media[i]);
+    s->grids.resize(h->media.size());
+    for (size_t i = 0; i < h->media.size(); i++) {
+        const rt_medium& m = h->media[i];
+        s->media[i].set(m);
+        if (m.type != RT_MEDIUM_GRID) continue;
+        Grid<R>& g = s->grids[i];
+        g.bmin = from3<R>(m.bounds_min);
+        g.bmax = from3<R>(m.bounds_max);
+        for (int a = 0; a < 3; a++) g.res[a] = m.grid_res[a];
+        g.mres = m.majorant_res > 0 ? m.majorant_res : 8;
+        R mx = R(0);
+        for (int c = 0; c < 3; c++) mx = dmax(mx, R(m.sigma_a[c]) + R(m.sigma_s[c]));
+        g.sigma_t = mx * R(m.scale);
+        V3<R> ss = from3<R>(m.sigma_s), st = from3<R>(m.sigma_a) + ss;
+        for (int c = 0; c < 3; c++) g.albedo[c] = st[c] > R(0) ? ss[c] / st[c] : R(0);
+        g.density = h->dens[i].data();
+        g.majorant = h->maj[i].data();
+        s->media[i].grid = &s->grids[i];
+    }
     s->env_w = h->env_w;
     s->env_h = h->env_h;
     s->tv = h->tv.data();
@@ -107,6 +127,23 @@ bool light_trace(const Scene<R>& sc, const V3<R>& o, const V3<R>& d, int* mi_in,
 }
 
 inline bool nee_pdf_ok(double p) { return p > 0.0 && std::isfinite(p); }
+
+template <class R>
+bool medium_sample(const Med<R>& m, const V3<R>& o, const V3<R>& d, R maxd, R& dist, R& tp, V3<R>& tr, Rng& rng) {
+    if (m.type == RT_MEDIUM_GRID) {
+        tp = R(1);
+        return grid_sample_distance(*m.grid, o, d, maxd, rng, dist, tr);
+    }
+    return sample_medium_distance(m, maxd, dist, tp, tr, rng);
+}
+template <class R>
+V3<R> medium_transmittance(const Med<R>& m, const V3<R>& o, const V3<R>& d, R dist, R& tp, Rng& rng) {
+    if (m.type == RT_MEDIUM_GRID) {
+        tp = R(1);
+        return V3<R>(grid_transmittance(*m.grid, o, d, dist, rng));
+    }
+    return eval_medium_distance(m, false, dist, tp);
+}
 
 template <class R>
 void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Cam<R>& cam, const rt_options& opt,
@@ -181,7 +218,7 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
             R distance = R(0);
             if (medium_index != -1) {
                 const Med<R>& med = sc.media[size_t(medium_index)];
-                scattered = sample_medium_distance(med, closest, distance, trans_pdf, transmittance, rng);
+                scattered = medium_sample(med, o, d, closest, distance, trans_pdf, transmittance, rng);
                 history *= (transmittance / trans_pdf);
                 mult_trans_pdf *= trans_pdf;
                 if (scattered) {
@@ -199,12 +236,13 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
                         closest = ld - EPS;
                         V3<R> tvv;
                         R tpdf;
-                        if (!light_trace(sc, so, sd, nullptr, nullptr, tvv, tpdf, closest) && !occ &&
+                        if (!light_trace(sc, so, sd, nullptr, nullptr, tvv, tpdf, closest) &&
                             nee_pdf_ok(double(light_pdf))) {
-                            transmittance = eval_medium_distance(med, false, closest, trans_pdf);
+                            transmittance = medium_transmittance(med, so, sd, closest, trans_pdf, rng);
                             attenuation = evaluate_phase(med, V, sd, phase_pdf);
                             R w = (l.type == RT_LIGHT_POINT) ? R(1) : power_heuristic(light_pdf, phase_pdf * trans_pdf);
-                            radiance += w * (transmittance / trans_pdf) * light_radiance * attenuation * history / light_pdf;
+                            if (!occ)
+                                radiance += w * (transmittance / trans_pdf) * light_radiance * attenuation * history / light_pdf;
                         }
                     }
                     attenuation = sample_phase(med, rng, V, L, phase_pdf);
@@ -261,18 +299,18 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
                 closest = FMAX;
                 V3<R> tvv;
                 R tpdf;
-                if (!light_trace(sc, so, sd, nullptr, nullptr, tvv, tpdf, closest) && !occ && nee_pdf_ok(double(light_pdf))) {
+                if (!light_trace(sc, so, sd, nullptr, nullptr, tvv, tpdf, closest) && nee_pdf_ok(double(light_pdf))) {
                     bsdf = eval_material(it, lut, V, sd, bsdf_pdf);
                     R ct = std::fabs(dot(it.sn, sd));
                     R w = power_heuristic(light_pdf, bsdf_pdf);
                     V3<R> th(R(1));
                     if (medium_index != -1) {
                         const Med<R>& med = sc.media[size_t(medium_index)];
-                        transmittance = eval_medium_distance(med, false, closest, trans_pdf);
+                        transmittance = medium_transmittance(med, so, sd, closest, trans_pdf, rng);
                         th = transmittance / trans_pdf;
                         w = power_heuristic(light_pdf, bsdf_pdf * trans_pdf);
                     }
-                    radiance += w * th * light_radiance * bsdf * ct * history / light_pdf;
+                    if (!occ) radiance += w * th * light_radiance * bsdf * ct * history / light_pdf;
                 }
             }
             if (nl != 0) {  // light NEE, devicePrograms.cu:426-471
@@ -287,18 +325,18 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
                 closest = ld - EPS;
                 V3<R> tvv;
                 R tpdf;
-                if (!light_trace(sc, so, sd, nullptr, nullptr, tvv, tpdf, closest) && !occ && nee_pdf_ok(double(light_pdf))) {
+                if (!light_trace(sc, so, sd, nullptr, nullptr, tvv, tpdf, closest) && nee_pdf_ok(double(light_pdf))) {
                     bsdf = eval_material(it, lut, V, sd, bsdf_pdf);
                     R ct = std::fabs(dot(it.sn, sd));
                     R w = (l.type == RT_LIGHT_POINT) ? R(1) : power_heuristic(light_pdf, bsdf_pdf);
                     V3<R> th(R(1));
                     if (medium_index != -1) {
                         const Med<R>& med = sc.media[size_t(medium_index)];
-                        transmittance = eval_medium_distance(med, false, closest, trans_pdf);
+                        transmittance = medium_transmittance(med, so, sd, closest, trans_pdf, rng);
                         th = transmittance / trans_pdf;
                         if (l.type != RT_LIGHT_POINT) w = power_heuristic(light_pdf, bsdf_pdf * trans_pdf);
                     }
-                    radiance += w * th * light_radiance * bsdf * ct * history / light_pdf;
+                    if (!occ) radiance += w * th * light_radiance * bsdf * ct * history / light_pdf;
                 }
             }
             // BSDF sampling, devicePrograms.cu:474-477
@@ -575,6 +613,16 @@ void* orc_scene_new(const float* tri_v, const float* tri_n, const float* tri_uv,
     h->mesh_media.assign(mesh_media, mesh_media + 2 * n_mesh);
     if (nl > 0) h->lights.assign(lights, lights + nl);
     if (nm > 0) h->media.assign(media, media + nm);
+    h->dens.resize(size_t(std::max(nm, 0)));
+    h->maj.resize(size_t(std::max(nm, 0)));
+    for (int i = 0; i < nm; i++) {
+        if (media[i].type != RT_MEDIUM_GRID || !media[i].density) continue;
+        size_t n = size_t(media[i].grid_res[0]) * media[i].grid_res[1] * media[i].grid_res[2];
+        h->dens[size_t(i)].assign(media[i].density, media[i].density + n);
+        int mres = media[i].majorant_res > 0 ? media[i].majorant_res : 8;
+        grid_majorants(h->dens[size_t(i)].data(), media[i].grid_res, mres, h->maj[size_t(i)]);
+        h->media[size_t(i)].density = nullptr;
+    }
     if (env_rgba && env_w > 0 && env_h > 0) {
         h->env.assign(env_rgba, env_rgba + size_t(env_w) * env_h * 4);
         h->cache.resize(h->env.size());
