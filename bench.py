@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import os
 import subprocess
 import sys
@@ -47,6 +48,7 @@ def parse():
     p.add_argument("--spp", type=int, default=WORKLOAD["spp"])
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library's choice)")
     return p.parse_args()
 
 
@@ -209,7 +211,7 @@ def main():
     from optixrender_b200 import scenes
     torch.cuda.set_device(local)
     spec = scenes.spheres(spp=args.spp, seed=1 + rank)
-    s, r = scenes.build_renderer(spec, collect_stats=0)
+    s, r = scenes.build_renderer(spec, collect_stats=0, wave_paths=args.wave_paths)
     stream = torch.cuda.Stream()
     r.set_stream(stream.cuda_stream)
     W, H = spec.settings["width"], spec.settings["height"]
@@ -229,7 +231,8 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    launches_per_step = r.stats()["launches"]
+    st0 = r.stats()
+    launches_per_step, wave_paths = st0["launches"], st0["wave_paths"]
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -291,19 +294,23 @@ def main():
                  counters["extend_rays"] * RAY_BYTES)
     ext_ms = kern["extend"]
     achieved = ext_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
+    # DRAM bytes per k_extend launch from the committed ncu summary of one wave
+    # of this workload (dram__bytes_read.sum + dram__bytes_write.sum)
+    # (used when the summary's wave size is the one this run used)
     traffic = None
-    prof = ROOT / "profiles" / "extend_traffic.json"
-    if prof.exists():
-        try:
-            traffic = json.loads(prof.read_text()).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    for prof in sorted((ROOT / "profiles").glob("k_extend*dram_traffic*.md")):
+        txt = prof.read_text()
+        m = re.search(r"k_extend bytes_per_launch: (\d+)", txt)
+        w = re.search(r"wave_paths: (\d+)", txt)
+        if m and w and int(w.group(1)) == wave_paths:
+            traffic = int(m.group(1))
     line = {
         "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "spheres-1080p", **dict(WORKLOAD, spp=args.spp), "triangles": spec.num_triangles,
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (scene + BVH ~0.3 GB)"},
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (scene + BVH ~0.3 GB)",
+                   "wave_paths": wave_paths},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": W * H * 4},
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,

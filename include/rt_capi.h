@@ -172,7 +172,8 @@ typedef struct rt_options {
     int32_t progressive;      /* running mean over Render() calls */
     uint64_t seed;            /* PCG32 seed (ignored by RT_RNG_LCG) */
     int32_t tonemap;          /* RT_TONEMAP_* */
-    int32_t wave_paths;       /* paths in flight per wave (0 = automatic) */
+    int32_t wave_paths;       /* paths in flight per wave (0 = automatic: up to 2^26, at most a quarter of
+                                 free device memory; at most 2^26) */
     int32_t collect_stats;    /* count rays, nodes and triangles */
     float exposure;           /* multiplier before tonemapping (1) */
 } rt_options;
@@ -196,6 +197,7 @@ typedef struct rt_render_stats {
     float ms_other;
     int64_t extend_launches;
     int64_t nan_throughput_paths; /* paths ended by IsNan(history), devicePrograms.cu:487-489 */
+    int64_t wave_paths;        /* path slots per wave of the last Render() */
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */
@@ -238,6 +240,19 @@ RT_API rt_status rt_scene_add_mesh_obj(rt_scene* s, const char* obj_path, const 
 RT_API rt_status rt_scene_add_light(rt_scene* s, const rt_light* light);
 /* Scene::AddMedium, core/src/Scene.cpp:75-77 (grid media copy `density`). */
 RT_API rt_status rt_scene_add_medium(rt_scene* s, const rt_medium* medium);
+/* Scene::AddTexture, core/src/Scene.cpp:66-69 + Texture, Scene.cpp:181-189:
+ * an RGBA8 image (w*h*4 bytes, row 0 = bottom, i.e. v = 0, as stbi's
+ * vertical flip gives).  Materials refer to it by the returned id in
+ * rt_material.texture_ids; it is sampled as the reference's tex2D (normalized
+ * coordinates, wrap, bilinear, texels read as byte/255). */
+RT_API rt_status rt_scene_add_texture(rt_scene* s, const uint8_t* rgba, int32_t width, int32_t height,
+                                      int32_t* texture_id);
+/* Scene::AddTexture(fileName): uncompressed BMP (8/24/32-bit) or binary
+ * PGM/PPM (P5/P6), flipped so that row 0 is the bottom. */
+RT_API rt_status rt_scene_add_texture_file(rt_scene* s, const char* path, int32_t* texture_id);
+/* Size of texture `texture_id` and, when `rgba` is not NULL, its texels as stored. */
+RT_API rt_status rt_scene_get_texture(const rt_scene* s, int32_t texture_id, int32_t* width, int32_t* height,
+                                      uint8_t* rgba);
 /* Scene::AddEnv, core/src/Scene.cpp:79-81 + HdrTexture, Scene.cpp:197-313:
  * an equirectangular RGBA float image (w*h*4 floats, row 0 = bottom) scaled
  * by `scale`; the sampling cache is built as in CalculateHdrCache. */
@@ -301,6 +316,79 @@ RT_API rt_status rt_renderer_frame_index(const rt_renderer* r, int32_t* frame);
  * `device_ptrs` nonzero means both buffers are device memory. */
 RT_API rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
                                    int32_t device_ptrs);
+
+/* ---------------------------------------------------------------------- */
+/* Serving: many render jobs batched into shared wavefront launches         */
+/* (no counterpart in the reference, which renders one frame at a time).    */
+/* ---------------------------------------------------------------------- */
+
+typedef struct rt_server rt_server;
+
+typedef struct rt_server_options {
+    int64_t hbm_budget_bytes;  /* device memory for resident scenes + admitted jobs (0 = 80% of free) */
+    int32_t wave_paths;        /* paths per shared wave (0 = 2^23) */
+    int32_t max_jobs;          /* jobs resident at once (<= 256; 0 = 64) */
+    int32_t max_depth;         /* bounce budget of the shared launches (>= every job's max_depth; 0 = 32) */
+    int32_t background;        /* nonzero: a server thread runs the loop; zero: call rt_server_step */
+    int32_t waves_in_flight;   /* waves queued ahead on the device (0 = 2) */
+    int32_t policy;            /* RT_SERVE_FAIR (default) or RT_SERVE_FIFO */
+} rt_server_options;
+
+/* How a wave's path slots are split among admitted jobs.  FAIR: up to 16 jobs,
+ * taken round-robin, share each wave evenly (small jobs finish early, latency
+ * grows with job size).  FIFO: the oldest job takes all it can. */
+enum { RT_SERVE_FAIR = 0, RT_SERVE_FIFO = 1 };
+
+/* One request: a resident scene, a camera and the renderer settings of one
+ * Render() (PCG32 streams seeded by `seed`). */
+typedef struct rt_job_desc {
+    int32_t scene;
+    rt_camera camera;
+    int32_t width, height, spp, max_depth, rr_depth, filter, tonemap;
+    uint64_t seed;
+    float exposure;
+    int32_t guided;            /* reserved for the learned proposal; 0 = plain */
+} rt_job_desc;
+
+enum { RT_JOB_QUEUED = 0, RT_JOB_RUNNING = 1, RT_JOB_DONE = 2, RT_JOB_FAILED = 3, RT_JOB_CANCELLED = 4 };
+
+typedef struct rt_job_status {
+    int32_t state;
+    int32_t pad;
+    double submit_ms;          /* host clock (ms since server creation) */
+    double admit_ms;
+    double done_ms;            /* time the finished image was observed ready */
+    int64_t paths;
+    int64_t bytes;             /* device bytes held while admitted */
+} rt_job_status;
+
+typedef struct rt_server_stats {
+    int64_t jobs_submitted, jobs_done, jobs_queued, jobs_running;
+    int64_t waves, paths;
+    int64_t bytes_in_use, bytes_budget;
+    int32_t max_segments_in_a_wave;
+    int32_t pad;
+} rt_server_stats;
+
+RT_API void rt_server_options_default(rt_server_options* o);
+RT_API rt_status rt_server_create(const rt_server_options* o, rt_server** out);
+RT_API rt_status rt_server_destroy(rt_server* s);
+/* Uploads a scene (BVH, triangles, materials, media, environment) and keeps it resident. */
+RT_API rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* scene_id);
+RT_API rt_status rt_server_submit(rt_server* s, const rt_job_desc* job, int64_t* job_id);
+RT_API rt_status rt_server_cancel(rt_server* s, int64_t job_id);
+RT_API rt_status rt_server_poll(rt_server* s, int64_t job_id, rt_job_status* st);
+/* Waits until the job is done (or timeout_ms passes; < 0 = forever); RT_ERR_TIMEOUT on expiry. */
+RT_API rt_status rt_server_wait(rt_server* s, int64_t job_id, double timeout_ms, rt_job_status* st);
+/* Float RGBA image of a finished job (width*height*4). */
+RT_API rt_status rt_server_download(rt_server* s, int64_t job_id, float* rgba);
+/* Tonemapped RGBA8 image of a finished job (width*height words). */
+RT_API rt_status rt_server_download_rgba8(rt_server* s, int64_t job_id, uint32_t* pixels);
+/* Frees a finished (or queued) job and forgets its id. */
+RT_API rt_status rt_server_release(rt_server* s, int64_t job_id);
+/* Manual mode: admits, issues one wave and retires finished jobs; *did_work = 0 when idle. */
+RT_API rt_status rt_server_step(rt_server* s, int32_t* did_work);
+RT_API rt_status rt_server_get_stats(rt_server* s, rt_server_stats* st);
 
 /* ---------------------------------------------------------------------- */
 /* Shading verification: runs the renderer's device shading code on         */

@@ -21,6 +21,8 @@ LIBRARY_PATH = _PKG / "_lib" / "liboptixrender_b200.so"
 
 # ---------------------------------------------------------------- constants
 RT_OK = 0
+(RT_ERR_INVALID_ARG, RT_ERR_CUDA, RT_ERR_OUT_OF_MEMORY, RT_ERR_IO, RT_ERR_PARSE, RT_ERR_STATE, RT_ERR_TIMEOUT,
+ RT_ERR_UNSUPPORTED, RT_ERR_DEVICE_WATCHDOG) = range(1, 10)
 MAT_DIFFUSE, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_PLASTIC = 0, 1, 2, 3
 MAT_METAL_WORKFLOW, MAT_THIN_DIELECTRIC, MAT_CLEARCOATED_CONDUCTOR, MAT_DIFFUSE_TRANSMITTER = 4, 5, 6, 7
 LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT = 0, 1, 2
@@ -82,10 +84,44 @@ class RenderStats(C.Structure):
                 ("extend_tris", C.c_int64), ("nan_samples", C.c_int64), ("waves", C.c_int32),
                 ("launches", C.c_int32), ("ms_total", C.c_float), ("ms_extend", C.c_float),
                 ("ms_shade", C.c_float), ("ms_shadow", C.c_float), ("ms_other", C.c_float),
-                ("extend_launches", C.c_int64), ("nan_throughput_paths", C.c_int64)]
+                ("extend_launches", C.c_int64), ("nan_throughput_paths", C.c_int64), ("wave_paths", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("wave_paths", C.c_int32), ("max_jobs", C.c_int32),
+                ("max_depth", C.c_int32), ("background", C.c_int32), ("waves_in_flight", C.c_int32),
+                ("policy", C.c_int32)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("camera", Camera), ("width", C.c_int32), ("height", C.c_int32),
+                ("spp", C.c_int32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32), ("filter", C.c_int32),
+                ("tonemap", C.c_int32), ("seed", C.c_uint64), ("exposure", C.c_float), ("guided", C.c_int32)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
+SERVE_FAIR, SERVE_FIFO = 0, 1
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("pad", C.c_int32), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
+                ("done_ms", C.c_double), ("paths", C.c_int64), ("bytes", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_submitted", C.c_int64), ("jobs_done", C.c_int64), ("jobs_queued", C.c_int64),
+                ("jobs_running", C.c_int64), ("waves", C.c_int64), ("paths", C.c_int64),
+                ("bytes_in_use", C.c_int64), ("bytes_budget", C.c_int64), ("max_segments_in_a_wave", C.c_int32),
+                ("pad", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
 class RTError(RuntimeError):
@@ -121,6 +157,9 @@ def load_library():
         "rt_scene_add_light": (I32, [VP, P(Light)]),
         "rt_scene_add_medium": (I32, [VP, P(Medium)]),
         "rt_scene_set_env": (I32, [VP, P(F), I32, I32, F]),
+        "rt_scene_add_texture": (I32, [VP, P(C.c_uint8), I32, I32, P(I32)]),
+        "rt_scene_add_texture_file": (I32, [VP, C.c_char_p, P(I32)]),
+        "rt_scene_get_texture": (I32, [VP, I32, P(I32), P(I32), P(C.c_uint8)]),
         "rt_scene_get_bounds": (I32, [VP, P(F), P(F)]),
         "rt_scene_counts": (I32, [VP, P(I64), P(I32), P(I32), P(I32)]),
         "rt_scene_load_json": (I32, [VP, C.c_char_p, P(Options), P(Camera)]),
@@ -144,6 +183,19 @@ def load_library():
         "rt_renderer_trace": (I32, [VP, I32, VP, I64, VP, I32]),
         "rt_verify_shading": (I32, [I32, P(Material), I32, P(Light), I32, P(Medium), I32, P(F), I64, P(F)]),
         "rt_kulla_conty_lut": (I32, [P(F), P(F)]),
+        "rt_server_options_default": (None, [P(ServerOptions)]),
+        "rt_server_create": (I32, [P(ServerOptions), P(VP)]),
+        "rt_server_destroy": (I32, [VP]),
+        "rt_server_add_scene": (I32, [VP, VP, P(I32)]),
+        "rt_server_submit": (I32, [VP, P(JobDesc), P(I64)]),
+        "rt_server_cancel": (I32, [VP, I64]),
+        "rt_server_poll": (I32, [VP, I64, P(JobStatus)]),
+        "rt_server_wait": (I32, [VP, I64, C.c_double, P(JobStatus)]),
+        "rt_server_download": (I32, [VP, I64, P(F)]),
+        "rt_server_download_rgba8": (I32, [VP, I64, P(C.c_uint32)]),
+        "rt_server_release": (I32, [VP, I64]),
+        "rt_server_step": (I32, [VP, P(I32)]),
+        "rt_server_get_stats": (I32, [VP, P(ServerStats)]),
         "rt_env_sampling_cache": (I32, [P(F), I32, I32, P(F)]),
     }
     for name, (res, args) in sig.items():
@@ -175,7 +227,11 @@ def material(type=MAT_DIFFUSE, **kw):
     lib.rt_material_default(C.byref(m))
     m.type = type
     for k, v in kw.items():
-        setattr(m, k, _f3(v) if k in ("albedo", "eta", "k", "specular") else v)
+        if k == "texture_ids":
+            ids = list(v) + [-1] * (8 - len(v))
+            m.texture_ids = (C.c_int32 * 8)(*ids)
+        else:
+            setattr(m, k, _f3(v) if k in ("albedo", "eta", "k", "specular") else v)
     return m
 
 
@@ -277,6 +333,28 @@ class Scene:
         mid = C.c_int32()
         _check(self._lib.rt_scene_add_mesh(self._h, C.byref(d), C.byref(mat), out_medium, in_medium, C.byref(mid)))
         return mid.value
+
+    def add_texture(self, rgba):
+        """Scene::AddTexture: (h, w, 4) uint8, row 0 at the bottom (v = 0); returns the texture id."""
+        a = np.ascontiguousarray(rgba, dtype=np.uint8)
+        if a.ndim != 3 or a.shape[2] != 4:
+            raise ValueError("texture must be (h, w, 4) uint8")
+        tid = C.c_int32()
+        _check(self._lib.rt_scene_add_texture(self._h, a.ctypes.data_as(C.POINTER(C.c_uint8)), a.shape[1],
+                                              a.shape[0], C.byref(tid)))
+        return tid.value
+
+    def add_texture_file(self, path):
+        tid = C.c_int32()
+        _check(self._lib.rt_scene_add_texture_file(self._h, str(path).encode(), C.byref(tid)))
+        return tid.value
+
+    def get_texture(self, tid):
+        w, h = C.c_int32(), C.c_int32()
+        _check(self._lib.rt_scene_get_texture(self._h, int(tid), C.byref(w), C.byref(h), None))
+        out = np.empty((h.value, w.value, 4), np.uint8)
+        _check(self._lib.rt_scene_get_texture(self._h, int(tid), None, None, out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out
 
     def add_mesh_obj(self, path, mat, out_medium=-1, in_medium=-1):
         mid = C.c_int32()
@@ -434,6 +512,94 @@ class Renderer:
 
     def trace_device(self, rays_ptr, n, hits_ptr, any_hit=False):
         _check(self._lib.rt_renderer_trace(self._h, 1 if any_hit else 0, rays_ptr, n, hits_ptr, 1))
+
+
+def server_options(**kw):
+    load_library()
+    o = ServerOptions()
+    _lib.rt_server_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def job(scene, cam, width, height, spp, max_depth=25, rr_depth=0, filter=FILTER_GAUSSIAN, tonemap=TONEMAP_REINHARD,
+        seed=1, exposure=1.0):
+    """One render request: the settings of a Renderer::Render() on a resident scene (PCG32 streams)."""
+    return JobDesc(scene=int(scene), camera=cam, width=int(width), height=int(height), spp=int(spp),
+                   max_depth=int(max_depth), rr_depth=int(rr_depth), filter=int(filter), tonemap=int(tonemap),
+                   seed=int(seed), exposure=float(exposure), guided=0)
+
+
+class Server:
+    """Continuous-batching render server: resident scenes, queued jobs packed into shared waves."""
+
+    def __init__(self, opts: ServerOptions | None = None):
+        self._lib = load_library()
+        self._h = C.c_void_p()
+        self._sizes = {}
+        _check(self._lib.rt_server_create(C.byref(opts) if opts is not None else None, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            self._lib.rt_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, scene: Scene) -> int:
+        i = C.c_int32()
+        _check(self._lib.rt_server_add_scene(self._h, scene.handle, C.byref(i)))
+        return i.value
+
+    def submit(self, desc: JobDesc) -> int:
+        i = C.c_int64()
+        _check(self._lib.rt_server_submit(self._h, C.byref(desc), C.byref(i)))
+        self._sizes[i.value] = (desc.height, desc.width)
+        return i.value
+
+    def cancel(self, job_id):
+        _check(self._lib.rt_server_cancel(self._h, int(job_id)))
+
+    def poll(self, job_id) -> dict:
+        st = JobStatus()
+        _check(self._lib.rt_server_poll(self._h, int(job_id), C.byref(st)))
+        return st.as_dict()
+
+    def wait(self, job_id, timeout_ms=-1.0) -> dict:
+        st = JobStatus()
+        _check(self._lib.rt_server_wait(self._h, int(job_id), float(timeout_ms), C.byref(st)))
+        return st.as_dict()
+
+    def download(self, job_id):
+        h, w = self._sizes[job_id]
+        out = np.empty((h, w, 4), dtype=np.float32)
+        _check(self._lib.rt_server_download(self._h, int(job_id), _fptr(out)))
+        return out
+
+    def download_pixels(self, job_id):
+        h, w = self._sizes[job_id]
+        out = np.empty((h, w), dtype=np.uint32)
+        _check(self._lib.rt_server_download_rgba8(self._h, int(job_id), out.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return out
+
+    def release(self, job_id):
+        _check(self._lib.rt_server_release(self._h, int(job_id)))
+        self._sizes.pop(job_id, None)
+
+    def step(self) -> bool:
+        w = C.c_int32()
+        _check(self._lib.rt_server_step(self._h, C.byref(w)))
+        return bool(w.value)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(self._lib.rt_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
 
 
 def verify_shading(op, inputs, materials=(), lights=(), media=()):

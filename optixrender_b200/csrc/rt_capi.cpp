@@ -90,7 +90,10 @@ DevMaterial to_dev(const rt_material& m) {
     d.nonlinear = m.nonlinear;
     d.coat_roughness_u = m.coat_roughness_u;
     d.coat_roughness_v = m.coat_roughness_v;
-    for (int t = 0; t < 8; t++) d.tex[t] = m.texture_ids[t];
+    for (int t = 0; t < 8; t++) {
+        d.tex[t] = m.texture_ids[t];
+        if (d.tex[t] >= 0) d.textured = 1;
+    }
     return d;
 }
 

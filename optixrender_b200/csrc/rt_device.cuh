@@ -117,8 +117,9 @@ struct __align__(16) DevMaterial {
     float specular[3];
     int nonlinear;
     float coat_roughness_u, coat_roughness_v;
-    float pad0, pad1;
-    int tex[8];
+    int textured;  // any tex[] >= 0
+    float pad1;
+    int tex[8];    // texture ids: albedo, roughness, anisotropy, specular, metallic, coat u, coat v, normal
 };
 static_assert(sizeof(DevMaterial) == 128, "DevMaterial layout");
 
@@ -199,6 +200,9 @@ struct SceneView {
     int env_w, env_h;
     const float* lut;
     const float* lut_avg;
+    const uint32_t* tex;     // RGBA8 texels of every material texture
+    const int4* tex_info;    // offset, width, height per texture
+    int num_tex;
 };
 
 // Camera vectors of Renderer::SetCamera (core/src/Renderer.cpp:796-813).

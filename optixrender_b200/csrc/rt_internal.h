@@ -24,6 +24,8 @@ struct rt_scene {
     std::vector<std::vector<float>> media_density;
     std::vector<float> env;
     int env_w = 0, env_h = 0;
+    std::vector<uint32_t> tex;       // RGBA8 texels of every texture, row 0 at v = 0
+    std::vector<int32_t> tex_info;   // offset, width, height per texture
     float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
     float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
 };
@@ -58,7 +60,7 @@ rtd::CameraView camera_view(const rt_camera& c, int w, int h);
 
 // Everything of a scene that lives on the device.
 struct DeviceScene {
-    DevBuf nodes, tri_v, tri_a, meshes, materials, lights, media, env, env_cache, lut, lut_avg;
+    DevBuf nodes, tri_v, tri_a, meshes, materials, lights, media, env, env_cache, lut, lut_avg, tex, tex_info;
     std::vector<DevBuf*> grids;
     rtd::SceneView view{};
     int bvh_depth = 0;

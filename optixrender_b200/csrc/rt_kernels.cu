@@ -25,6 +25,7 @@
 namespace rtd {
 
 constexpr int kBlock = 128;
+constexpr int kStaleTextured = 1 << 30;  // stale.w flag: the slot's mat_tex holds the last hit's material
 
 RT_D const WaveParams& wave_of(const Ctx& c) { return c.waves[*c.wave_index]; }
 
@@ -81,6 +82,7 @@ __global__ void k_raygen(Ctx c) {
         ctl->fetch_ext = 0;
         ctl->fetch_shade = 0;
         ctl->fetch_shadow = 0;
+        for (int b = 0; b < kShadeBuckets; b++) ctl->bucket[b] = 0;
     }
     if (slot >= W.wave_count) return;
     const Segment sg = W.seg[find_segment(W, slot)];
@@ -130,8 +132,24 @@ struct ExtendSrc {
         r.tmin = kEps;
         r.tmax = FLT_MAX;
     }
-    RT_D void finish(int i, int tri, float t, float b1, float b2) {
-        c->wb.hit[q[i]] = make_float4(tri >= 0 ? t : FLT_MAX, b1, b2, __int_as_float(tri));
+    // Stores the hit and, when the shade queue is sorted, appends the slot to
+    // the bucket of the hit surface's material type (tri_v[1].w of the
+    // triangle) with one atomicAdd per bucket present in the warp.
+    RT_D void finish(bool fin, int i, int tri, float t, float b1, float b2, const float4* tri_v) {
+        int slot = fin ? q[i] : 0;
+        if (fin) c->wb.hit[slot] = make_float4(tri >= 0 ? t : FLT_MAX, b1, b2, __int_as_float(tri));
+        int* sorted = c->wb.sorted;
+        if (sorted == nullptr || __ballot_sync(0xffffffffu, fin) == 0u) return;
+        int key = -1;
+        if (fin) key = tri >= 0 ? __float_as_int(__ldg(reinterpret_cast<const float*>(tri_v + size_t(tri) * 3 + 1) + 3))
+                                : kMissBucket;
+        const int lane = threadIdx.x & 31;
+        unsigned peers = __match_any_sync(0xffffffffu, key);
+        int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (fin && lane == leader) base = atomicAdd(&c->wb.ctl->bucket[key], __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (fin) sorted[size_t(key) * size_t(c->wb.capacity) + size_t(base + __popc(peers & ((1u << lane) - 1u)))] = slot;
     }
 };
 
@@ -211,6 +229,18 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
     const WaveParams& W = wave_of(c);
     const int lane = threadIdx.x & 31;
     uint32_t nan_paths = 0;
+    // Sorted queue: item i lies in the bucket whose prefix range holds it.
+    __shared__ int prefix[kShadeBuckets + 1];
+    const bool sorted = B.sorted != nullptr;
+    if (sorted && threadIdx.x == 0) {
+        int acc = 0;
+        for (int b = 0; b < kShadeBuckets; b++) {
+            prefix[b] = acc;
+            acc += ctl->bucket[b];
+        }
+        prefix[kShadeBuckets] = acc;
+    }
+    __syncthreads();
     while (true) {
         int base = warp_fetch(&ctl->fetch_shade, lane);
         if (base >= total) break;
@@ -221,7 +251,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
         v3 s0o, s0d, s1o, s1d;
         float s0t = 0.f, s1t = 0.f;
         if (i < total) {
-            slot = q[i];
+            if (sorted) {
+                int b = 0;
+                while (b < kShadeBuckets - 1 && i >= prefix[b + 1]) b++;
+                slot = B.sorted[size_t(b) * size_t(B.capacity) + size_t(i - prefix[b])];
+            } else {
+                slot = q[i];
+            }
             const Segment& sgm = W.seg[find_segment(W, slot)];
             const JobDesc* jd = c.jobs + sgm.job;
             const SceneView& sc = jd->sc;
@@ -258,17 +294,46 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 float u = h4.y, v = h4.z;
                 float w0 = 1.0f - u - v;
                 v3 Ns = normalize(w0 * xyz(a0) + u * xyz(a1) + v * xyz(a2));
-                v3 P = w0 * xyz(p0) + u * xyz(p1) + v * xyz(p2);
                 int mesh = __float_as_int(a3.w);
                 MeshInfo mi = sc.meshes[mesh];
+                s.mat = sc.materials + mi.material;
+                int stale_mesh = mesh;
+                const int4* mt = reinterpret_cast<const int4*>(s.mat);
+                if (__ldg(mt + 5).z != 0 && B.mat_tex != nullptr) {
+                    // texture overrides of the closest-hit program (devicePrograms.cu:84-115)
+                    float tcx = w0 * a0.w + u * a2.w + v * a3.y;
+                    float tcy = w0 * a1.w + u * a3.x + v * a3.z;
+                    const int4 ta = __ldg(mt + 6), tb = __ldg(mt + 7);
+                    DevMaterial* dm = B.mat_tex + slot;
+                    const float4* src = reinterpret_cast<const float4*>(s.mat);
+                    float4* dst = reinterpret_cast<float4*>(dm);
+#pragma unroll
+                    for (int w = 0; w < 6; w++) dst[w] = __ldg(src + w);
+                    if (ta.x >= 0) {
+                        float4 t = tex_lookup(sc, ta.x, tcx, tcy);
+                        dm->albedo[0] = t.x, dm->albedo[1] = t.y, dm->albedo[2] = t.z;
+                    }
+                    if (ta.y >= 0) dm->roughness = tex_lookup(sc, ta.y, tcx, tcy).x;
+                    if (ta.z >= 0) dm->anisotropy = tex_lookup(sc, ta.z, tcx, tcy).x;
+                    if (ta.w >= 0) {
+                        float4 t = tex_lookup(sc, ta.w, tcx, tcy);
+                        dm->specular[0] = t.x, dm->specular[1] = t.y, dm->specular[2] = t.z;
+                    }
+                    if (tb.x >= 0) dm->metallic = tex_lookup(sc, tb.x, tcx, tcy).x;
+                    if (tb.y >= 0) dm->coat_roughness_u = tex_lookup(sc, tb.y, tcx, tcy).x;
+                    if (tb.z >= 0) dm->coat_roughness_v = tex_lookup(sc, tb.z, tcx, tcy).x;
+                    if (tb.w >= 0) Ns = normal_from_tangent(Ns, xyz(tex_lookup(sc, tb.w, tcx, tcy)));
+                    s.mat = dm;
+                    stale_mesh = mesh | kStaleTextured;
+                }
+                v3 P = w0 * xyz(p0) + u * xyz(p1) + v * xyz(p2);
                 s.front = dot(d, Ns) < 0.0f;
                 s.sn = s.front ? Ns : -Ns;
-                s.mat = sc.materials + mi.material;
                 closest = length(P - o);
                 pos = P;
                 in_m = mi.in_medium;
                 out_m = mi.out_medium;
-                B.stale[slot] = make_float4(s.sn.x, s.sn.y, s.sn.z, __int_as_float(mesh));
+                B.stale[slot] = make_float4(s.sn.x, s.sn.y, s.sn.z, __int_as_float(stale_mesh));
                 if (bounce == 0) {
                     B.aov_a[slot] = make_float4(s.mat->albedo[0], s.mat->albedo[1], s.mat->albedo[2], Ns.x);
                     B.aov_n[slot] = make_float2(Ns.y, Ns.z);
@@ -278,7 +343,12 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 int mesh = __float_as_int(st.w);
                 s.sn = xyz(st);
                 s.front = true;
-                s.mat = mesh >= 0 ? sc.materials + sc.meshes[mesh].material : nullptr;
+                if (mesh < 0)
+                    s.mat = nullptr;
+                else if (mesh & kStaleTextured)  // the last hit's textured material stays, as isect.material does
+                    s.mat = B.mat_tex + slot;
+                else
+                    s.mat = sc.materials + sc.meshes[mesh].material;
                 closest = FLT_MAX;
                 in_m = out_m = jd->cam.medium;
                 if (bounce == 0) {
@@ -499,8 +569,8 @@ struct ShadowSrc {
         r.tmin = kEps;
         r.tmax = o.w;
     }
-    RT_D void finish(int i, int tri, float, float, float) {
-        if (tri < 0) return;
+    RT_D void finish(bool fin, int i, int tri, float, float, float, const float4*) {
+        if (!fin || tri < 0) return;
         int code = __float_as_int(c->wb.sh_d[i].w);
         int slot = code >> 1;
         (code & 1 ? c->wb.nee1 : c->wb.nee0)[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -510,6 +580,7 @@ struct ShadowSrc {
 template <bool Stats>
 __global__ void __launch_bounds__(kBlock, 8) k_shadow(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
+    if (blockIdx.x == 0 && threadIdx.x < kShadeBuckets) ctl->bucket[threadIdx.x] = 0;  // for the next extend
     const int total = ctl->shadow_count;
     uint32_t nodes = 0, tris = 0, rays = 0;
     ShadowSrc src{&c};
@@ -591,7 +662,7 @@ __global__ void k_resolve(Ctx c) {
     if (nans) atomicAdd(&B.ctl->stats[6], (unsigned long long)nans);
 }
 
-__global__ void k_next_wave(int* wave_index) { *wave_index += 1; }
+__global__ void k_next_wave(int* wave_index, int ring) { *wave_index = (*wave_index + 1) % ring; }
 
 // ------------------------------------------------------------------ finalize
 RT_D uint32_t tonemap_pixel(float4 c, int mode, float exposure) {
@@ -799,9 +870,13 @@ void launch_shadow(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t 
         k_shadow<false><<<s.blocks_shadow, kBlock, 0, st>>>(c);
 }
 void launch_resolve(const Ctx& c, cudaStream_t st) { k_resolve<<<grid_for(c.wb.capacity, 256), 256, 0, st>>>(c); }
-void launch_next_wave(const Ctx& c, cudaStream_t st) { k_next_wave<<<1, 1, 0, st>>>(c.wave_index); }
+void launch_next_wave(const Ctx& c, cudaStream_t st) { k_next_wave<<<1, 1, 0, st>>>(c.wave_index, c.wave_ring); }
 void launch_finalize(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_finalize<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
+}
+void launch_begin_n(const JobDesc* dj, int64_t npix, cudaStream_t st) { k_begin<<<grid_for(npix, 256), 256, 0, st>>>(dj); }
+void launch_finalize_n(const JobDesc* dj, int64_t npix, cudaStream_t st) {
+    k_finalize<<<grid_for(npix, 256), 256, 0, st>>>(dj);
 }
 void launch_trace(const SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st) {
     if (n <= 0) return;

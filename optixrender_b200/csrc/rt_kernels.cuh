@@ -11,6 +11,9 @@
 namespace rtd {
 
 constexpr int kMaxSegments = 16;
+// Shade queue buckets: the material type of the hit surface (0..7), or a miss.
+constexpr int kShadeBuckets = 9;
+constexpr int kMissBucket = 8;
 
 // Per-render parameters and per-pixel buffers of one job.
 struct JobParams {
@@ -55,6 +58,8 @@ struct WaveCtl {
     int pad;
     unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris,
                                   // NaN samples, paths ended by a NaN throughput
+    int bucket[kShadeBuckets];    // extend results per shade bucket
+    int pad2[3];
 };
 
 // Structure-of-arrays path state, one entry per slot of a wave.
@@ -73,6 +78,8 @@ struct WaveBufs {
     int* queue[2];   // active slots
     float4* sh_o;    // shadow ray origin, tmax
     float4* sh_d;    // shadow ray direction, slot * 2 + channel (bits)
+    int* sorted;     // kShadeBuckets regions of `capacity` slots: extend results by material type (or null)
+    DevMaterial* mat_tex;  // per slot: the textured copy of the last hit's material (null: no textures)
     WaveCtl* ctl;
     int capacity;
 };
@@ -91,6 +98,7 @@ struct Ctx {
     WaveBufs wb;
     const WaveParams* waves;
     int* wave_index;  // advanced by k_next_wave at the end of each wave
+    int wave_ring;    // number of WaveParams entries; the index wraps around
     int bounce;
     int max_depth;  // largest max_depth of the jobs in the wave
 };
@@ -112,6 +120,8 @@ void launch_shadow(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStre
 void launch_resolve(const rtd::Ctx& c, cudaStream_t st);
 void launch_next_wave(const rtd::Ctx& c, cudaStream_t st);
 void launch_finalize(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);
+void launch_begin_n(const rtd::JobDesc* dev_job, int64_t npix, cudaStream_t st);
+void launch_finalize_n(const rtd::JobDesc* dev_job, int64_t npix, cudaStream_t st);
 void launch_trace(const rtd::SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st);
 void launch_verify(int op, const rtd::SceneView& sc, const rtd::DevLight* lights, const rtd::DevMedium* media,
                    const float* in, int64_t n, float* out, cudaStream_t st);

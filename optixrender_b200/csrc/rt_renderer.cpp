@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -66,7 +67,12 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
         float4 id;
         std::memcpy(&id.x, &o, 4);
         tv[size_t(t) * 3 + 0] = make_float4(p[0], p[1], p[2], id.x);
-        tv[size_t(t) * 3 + 1] = make_float4(p[3], p[4], p[5], 0.0f);
+        // v1.w: the shade bucket (material type) of the triangle's mesh
+        int mt = s.mesh_mat[size_t(s.tri_mesh[size_t(o)])].type;
+        int key = (mt >= 0 && mt < kMissBucket) ? mt : 0;
+        float kf;
+        std::memcpy(&kf, &key, 4);
+        tv[size_t(t) * 3 + 1] = make_float4(p[3], p[4], p[5], kf);
         tv[size_t(t) * 3 + 2] = make_float4(p[6], p[7], p[8], 0.0f);
         int mesh = s.tri_mesh[size_t(o)];
         float mf;
@@ -76,6 +82,13 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
         ta[size_t(t) * 4 + 2] = make_float4(n[6], n[7], n[8], uv[2]);
         ta[size_t(t) * 4 + 3] = make_float4(uv[3], uv[4], uv[5], mf);
     }
+    const int ntex = int(s.tex_info.size() / 3);
+    for (size_t i = 0; i < s.mesh_mat.size(); i++)
+        for (int t = 0; t < 8; t++)
+            if (s.mesh_mat[i].texture_ids[t] >= ntex)
+                return fail(RT_ERR_INVALID_ARG, "mesh " + std::to_string(i) + " refers to texture " +
+                                                    std::to_string(s.mesh_mat[i].texture_ids[t]) + " of " +
+                                                    std::to_string(ntex));
     std::vector<MeshInfo> meshes(s.mesh_mat.size());
     std::vector<DevMaterial> mats(s.mesh_mat.size());
     for (size_t i = 0; i < meshes.size(); i++) {
@@ -95,6 +108,14 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
     RT_CUDA(ds.meshes.upload(meshes.data(), meshes.size() * sizeof(MeshInfo), st), "upload meshes");
     RT_CUDA(ds.materials.upload(mats.data(), mats.size() * sizeof(DevMaterial), st), "upload materials");
     RT_CUDA(ds.lights.upload(lights.data(), lights.size() * sizeof(DevLight), st), "upload lights");
+    if (ntex > 0) {
+        std::vector<int4> info(static_cast<size_t>(ntex));
+        for (int t = 0; t < ntex; t++)
+            info[size_t(t)] = make_int4(s.tex_info[3 * size_t(t)], s.tex_info[3 * size_t(t) + 1],
+                                        s.tex_info[3 * size_t(t) + 2], 0);
+        RT_CUDA(ds.tex.upload(s.tex.data(), s.tex.size() * sizeof(uint32_t), st), "upload textures");
+        RT_CUDA(ds.tex_info.upload(info.data(), info.size() * sizeof(int4), st), "upload textures");
+    }
     const float* avg = nullptr;
     const float* lut = kc_tables(&avg);
     RT_CUDA(ds.lut.upload(lut, 64 * 64 * sizeof(float), st), "upload LUT");
@@ -141,7 +162,11 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
     v.env_h = s.env_h;
     v.lut = ds.lut.as<float>();
     v.lut_avg = ds.lut_avg.as<float>();
-    ds.bytes = ds.nodes.bytes + ds.tri_v.bytes + ds.tri_a.bytes + ds.env.bytes + ds.env_cache.bytes;
+    v.tex = ds.tex.as<uint32_t>();
+    v.tex_info = ds.tex_info.as<int4>();
+    v.num_tex = ntex;
+    ds.bytes = ds.nodes.bytes + ds.tri_v.bytes + ds.tri_a.bytes + ds.env.bytes + ds.env_cache.bytes + ds.tex.bytes;
+    for (DevBuf* g : ds.grids) ds.bytes += g->bytes;
     return RT_OK;
 }
 
@@ -180,10 +205,14 @@ struct rt_renderer {
     DevBuf acc_color, acc_albedo, acc_normal, lcg_state, color, albedo, normal, rgba8;
     int capacity = 0;
     DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, ctl, segs, job;
+    DevBuf sorted;            // shade queue by material type
+    DevBuf mat_tex;           // per-slot textured materials (scenes with textures)
+    bool sort_shade = true;   // RT_SORT_SHADE=0 keeps the shade queue in extend order
+    int wave_paths = 0;       // slots per wave of the last render
     DevBuf wave_index;
     // one captured wave (raygen, (extend, shade, shadow) x depth, resolve, advance)
     cudaGraphExec_t graph = nullptr;
-    int graph_capacity = -1, graph_depth = -1;
+    int graph_capacity = -1, graph_depth = -1, graph_ring = -1;
     const void* graph_waves = nullptr;
     rth::LaunchShape shape{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -227,13 +256,24 @@ rt_status ensure_waves(rt_renderer* r, int cap) {
     RT_CUDA(r->q1.alloc(n * sizeof(int)), "allocate queues");
     RT_CUDA(r->sh_o.alloc(2 * n * sizeof(float4)), "allocate shadow queue");
     RT_CUDA(r->sh_d.alloc(2 * n * sizeof(float4)), "allocate shadow queue");
+    if (r->sort_shade) RT_CUDA(r->sorted.alloc(size_t(kShadeBuckets) * n * sizeof(int)), "allocate shade buckets");
+    if (r->ds.view.num_tex > 0) RT_CUDA(r->mat_tex.alloc(n * sizeof(DevMaterial)), "allocate textured materials");
     r->capacity = cap;
     return RT_OK;
 }
 
 int auto_capacity(const rt_options& o, int64_t npix, int64_t total) {
-    int64_t cap = o.wave_paths > 0 ? int64_t(o.wave_paths) : std::max<int64_t>(npix, int64_t(1) << 21);
-    cap = std::min<int64_t>(cap, int64_t(1) << 24);
+    // Large waves: the last bounces of a wave carry few paths and run at the
+    // latency of a handful of rays, so fewer, larger waves spend less time
+    // there.  Automatic: up to 2^26 slots (268 B each, 18 GB), at most a
+    // quarter of the free device memory.
+    int64_t cap = o.wave_paths > 0 ? int64_t(o.wave_paths) : std::max<int64_t>(npix, int64_t(1) << 26);
+    if (o.wave_paths <= 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+            cap = std::min<int64_t>(cap, std::max<int64_t>(int64_t(1) << 20, int64_t(fr / 4) / 400));
+    }
+    cap = std::min<int64_t>(cap, int64_t(1) << 26);
     if (o.rng == RT_RNG_LCG) cap = std::min<int64_t>(cap, npix);
     cap = std::min<int64_t>(cap, total);
     return int(std::max<int64_t>(cap, 1));
@@ -269,6 +309,7 @@ rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_rende
     }
     r->own_stream = true;
     r->opt = o;
+    if (const char* v = std::getenv("RT_SORT_SHADE")) r->sort_shade = std::atoi(v) != 0;
     rt_camera_default(&r->cam);
     st = upload_scene(*s, r->ds, r->stream);
     if (st == RT_OK) {
@@ -362,6 +403,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
     const int64_t npix = int64_t(o.width) * o.height;
     const int64_t total = npix * o.spp;
     const int cap = auto_capacity(o, npix, total);
+    r->wave_paths = cap;
     st = ensure_waves(r, cap);
     if (st) return st;
     if (!o.progressive) r->frame = 0;  // Renderer.cpp:642-644
@@ -437,10 +479,13 @@ rt_status rt_renderer_render(rt_renderer* r) {
     b.queue[1] = r->q1.as<int>();
     b.sh_o = r->sh_o.as<float4>();
     b.sh_d = r->sh_d.as<float4>();
+    b.sorted = r->sort_shade ? r->sorted.as<int>() : nullptr;
+    b.mat_tex = r->ds.view.num_tex > 0 ? r->mat_tex.as<DevMaterial>() : nullptr;
     b.ctl = r->ctl.as<WaveCtl>();
     b.capacity = r->capacity;
     c.waves = r->segs.as<WaveParams>();
     c.wave_index = r->wave_index.as<int>();
+    c.wave_ring = int(nwaves);
     c.max_depth = o.max_depth;
     auto issue_wave = [&](bool timed) {
         c.bounce = 0;
@@ -469,7 +514,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
         for (int64_t w = 0; w < nwaves; w++) issue_wave(stats);
     } else {
         if (!r->graph || r->graph_capacity != r->capacity || r->graph_depth != o.max_depth ||
-            r->graph_waves != r->segs.ptr) {
+            r->graph_waves != r->segs.ptr || r->graph_ring != int(nwaves)) {
             if (r->graph) cudaGraphExecDestroy(r->graph);
             r->graph = nullptr;
             cudaGraph_t g = nullptr;
@@ -482,6 +527,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
             r->graph_capacity = r->capacity;
             r->graph_depth = o.max_depth;
             r->graph_waves = r->segs.ptr;
+            r->graph_ring = int(nwaves);
         }
         for (int64_t w = 0; w < nwaves; w++) RT_CUDA(cudaGraphLaunch(r->graph, s), "launch wave graph");
     }
@@ -565,6 +611,7 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     out->waves = r->waves;
     out->launches = r->launches;
     out->extend_launches = r->extend_launches;
+    out->wave_paths = r->wave_paths;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, r->ev0, r->ev1);
     out->ms_total = ms;

@@ -3,6 +3,8 @@
 // Wavefront OBJ meshes (TriangleMesh::LoadMesh, core/src/Scene.cpp:83-179) and
 // Radiance RGBE environment images (HdrTexture, core/src/Scene.cpp:197-206).
 #include <cmath>
+#include <cctype>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -356,6 +358,146 @@ rt_status add_obj(rt_scene* s, const std::string& path, const rt_material* mat, 
     return rt_scene_add_mesh(s, &m, mat, out_m, in_m, out_id);
 }
 
+// ------------------------------------------------------------------ LDR images
+// Texture files for Scene::AddTexture (core/src/Scene.cpp:66-69, 181-189:
+// stbi_load forced to RGBA with a vertical flip, so row 0 is the bottom of
+// the picture).  Read here without an image library: uncompressed BMP (8-bit
+// palette, 24-bit, 32-bit) and binary PGM/PPM (P5/P6, maxval <= 255).
+uint32_t rd32(const std::string& d, size_t o) {
+    return uint32_t(uint8_t(d[o])) | (uint32_t(uint8_t(d[o + 1])) << 8) | (uint32_t(uint8_t(d[o + 2])) << 16) |
+           (uint32_t(uint8_t(d[o + 3])) << 24);
+}
+uint32_t rd16(const std::string& d, size_t o) { return uint32_t(uint8_t(d[o])) | (uint32_t(uint8_t(d[o + 1])) << 8); }
+
+bool read_bmp(const std::string& d, std::vector<uint8_t>& rgba, int& w, int& h, std::string& err) {
+    if (d.size() < 54) {
+        err = "truncated BMP header";
+        return false;
+    }
+    const uint32_t off = rd32(d, 10), hdr = rd32(d, 14);
+    const int32_t bw = int32_t(rd32(d, 18)), bh = int32_t(rd32(d, 22));
+    const uint32_t bpp = rd16(d, 28), comp = rd32(d, 30);
+    if (hdr < 40 || bw <= 0 || bh == 0 || (bpp != 8 && bpp != 24 && bpp != 32) ||
+        !(comp == 0 || (comp == 3 && bpp == 32))) {
+        err = "unsupported BMP (only uncompressed 8/24/32-bit)";
+        return false;
+    }
+    w = bw;
+    h = bh < 0 ? -bh : bh;
+    const size_t stride = (size_t(w) * bpp / 8 + 3) & ~size_t(3);
+    if (size_t(off) + stride * size_t(h) > d.size()) {
+        err = "truncated BMP pixel data";
+        return false;
+    }
+    uint32_t masks[4] = {0x00FF0000u, 0x0000FF00u, 0x000000FFu, 0xFF000000u};
+    if (comp == 3 && d.size() >= 14 + 52) {
+        for (int c = 0; c < 3; c++) masks[c] = rd32(d, 54 + 4 * size_t(c));
+        masks[3] = hdr >= 56 ? rd32(d, 66) : 0u;
+    }
+    const size_t ncol = bpp == 8 ? (rd32(d, 46) ? rd32(d, 46) : 256u) : 0u;
+    if (bpp == 8 && 14 + hdr + ncol * 4 > d.size()) {
+        err = "truncated BMP palette";
+        return false;
+    }
+    auto channel = [](uint32_t px, uint32_t mask) -> uint8_t {
+        if (!mask) return 255;
+        int shift = __builtin_ctz(mask);
+        uint32_t v = (px & mask) >> shift, mx = mask >> shift;
+        return uint8_t((v * 255u + mx / 2) / mx);
+    };
+    rgba.assign(size_t(w) * h * 4, 0);
+    bool any_alpha = false;
+    for (int y = 0; y < h; y++) {
+        // stored bottom-up when the height is positive: file row y is picture row y from the bottom
+        const int out_row = bh > 0 ? y : h - 1 - y;
+        const size_t row = size_t(off) + stride * size_t(y);
+        for (int x = 0; x < w; x++) {
+            uint8_t* o = &rgba[(size_t(out_row) * w + x) * 4];
+            if (bpp == 8) {
+                size_t idx = uint8_t(d[row + size_t(x)]);
+                if (idx >= ncol) idx = 0;
+                size_t pe = 14 + hdr + idx * 4;
+                o[0] = uint8_t(d[pe + 2]), o[1] = uint8_t(d[pe + 1]), o[2] = uint8_t(d[pe]), o[3] = 255;
+            } else if (bpp == 24) {
+                size_t q = row + size_t(x) * 3;
+                o[0] = uint8_t(d[q + 2]), o[1] = uint8_t(d[q + 1]), o[2] = uint8_t(d[q]), o[3] = 255;
+            } else {
+                uint32_t px = rd32(d, row + size_t(x) * 4);
+                for (int c = 0; c < 3; c++) o[c] = channel(px, masks[c]);
+                o[3] = masks[3] ? channel(px, masks[3]) : 255;
+                any_alpha = any_alpha || o[3] != 0;
+            }
+        }
+    }
+    if (bpp == 32 && masks[3] && !any_alpha)  // an all-zero alpha channel is taken as opaque
+        for (size_t i = 3; i < rgba.size(); i += 4) rgba[i] = 255;
+    return true;
+}
+
+bool read_pnm(const std::string& d, std::vector<uint8_t>& rgba, int& w, int& h, std::string& err) {
+    size_t pos = 2;
+    auto token = [&]() -> long {
+        while (pos < d.size()) {
+            if (d[pos] == '#') {
+                while (pos < d.size() && d[pos] != '\n') pos++;
+            } else if (std::isspace(uint8_t(d[pos]))) {
+                pos++;
+            } else {
+                break;
+            }
+        }
+        long v = -1;
+        while (pos < d.size() && std::isdigit(uint8_t(d[pos]))) v = (v < 0 ? 0 : v * 10) + (d[pos++] - '0');
+        return v;
+    };
+    const bool color = d[1] == '6';
+    long lw = token(), lh = token(), mx = token();
+    if (lw <= 0 || lh <= 0 || mx <= 0 || mx > 255) {
+        err = "unsupported PNM header (binary P5/P6 with maxval <= 255)";
+        return false;
+    }
+    pos++;  // the single whitespace after maxval
+    w = int(lw);
+    h = int(lh);
+    const size_t ch = color ? 3 : 1;
+    if (pos + size_t(w) * h * ch > d.size()) {
+        err = "truncated PNM pixel data";
+        return false;
+    }
+    rgba.assign(size_t(w) * h * 4, 255);
+    for (int y = 0; y < h; y++) {
+        const int out_row = h - 1 - y;  // stored top-down
+        for (int x = 0; x < w; x++) {
+            const size_t q = pos + (size_t(y) * w + x) * ch;
+            uint8_t* o = &rgba[(size_t(out_row) * w + x) * 4];
+            for (int c = 0; c < 3; c++) {
+                unsigned v = uint8_t(d[q + (color ? size_t(c) : 0)]);
+                o[c] = uint8_t((v * 255u + unsigned(mx) / 2) / unsigned(mx));
+            }
+        }
+    }
+    return true;
+}
+
+bool read_image(const std::string& path, std::vector<uint8_t>& rgba, int& w, int& h, std::string& err) {
+    std::string d;
+    if (!read_file(path, d)) {
+        err = "could not read " + path;
+        return false;
+    }
+    bool ok;
+    if (d.size() >= 2 && d[0] == 'B' && d[1] == 'M')
+        ok = read_bmp(d, rgba, w, h, err);
+    else if (d.size() >= 2 && d[0] == 'P' && (d[1] == '5' || d[1] == '6'))
+        ok = read_pnm(d, rgba, w, h, err);
+    else {
+        err = "unsupported image format (BMP or binary PGM/PPM)";
+        ok = false;
+    }
+    if (!ok) err = path + ": " + err;
+    return ok;
+}
+
 // ------------------------------------------------------------------ RGBE
 bool read_hdr(const std::string& path, std::vector<float>& rgba, int& w, int& h, std::string& err) {
     std::string data;
@@ -463,7 +605,7 @@ void rotation_matrix(const float deg[3], float m[9]) {
     m[8] = cy * cx;
 }
 
-bool material_from_json(const Json& j, rt_material& m, std::string& err) {
+bool material_from_json(const Json& j, rt_material& m, std::string& err, rt_scene* scene, const std::string& base) {
     rt_material_default(&m);
     std::string t = str(j.get("type"), "diffuse");
     float rough_default = m.roughness;
@@ -504,11 +646,26 @@ bool material_from_json(const Json& j, rt_material& m, std::string& err) {
     m.coat_weight = float(num(j.get("coat_weight"), m.coat_weight));
     m.coat_roughness_u = float(num(j.get("coat_roughness_u"), m.coat_roughness_u));
     m.coat_roughness_v = float(num(j.get("coat_roughness_v"), m.coat_roughness_v));
-    for (auto& kv : j.o) {
-        const std::string& k = kv.first;
-        if (k.size() > 13 && k.compare(k.size() - 13, 13, "_texture_type") == 0 && str(&kv.second, "") == "image")
-            std::fprintf(stderr, "[optixrender_b200] scene JSON: image texture for '%s' not supported; using the constant\n",
-                         k.substr(0, k.size() - 13).c_str());
+    // "<name>_texture_type": "image" with "<name>_path" (models/test.json:67-74)
+    static const char* kTexNames[8] = {"albedo",   "roughness",        "anisotropy",       "specular",
+                                       "metallic", "coat_roughness_u", "coat_roughness_v", "normal"};
+    for (int t = 0; t < 8; t++) {
+        const std::string name = kTexNames[t];
+        if (str(j.get((name + "_texture_type").c_str()), "constant") != "image") continue;
+        const std::string path = str(j.get((name + "_path").c_str()), "");
+        if (path.empty()) {
+            err = name + "_texture_type is image but " + name + "_path is missing";
+            return false;
+        }
+        std::vector<uint8_t> px;
+        int w = 0, h = 0;
+        if (!read_image(join_path(base, path), px, w, h, err)) return false;
+        int32_t id = -1;
+        if (rt_scene_add_texture(scene, px.data(), w, h, &id) != RT_OK) {
+            err = g_error;
+            return false;
+        }
+        m.texture_ids[t] = id;
     }
     return true;
 }
@@ -589,7 +746,7 @@ rt_status load_json(rt_scene* s, const std::string& text, const std::string& bas
         for (const Json& mj : ms->a) {
             rt_material m;
             std::string err;
-            if (!material_from_json(mj, m, err)) return fail(RT_ERR_PARSE, "scene JSON: " + err);
+            if (!material_from_json(mj, m, err, s, base)) return fail(RT_ERR_PARSE, "scene JSON: " + err);
             mats[str(mj.get("name"), "")] = m;
         }
     }
@@ -689,6 +846,44 @@ rt_status rt_scene_add_mesh_obj(rt_scene* s, const char* path, const rt_material
                                 int32_t* out_id) {
     if (!s || !path || !mat) return fail(RT_ERR_INVALID_ARG, "rt_scene_add_mesh_obj: NULL argument");
     return add_obj(s, path, mat, out_m, in_m, nullptr, out_id);
+}
+
+// Scene::AddTexture from pixels: RGBA8, row 0 at the bottom (v = 0).
+RT_API rt_status rt_scene_add_texture(rt_scene* s, const uint8_t* rgba, int32_t width, int32_t height, int32_t* id) {
+    if (!s || !rgba) return fail(RT_ERR_INVALID_ARG, "rt_scene_add_texture: NULL argument");
+    if (width <= 0 || height <= 0 || int64_t(width) * height > (int64_t(1) << 28))
+        return fail(RT_ERR_INVALID_ARG, "rt_scene_add_texture: bad size");
+    const size_t n = size_t(width) * size_t(height);
+    const int64_t off = int64_t(s->tex.size());
+    if (off + int64_t(n) > int64_t(INT32_MAX))
+        return fail(RT_ERR_OUT_OF_MEMORY, "rt_scene_add_texture: more than 2^31 texels in one scene");
+    s->tex.resize(s->tex.size() + n);
+    std::memcpy(s->tex.data() + off, rgba, n * 4);
+    s->tex_info.push_back(int32_t(off));
+    s->tex_info.push_back(width);
+    s->tex_info.push_back(height);
+    if (id) *id = int32_t(s->tex_info.size() / 3) - 1;
+    return RT_OK;
+}
+
+RT_API rt_status rt_scene_get_texture(const rt_scene* s, int32_t id, int32_t* width, int32_t* height, uint8_t* rgba) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_scene_get_texture: NULL scene");
+    if (id < 0 || size_t(id) * 3 >= s->tex_info.size()) return fail(RT_ERR_INVALID_ARG, "rt_scene_get_texture: bad id");
+    const int32_t off = s->tex_info[3 * size_t(id)], w = s->tex_info[3 * size_t(id) + 1], h = s->tex_info[3 * size_t(id) + 2];
+    if (width) *width = w;
+    if (height) *height = h;
+    if (rgba) std::memcpy(rgba, s->tex.data() + off, size_t(w) * size_t(h) * 4);
+    return RT_OK;
+}
+
+// Scene::AddTexture(fileName): BMP or binary PGM/PPM.
+RT_API rt_status rt_scene_add_texture_file(rt_scene* s, const char* path, int32_t* id) {
+    if (!s || !path) return fail(RT_ERR_INVALID_ARG, "rt_scene_add_texture_file: NULL argument");
+    std::vector<uint8_t> px;
+    int w = 0, h = 0;
+    std::string err;
+    if (!read_image(path, px, w, h, err)) return fail(RT_ERR_IO, "rt_scene_add_texture_file: " + err);
+    return rt_scene_add_texture(s, px.data(), w, h, id);
 }
 
 rt_status rt_scene_load_json(rt_scene* s, const char* path, rt_options* opts, rt_camera* cam) {

@@ -1,0 +1,658 @@
+// rt_server.cpp - continuous-batching render server.
+//
+// Scenes are uploaded once and stay resident.  Jobs are admitted in arrival
+// order while the device-memory budget and the job table allow; each
+// admitted job owns its accumulation and output buffers.  Every wave the
+// scheduler fills the shared path slots with contiguous path ranges taken
+// from the admitted jobs in admission order (up to kMaxSegments jobs per
+// wave), so a job that arrives while others run joins the next wave.  A wave
+// is one replay of a captured CUDA graph (raygen, (extend, shade, shadow) x
+// depth, resolve, advance) whose parameters come from a device ring.  A job
+// whose paths have all been issued gets its finalize kernel and an event; the
+// host marks it done when the event completes.
+//
+// Paths draw PCG32 streams keyed by (job seed, path index) and each pixel's
+// samples are summed in sample order, so a job's image does not depend on
+// which jobs share its waves.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "rt_internal.h"
+
+using namespace rtd;
+using namespace rti;
+
+namespace {
+
+#define SV_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+struct Job {
+    int64_t id;
+    rt_job_desc desc;
+    int state = RT_JOB_QUEUED;
+    double submit_ms = 0, admit_ms = 0, done_ms = 0;
+    int slot = -1;
+    int64_t npix = 0, total = 0, issued = 0;
+    int64_t bytes = 0;
+    DevBuf acc_color, acc_albedo, acc_normal, lcg, color, albedo, normal, rgba8;
+    cudaEvent_t done_ev = nullptr;
+    bool finalize_issued = false;
+};
+
+int64_t job_bytes(int64_t npix) { return npix * (6 * 16 + 2 * 4); }
+
+}  // namespace
+
+struct rt_server {
+    rt_server_options opt{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::chrono::steady_clock::time_point t0;
+    std::vector<std::unique_ptr<DeviceScene>> scenes;
+    int64_t scene_bytes = 0;
+    std::map<int64_t, std::unique_ptr<Job>> jobs;
+    std::deque<int64_t> queued;
+    std::vector<int64_t> running;  // admission order
+    std::vector<int> free_slots;
+    int64_t next_id = 1;
+    size_t rr = 0;  // round-robin position of the fair-share policy
+    int64_t bytes_in_use = 0;
+    // device state
+    DevBuf job_table, ring, wave_index, ctl;
+    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, sorted;
+    DevBuf mat_tex;  // per-slot textured materials, once a scene with textures is resident
+    int capacity = 0;
+    int ring_size = 0;
+    int ring_pos = 0;
+    WaveParams* host_ring = nullptr;   // pinned
+    std::vector<cudaEvent_t> ring_ev;
+    std::map<int, cudaGraphExec_t> graphs;  // by bounce count
+    rth::LaunchShape shape{};
+    // stats
+    int64_t waves = 0, paths = 0, done = 0, submitted = 0;
+    int max_segments = 0;
+    // background thread
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread worker;
+    bool stop = false;
+    std::string bg_error;
+
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+rt_status setup(rt_server* s) {
+    SV_CUDA(cudaGetDevice(&s->device), "rt_server_create");
+    SV_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "rt_server_create");
+    const int n = s->opt.max_jobs;
+    SV_CUDA(s->job_table.alloc(size_t(n) * sizeof(JobDesc)), "allocate job table");
+    SV_CUDA(cudaMemset(s->job_table.ptr, 0, size_t(n) * sizeof(JobDesc)), "clear job table");
+    s->ring_size = std::max(2, s->opt.waves_in_flight + 1);
+    SV_CUDA(s->ring.alloc(size_t(s->ring_size) * sizeof(WaveParams)), "allocate wave ring");
+    SV_CUDA(s->wave_index.alloc(sizeof(int)), "allocate wave counter");
+    SV_CUDA(cudaMemset(s->wave_index.ptr, 0, sizeof(int)), "clear wave counter");
+    SV_CUDA(s->ctl.alloc(sizeof(WaveCtl)), "allocate counters");
+    SV_CUDA(cudaMemset(s->ctl.ptr, 0, sizeof(WaveCtl)), "clear counters");
+    SV_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s->host_ring), size_t(s->ring_size) * sizeof(WaveParams)),
+            "allocate pinned wave ring");
+    for (int i = 0; i < s->ring_size; i++) {
+        cudaEvent_t e;
+        SV_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
+        s->ring_ev.push_back(e);
+    }
+    const size_t cap = size_t(s->opt.wave_paths);
+    DevBuf* f4s[] = {&s->ray_o, &s->ray_d, &s->hit, &s->thr, &s->rad, &s->nee0, &s->nee1, &s->stale, &s->aov_a};
+    for (DevBuf* b : f4s) SV_CUDA(b->alloc(cap * sizeof(float4)), "allocate path state");
+    SV_CUDA(s->aov_n.alloc(cap * sizeof(float2)), "allocate path state");
+    SV_CUDA(s->rng.alloc(cap * sizeof(uint2)), "allocate path state");
+    SV_CUDA(s->q0.alloc(cap * sizeof(int)), "allocate queues");
+    SV_CUDA(s->q1.alloc(cap * sizeof(int)), "allocate queues");
+    SV_CUDA(s->sh_o.alloc(2 * cap * sizeof(float4)), "allocate shadow queue");
+    SV_CUDA(s->sh_d.alloc(2 * cap * sizeof(float4)), "allocate shadow queue");
+    SV_CUDA(s->sorted.alloc(size_t(kShadeBuckets) * cap * sizeof(int)), "allocate shade buckets");
+    s->capacity = int(cap);
+    for (int i = n - 1; i >= 0; i--) s->free_slots.push_back(i);
+    rth::query_shape(s->shape);
+    if (s->opt.hbm_budget_bytes <= 0) {
+        size_t fr = 0, tot = 0;
+        SV_CUDA(cudaMemGetInfo(&fr, &tot), "query device memory");
+        s->opt.hbm_budget_bytes = int64_t(double(fr) * 0.8);
+    }
+    return RT_OK;
+}
+
+Ctx make_ctx(rt_server* s) {
+    Ctx c;
+    std::memset(&c, 0, sizeof(c));
+    c.jobs = s->job_table.as<JobDesc>();
+    WaveBufs& b = c.wb;
+    b.ray_o = s->ray_o.as<float4>();
+    b.ray_d = s->ray_d.as<float4>();
+    b.hit = s->hit.as<float4>();
+    b.thr = s->thr.as<float4>();
+    b.rad = s->rad.as<float4>();
+    b.nee0 = s->nee0.as<float4>();
+    b.nee1 = s->nee1.as<float4>();
+    b.stale = s->stale.as<float4>();
+    b.aov_a = s->aov_a.as<float4>();
+    b.aov_n = s->aov_n.as<float2>();
+    b.rng = s->rng.as<uint2>();
+    b.queue[0] = s->q0.as<int>();
+    b.queue[1] = s->q1.as<int>();
+    b.sh_o = s->sh_o.as<float4>();
+    b.sh_d = s->sh_d.as<float4>();
+    b.sorted = s->sorted.as<int>();
+    b.mat_tex = s->mat_tex.ptr ? s->mat_tex.as<DevMaterial>() : nullptr;
+    b.ctl = s->ctl.as<WaveCtl>();
+    b.capacity = s->capacity;
+    c.waves = s->ring.as<WaveParams>();
+    c.wave_index = s->wave_index.as<int>();
+    c.wave_ring = s->ring_size;
+    c.max_depth = s->opt.max_depth;
+    return c;
+}
+
+// One captured wave per bounce count: raygen, (extend, shade, shadow) x depth,
+// resolve, advance of the wave ring.  A wave uses the graph of the deepest
+// job in it; each path still stops at its own job's max_depth.
+rt_status wave_graph(rt_server* s, int depth, cudaGraphExec_t* out) {
+    auto it = s->graphs.find(depth);
+    if (it != s->graphs.end()) {
+        *out = it->second;
+        return RT_OK;
+    }
+    Ctx c = make_ctx(s);
+    c.max_depth = depth;
+    cudaGraph_t g = nullptr;
+    SV_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+    c.bounce = 0;
+    rth::launch_raygen(c, s->stream);
+    for (int b = 0; b < depth; b++) {
+        c.bounce = b;
+        rth::launch_extend(c, s->shape, false, s->stream);
+        rth::launch_shade(c, s->shape, false, s->stream);
+        rth::launch_shadow(c, s->shape, false, s->stream);
+    }
+    rth::launch_resolve(c, s->stream);
+    rth::launch_next_wave(c, s->stream);
+    SV_CUDA(cudaStreamEndCapture(s->stream, &g), "end graph capture");
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "instantiate wave graph");
+    s->graphs[depth] = ge;
+    *out = ge;
+    return RT_OK;
+}
+
+rt_status admit(rt_server* s, Job& j) {
+    const rt_job_desc& d = j.desc;
+    j.npix = int64_t(d.width) * d.height;
+    j.total = j.npix * d.spp;
+    j.bytes = job_bytes(j.npix);
+    DevBuf* f4s[] = {&j.acc_color, &j.acc_albedo, &j.acc_normal, &j.color, &j.albedo, &j.normal};
+    for (DevBuf* b : f4s) SV_CUDA(b->alloc(size_t(j.npix) * sizeof(float4)), "allocate job buffers");
+    SV_CUDA(j.lcg.alloc(size_t(j.npix) * 4), "allocate job buffers");
+    SV_CUDA(j.rgba8.alloc(size_t(j.npix) * 4), "allocate job buffers");
+    SV_CUDA(cudaEventCreateWithFlags(&j.done_ev, cudaEventDisableTiming), "create event");
+    j.slot = s->free_slots.back();
+    s->free_slots.pop_back();
+    JobDesc hj;
+    std::memset(&hj, 0, sizeof(hj));
+    hj.sc = s->scenes[size_t(d.scene)]->view;
+    hj.cam = camera_view(d.camera, d.width, d.height);
+    JobParams& p = hj.job;
+    p.width = d.width;
+    p.height = d.height;
+    p.spp = d.spp;
+    p.max_depth = d.max_depth;
+    p.filter = d.filter;
+    p.rng = RT_RNG_PCG32;
+    p.rr_depth = d.rr_depth;
+    p.frame = 0;
+    p.seed = d.seed;
+    p.npix = j.npix;
+    p.tonemap = d.tonemap;
+    p.exposure = d.exposure;
+    p.acc_color = j.acc_color.as<float4>();
+    p.acc_albedo = j.acc_albedo.as<float4>();
+    p.acc_normal = j.acc_normal.as<float4>();
+    p.lcg_state = j.lcg.as<uint32_t>();
+    p.color = j.color.as<float4>();
+    p.albedo = j.albedo.as<float4>();
+    p.normal = j.normal.as<float4>();
+    p.rgba8 = j.rgba8.as<uint32_t>();
+    JobDesc* dj = s->job_table.as<JobDesc>() + j.slot;
+    SV_CUDA(cudaMemcpyAsync(dj, &hj, sizeof(hj), cudaMemcpyHostToDevice, s->stream), "upload job");
+    SV_CUDA(cudaStreamSynchronize(s->stream), "upload job");  // hj is a stack object
+    rth::launch_begin_n(dj, j.npix, s->stream);
+    j.state = RT_JOB_RUNNING;
+    j.admit_ms = s->now_ms();
+    s->bytes_in_use += j.bytes;
+    return RT_OK;
+}
+
+void free_job(rt_server* s, Job& j) {
+    DevBuf* all[] = {&j.acc_color, &j.acc_albedo, &j.acc_normal, &j.lcg, &j.color, &j.albedo, &j.normal, &j.rgba8};
+    for (DevBuf* b : all) b->release();
+    if (j.done_ev) cudaEventDestroy(j.done_ev);
+    j.done_ev = nullptr;
+    if (j.slot >= 0) s->free_slots.push_back(j.slot);
+    j.slot = -1;
+    s->bytes_in_use -= j.bytes;
+    j.bytes = 0;
+}
+
+// One scheduling step with the lock held.  When the next slot of the wave
+// ring is still read by a queued wave, nothing is issued and *blocked names
+// the event to wait for (outside the lock).
+rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
+    int work = 0;
+    *blocked = nullptr;
+    // retire finished jobs
+    for (size_t i = 0; i < s->running.size();) {
+        Job& j = *s->jobs[s->running[i]];
+        if (j.finalize_issued && cudaEventQuery(j.done_ev) == cudaSuccess) {
+            j.state = RT_JOB_DONE;
+            j.done_ms = s->now_ms();
+            s->done++;
+            s->running.erase(s->running.begin() + long(i));
+            work = 1;
+        } else {
+            i++;
+        }
+    }
+    // admission in arrival order by memory budget and free slots (a finished
+    // job holds its memory and slot until it is released)
+    while (!s->queued.empty() && !s->free_slots.empty()) {
+        Job& j = *s->jobs[s->queued.front()];
+        int64_t need = job_bytes(int64_t(j.desc.width) * j.desc.height);
+        if (s->bytes_in_use + s->scene_bytes + need > s->opt.hbm_budget_bytes) break;
+        s->queued.pop_front();
+        rt_status st = admit(s, j);
+        if (st) {
+            j.state = RT_JOB_FAILED;
+            free_job(s, j);
+            return st;
+        }
+        s->running.push_back(j.id);
+        work = 1;
+    }
+    // fill a wave from the running jobs
+    if (cudaEventQuery(s->ring_ev[size_t(s->ring_pos)]) == cudaErrorNotReady) {
+        *blocked = s->ring_ev[size_t(s->ring_pos)];
+        if (did_work) *did_work = 1;
+        return RT_OK;
+    }
+    // Paths each job gets in this wave.
+    std::vector<Job*> active;
+    for (int64_t id : s->running) {
+        Job& j = *s->jobs[id];
+        if (j.issued < j.total) active.push_back(&j);
+    }
+    std::vector<std::pair<Job*, int64_t>> plan;
+    if (!active.empty()) {
+        if (s->opt.policy == RT_SERVE_FIFO) {
+            int64_t left = s->capacity;
+            for (Job* j : active) {
+                if (left == 0 || int(plan.size()) == kMaxSegments) break;
+                int64_t take = std::min(j->total - j->issued, left);
+                plan.emplace_back(j, take);
+                left -= take;
+            }
+        } else {
+            // Fair share: up to kMaxSegments jobs, taken round-robin, split the
+            // wave evenly; a job that needs less than its share gives the rest
+            // to the others (water filling).
+            const size_t k = std::min(active.size(), size_t(kMaxSegments));
+            const size_t start = s->rr % active.size();
+            std::vector<Job*> chosen;
+            for (size_t i = 0; i < k; i++) chosen.push_back(active[(start + i) % active.size()]);
+            s->rr = start + k;
+            std::vector<size_t> order(k);
+            for (size_t i = 0; i < k; i++) order[i] = i;
+            std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+                return chosen[a]->total - chosen[a]->issued < chosen[b]->total - chosen[b]->issued;
+            });
+            std::vector<int64_t> give(k, 0);
+            int64_t left = s->capacity;
+            for (size_t n = 0; n < k; n++) {
+                size_t i = order[n];
+                give[i] = std::min(chosen[i]->total - chosen[i]->issued, left / int64_t(k - n));
+                left -= give[i];
+            }
+            for (size_t i = 0; i < k && left > 0; i++) {  // remainder of the integer split
+                int64_t extra = std::min(left, chosen[i]->total - chosen[i]->issued - give[i]);
+                give[i] += extra;
+                left -= extra;
+            }
+            for (size_t i = 0; i < k; i++)
+                if (give[i] > 0) plan.emplace_back(chosen[i], give[i]);
+        }
+    }
+    WaveParams wp;
+    std::memset(&wp, 0, sizeof(wp));
+    int filled = 0, depth = 1;
+    std::vector<Job*> completing;
+    for (auto& pj : plan) {
+        Job& j = *pj.first;
+        Segment& g = wp.seg[wp.num_seg++];
+        g.job = j.slot;
+        g.slot_begin = filled;
+        g.count = int(pj.second);
+        g.path_begin = j.issued;
+        j.issued += pj.second;
+        filled += int(pj.second);
+        depth = std::max(depth, j.desc.max_depth);
+        if (j.issued >= j.total) completing.push_back(&j);
+    }
+    if (filled > 0) {
+        wp.wave_count = filled;
+        cudaGraphExec_t graph = nullptr;
+        rt_status gs = wave_graph(s, depth, &graph);
+        if (gs) return gs;
+        int pos = s->ring_pos;
+        s->host_ring[pos] = wp;
+        SV_CUDA(cudaMemcpyAsync(s->ring.as<WaveParams>() + pos, &s->host_ring[pos], sizeof(WaveParams),
+                                cudaMemcpyHostToDevice, s->stream),
+                "upload wave");
+        SV_CUDA(cudaGraphLaunch(graph, s->stream), "launch wave");
+        SV_CUDA(cudaEventRecord(s->ring_ev[size_t(pos)], s->stream), "record event");
+        s->ring_pos = (pos + 1) % s->ring_size;
+        s->waves++;
+        s->paths += filled;
+        s->max_segments = std::max(s->max_segments, wp.num_seg);
+        for (Job* j : completing) {
+            JobDesc* dj = s->job_table.as<JobDesc>() + j->slot;
+            rth::launch_finalize_n(dj, j->npix, s->stream);
+            SV_CUDA(cudaEventRecord(j->done_ev, s->stream), "record event");
+            j->finalize_issued = true;
+        }
+        work = 1;
+    } else if (!s->running.empty()) {
+        work = 1;  // waiting for finalize events
+    }
+    if (did_work) *did_work = work;
+    return RT_OK;
+}
+
+void worker_loop(rt_server* s) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        if (s->queued.empty() && s->running.empty()) {
+            s->cv.wait(lk);
+            continue;
+        }
+        int32_t w = 0;
+        cudaEvent_t blocked = nullptr;
+        rt_status st = step_locked(s, &w, &blocked);
+        if (blocked) {
+            lk.unlock();
+            cudaEventSynchronize(blocked);
+            lk.lock();
+            continue;
+        }
+        if (st) {
+            s->bg_error = g_error;
+            for (int64_t id : s->running) s->jobs[id]->state = RT_JOB_FAILED;
+            s->running.clear();
+        }
+        bool waiting_only = true;
+        for (int64_t id : s->running)
+            if (s->jobs[id]->issued < s->jobs[id]->total) waiting_only = false;
+        s->cv.notify_all();
+        if (waiting_only && s->queued.empty()) {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+            lk.lock();
+        }
+    }
+}
+
+void fill_status(const rt_server* s, const Job& j, rt_job_status* st) {
+    std::memset(st, 0, sizeof(*st));
+    st->state = j.state;
+    st->submit_ms = j.submit_ms;
+    st->admit_ms = j.admit_ms;
+    st->done_ms = j.done_ms;
+    st->paths = j.total ? j.total : int64_t(j.desc.width) * j.desc.height * j.desc.spp;
+    st->bytes = j.bytes;
+    (void)s;
+}
+
+}  // namespace
+
+extern "C" {
+
+void rt_server_options_default(rt_server_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->wave_paths = 1 << 23;
+    o->max_jobs = 64;
+    o->max_depth = 32;
+    o->background = 1;
+    o->waves_in_flight = 2;
+}
+
+rt_status rt_server_create(const rt_server_options* o, rt_server** out) {
+    if (!out) return fail(RT_ERR_INVALID_ARG, "rt_server_create: out is NULL");
+    rt_server* s = new (std::nothrow) rt_server();
+    if (!s) return fail(RT_ERR_OUT_OF_MEMORY, "rt_server_create: out of host memory");
+    rt_server_options_default(&s->opt);
+    if (o) {
+        s->opt = *o;
+        if (s->opt.wave_paths <= 0) s->opt.wave_paths = 1 << 23;
+        if (s->opt.max_jobs <= 0) s->opt.max_jobs = 64;
+        if (s->opt.max_depth <= 0) s->opt.max_depth = 32;
+        if (s->opt.waves_in_flight <= 0) s->opt.waves_in_flight = 2;
+    }
+    if (s->opt.policy != RT_SERVE_FAIR && s->opt.policy != RT_SERVE_FIFO) {
+        delete s;
+        return fail(RT_ERR_INVALID_ARG, "rt_server_create: unknown policy");
+    }
+    if (s->opt.max_jobs > 256 || s->opt.wave_paths > (1 << 26)) {
+        delete s;
+        return fail(RT_ERR_INVALID_ARG, "rt_server_create: max_jobs <= 256 and wave_paths <= 2^26");
+    }
+    s->t0 = std::chrono::steady_clock::now();
+    rt_status st = setup(s);
+    if (st) {
+        rt_server_destroy(s);
+        return st;
+    }
+    if (s->opt.background) s->worker = std::thread(worker_loop, s);
+    *out = s;
+    return RT_OK;
+}
+
+rt_status rt_server_destroy(rt_server* s) {
+    if (!s) return RT_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& kv : s->jobs) free_job(s, *kv.second);
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    for (cudaEvent_t e : s->ring_ev) cudaEventDestroy(e);
+    if (s->host_ring) cudaFreeHost(s->host_ring);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return RT_OK;
+}
+
+rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* id) {
+    if (!s || !scene) return fail(RT_ERR_INVALID_ARG, "rt_server_add_scene: NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::unique_ptr<DeviceScene> ds(new DeviceScene());
+    rt_status st = upload_scene(*scene, *ds, s->stream);
+    if (st) return st;
+    if (ds->view.num_tex > 0 && !s->mat_tex.ptr) {
+        SV_CUDA(cudaStreamSynchronize(s->stream), "rt_server_add_scene");
+        SV_CUDA(s->mat_tex.alloc(size_t(s->capacity) * sizeof(DevMaterial)), "allocate textured materials");
+        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);  // captured without the buffer
+        s->graphs.clear();
+    }
+    s->scene_bytes += int64_t(ds->bytes);
+    s->scenes.push_back(std::move(ds));
+    if (id) *id = int32_t(s->scenes.size()) - 1;
+    return RT_OK;
+}
+
+rt_status rt_server_submit(rt_server* s, const rt_job_desc* d, int64_t* id) {
+    if (!s || !d) return fail(RT_ERR_INVALID_ARG, "rt_server_submit: NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (d->scene < 0 || d->scene >= int(s->scenes.size())) return fail(RT_ERR_INVALID_ARG, "rt_server_submit: unknown scene");
+    if (d->width <= 0 || d->height <= 0 || d->spp <= 0 || d->max_depth <= 0 || d->max_depth > s->opt.max_depth)
+        return fail(RT_ERR_INVALID_ARG, "rt_server_submit: bad size, spp or max_depth (<= the server's max_depth)");
+    if (job_bytes(int64_t(d->width) * d->height) + s->scene_bytes > s->opt.hbm_budget_bytes)
+        return fail(RT_ERR_OUT_OF_MEMORY, "rt_server_submit: the job alone exceeds the memory budget");
+    std::unique_ptr<Job> j(new Job());
+    j->id = s->next_id++;
+    j->desc = *d;
+    j->submit_ms = s->now_ms();
+    int64_t jid = j->id;
+    s->jobs[jid] = std::move(j);
+    s->queued.push_back(jid);
+    s->submitted++;
+    if (id) *id = jid;
+    s->cv.notify_all();
+    return RT_OK;
+}
+
+rt_status rt_server_cancel(rt_server* s, int64_t id) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_cancel: NULL server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_cancel: unknown job");
+    Job& j = *it->second;
+    if (j.state != RT_JOB_QUEUED) return fail(RT_ERR_STATE, "rt_server_cancel: only queued jobs can be cancelled");
+    s->queued.erase(std::find(s->queued.begin(), s->queued.end(), id));
+    j.state = RT_JOB_CANCELLED;
+    return RT_OK;
+}
+
+rt_status rt_server_poll(rt_server* s, int64_t id, rt_job_status* st) {
+    if (!s || !st) return fail(RT_ERR_INVALID_ARG, "rt_server_poll: NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_poll: unknown job");
+    fill_status(s, *it->second, st);
+    return RT_OK;
+}
+
+rt_status rt_server_wait(rt_server* s, int64_t id, double timeout_ms, rt_job_status* st) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_wait: NULL server");
+    const auto t_end = std::chrono::steady_clock::now() + std::chrono::microseconds(int64_t(timeout_ms * 1000.0));
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        auto it = s->jobs.find(id);
+        if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_wait: unknown job");
+        Job& j = *it->second;
+        if (j.state == RT_JOB_DONE || j.state == RT_JOB_FAILED || j.state == RT_JOB_CANCELLED) {
+            if (st) fill_status(s, j, st);
+            if (j.state == RT_JOB_FAILED) return fail(RT_ERR_CUDA, "job failed: " + s->bg_error);
+            return RT_OK;
+        }
+        if (timeout_ms >= 0 && std::chrono::steady_clock::now() >= t_end)
+            return fail(RT_ERR_TIMEOUT, "rt_server_wait: timed out");
+        if (!s->opt.background) {  // manual mode: the caller's thread drives the loop
+            int32_t w = 0;
+            cudaEvent_t blocked = nullptr;
+            rt_status e = step_locked(s, &w, &blocked);
+            if (e) return e;
+            if (blocked) SV_CUDA(cudaEventSynchronize(blocked), "rt_server_wait");
+            if (!w)
+                return fail(RT_ERR_STATE, "rt_server_wait: the job can make no progress (memory budget or job slots "
+                                          "held by finished jobs that were not released)");
+        } else if (timeout_ms >= 0) {
+            s->cv.wait_until(lk, t_end);
+        } else {
+            s->cv.wait(lk);
+        }
+    }
+}
+
+static rt_status download_job(rt_server* s, int64_t id, void* dst, bool rgba8) {
+    if (!s || !dst) return fail(RT_ERR_INVALID_ARG, "rt_server_download: NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_download: unknown job");
+    Job& j = *it->second;
+    if (j.state != RT_JOB_DONE) return fail(RT_ERR_STATE, "rt_server_download: job not done");
+    const DevBuf& b = rgba8 ? j.rgba8 : j.color;
+    if (!b.ptr) return fail(RT_ERR_STATE, "rt_server_download: job released");
+    SV_CUDA(cudaMemcpyAsync(dst, b.ptr, size_t(j.npix) * (rgba8 ? 4 : 16), cudaMemcpyDeviceToHost, s->stream),
+            "rt_server_download");
+    SV_CUDA(cudaStreamSynchronize(s->stream), "rt_server_download");
+    return RT_OK;
+}
+
+rt_status rt_server_download(rt_server* s, int64_t id, float* rgba) { return download_job(s, id, rgba, false); }
+
+rt_status rt_server_download_rgba8(rt_server* s, int64_t id, uint32_t* pixels) {
+    return download_job(s, id, pixels, true);
+}
+
+rt_status rt_server_release(rt_server* s, int64_t id) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_release: NULL server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_release: unknown job");
+    Job& j = *it->second;
+    if (j.state == RT_JOB_RUNNING) return fail(RT_ERR_STATE, "rt_server_release: job still running");
+    if (j.state == RT_JOB_QUEUED) s->queued.erase(std::find(s->queued.begin(), s->queued.end(), id));
+    free_job(s, j);
+    s->jobs.erase(it);
+    s->cv.notify_all();
+    return RT_OK;
+}
+
+rt_status rt_server_step(rt_server* s, int32_t* did_work) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_step: NULL server");
+    if (s->opt.background) return fail(RT_ERR_STATE, "rt_server_step: server runs in the background");
+    std::lock_guard<std::mutex> lk(s->mu);
+    cudaEvent_t blocked = nullptr;
+    rt_status st = step_locked(s, did_work, &blocked);
+    if (st) return st;
+    if (blocked) SV_CUDA(cudaEventSynchronize(blocked), "rt_server_step");
+    return RT_OK;
+}
+
+rt_status rt_server_get_stats(rt_server* s, rt_server_stats* st) {
+    if (!s || !st) return fail(RT_ERR_INVALID_ARG, "rt_server_get_stats: NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::memset(st, 0, sizeof(*st));
+    st->jobs_submitted = s->submitted;
+    st->jobs_done = s->done;
+    st->jobs_queued = int64_t(s->queued.size());
+    st->jobs_running = int64_t(s->running.size());
+    st->waves = s->waves;
+    st->paths = s->paths;
+    st->bytes_in_use = s->bytes_in_use + s->scene_bytes;
+    st->bytes_budget = s->opt.hbm_budget_bytes;
+    st->max_segments_in_a_wave = s->max_segments;
+    return RT_OK;
+}
+
+}  // extern "C"

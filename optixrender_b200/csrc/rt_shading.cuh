@@ -206,9 +206,9 @@ struct MatParams {
 };
 RT_D MatParams load_material(const DevMaterial* m) {
     MatParams p;
+    // plain loads: `m` may be a path's textured copy written earlier in the same kernel
     const float4* q = reinterpret_cast<const float4*>(m);
-    float4 w0 = __ldg(q + 0), w1 = __ldg(q + 1), w2 = __ldg(q + 2), w3 = __ldg(q + 3), w4 = __ldg(q + 4),
-           w5 = __ldg(q + 5);
+    float4 w0 = q[0], w1 = q[1], w2 = q[2], w3 = q[3], w4 = q[4], w5 = q[5];
     p.type = __float_as_int(w0.x);
     p.albedo = v3(w0.y, w0.z, w0.w);
     p.rough = w1.x;
@@ -865,6 +865,51 @@ RT_D float4 tex_bilinear(const float4* img, int w, int h, float u, float v) {
     r.z = mixf(mixf(t00.z, t10.z, a), mixf(t01.z, t11.z, a), b);
     r.w = mixf(mixf(t00.w, t10.w, a), mixf(t01.w, t11.w, a), b);
     return r;
+}
+
+// ------------------------------------------------------------ material textures
+// tex2D<float4> of an RGBA8 texture with cudaReadModeNormalizedFloat,
+// normalized coordinates, wrap addressing and linear filtering
+// (core/src/Renderer.cpp:100-143), evaluated in software with FP32 weights on
+// texels converted as byte * (1/255).
+RT_D float4 texel_rgba8(uint32_t p) {
+    const float s = 1.0f / 255.0f;
+    return make_float4(float(p & 0xFFu) * s, float((p >> 8) & 0xFFu) * s, float((p >> 16) & 0xFFu) * s,
+                       float(p >> 24) * s);
+}
+RT_D float4 tex_rgba8(const uint32_t* img, int w, int h, float u, float v) {
+    u = u - floorf(u);
+    v = v - floorf(v);
+    float x = u * float(w) - 0.5f, y = v * float(h) - 0.5f;
+    float fx = floorf(x), fy = floorf(y);
+    float a = x - fx, b = y - fy;
+    int x0 = int(fx), y0 = int(fy);
+    int x1 = x0 + 1, y1 = y0 + 1;
+    x0 = x0 < 0 ? x0 + w : (x0 >= w ? x0 - w : x0);
+    x1 = x1 < 0 ? x1 + w : (x1 >= w ? x1 - w : x1);
+    y0 = y0 < 0 ? y0 + h : (y0 >= h ? y0 - h : y0);
+    y1 = y1 < 0 ? y1 + h : (y1 >= h ? y1 - h : y1);
+    float4 t00 = texel_rgba8(__ldg(img + size_t(y0) * w + x0)), t10 = texel_rgba8(__ldg(img + size_t(y0) * w + x1));
+    float4 t01 = texel_rgba8(__ldg(img + size_t(y1) * w + x0)), t11 = texel_rgba8(__ldg(img + size_t(y1) * w + x1));
+    float4 r;
+    r.x = mixf(mixf(t00.x, t10.x, a), mixf(t01.x, t11.x, a), b);
+    r.y = mixf(mixf(t00.y, t10.y, a), mixf(t01.y, t11.y, a), b);
+    r.z = mixf(mixf(t00.z, t10.z, a), mixf(t01.z, t11.z, a), b);
+    r.w = mixf(mixf(t00.w, t10.w, a), mixf(t01.w, t11.w, a), b);
+    return r;
+}
+RT_D float4 tex_lookup(const SceneView& sc, int id, float u, float v) {
+    int4 info = __ldg(sc.tex_info + id);
+    return tex_rgba8(sc.tex + info.x, info.y, info.z, u, v);
+}
+
+// NormalFromTangentToWorld, core/cuda/Utils.h:85-94.
+RT_D v3 normal_from_tangent(v3 n, v3 t) {
+    t = normalize(t * 2.0f - v3(1.0f));
+    v3 up = fabsf(n.z) < 0.9f ? v3(0.0f, 0.0f, 1.0f) : v3(1.0f, 0.0f, 0.0f);
+    v3 tx = normalize(cross(up, n));
+    v3 ty = normalize(cross(n, tx));
+    return normalize(tx * t.x + ty * t.y + n * t.z);
 }
 
 // ------------------------------------------------------------ filter

@@ -195,8 +195,9 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
 // every lane traverses its own ray one wide node at a time; when enough lanes
 // of a warp have finished, they take new rays from the queue with a single
 // warp-aggregated atomicAdd, so a warp never waits for its slowest ray while
-// work remains.  `src.load(i, ray, scene)` fetches queue entry i and
-// `src.finish(i, tri, t, b1, b2)` stores its result.
+// work remains.  `src.load(i, ray, scene)` fetches queue entry i;
+// `src.finish(fin, i, tri, t, b1, b2, tri_v)` is called by the whole warp after
+// every step and stores the result of the lanes whose `fin` is set.
 constexpr int kRefillLanes = 12;
 
 struct TravState {
@@ -255,6 +256,7 @@ RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& node
     int item = -1;
     bool active = false, exhausted = false;
     while (true) {
+        bool fin = false;
         unsigned idle = __ballot_sync(0xffffffffu, !active);
         if (!exhausted && idle && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
             int leader = __ffs(idle) - 1;
@@ -276,22 +278,20 @@ RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& node
                     s.sp = 0;
                     s.g = make_uint2(0u, 1u << (24 + s.r.oct));
                     rays++;
-                    if (sc->num_nodes > 0) {
+                    if (sc->num_nodes > 0)
                         active = true;
-                    } else {
-                        src.finish(item, -1, 0.0f, 0.0f, 0.0f);
-                    }
+                    else
+                        fin = true;  // empty scene: a miss
                 }
             }
         }
-        if (__ballot_sync(0xffffffffu, active) == 0) {
-            if (exhausted) break;
-            continue;
-        }
         if (active && trav_step<AnyHit, Stats>(s, stack, nodes_visited, tris_tested)) {
-            src.finish(item, s.hit, s.t, s.b1, s.b2);
+            fin = true;
             active = false;
         }
+        // called by the whole warp; lanes with `fin` store their result
+        src.finish(fin, item, s.hit, s.t, s.b1, s.b2, s.tri_v);
+        if (__ballot_sync(0xffffffffu, active) == 0 && exhausted) break;
     }
 }
 

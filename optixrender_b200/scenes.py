@@ -23,7 +23,7 @@ from typing import Optional
 
 import numpy as np
 
-from . import (FILTER_GAUSSIAN, LIGHT_QUAD, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_DIFFUSE, MAT_PLASTIC,
+from . import (FILTER_GAUSSIAN, LIGHT_QUAD, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_DIFFUSE, MAT_METAL_WORKFLOW, MAT_PLASTIC,
                MEDIUM_GRID, MEDIUM_HOMOGENEOUS, PHASE_HG, PHASE_ISOTROPIC, RNG_PCG32, Renderer, Scene, camera,
                light, material, medium, options)
 
@@ -35,12 +35,23 @@ class MeshSpec:
     material: dict
     out_medium: int = -1
     in_medium: int = -1
+    normals: Optional[np.ndarray] = None     # (n, 3) per vertex, or None (face normals)
+    texcoords: Optional[np.ndarray] = None   # (n, 2) per vertex, or None
+
+    def _deindex(self, a, k):
+        if self.indices is None:
+            return np.ascontiguousarray(a.reshape(-1, 3 * k), dtype=np.float32)
+        return np.ascontiguousarray(a[self.indices].reshape(-1, 3 * k), dtype=np.float32)
 
     def triangles(self) -> np.ndarray:
         """(m, 9) float32 de-indexed vertex positions."""
-        if self.indices is None:
-            return np.ascontiguousarray(self.positions.reshape(-1, 9), dtype=np.float32)
-        return np.ascontiguousarray(self.positions[self.indices].reshape(-1, 9), dtype=np.float32)
+        return self._deindex(self.positions, 3)
+
+    def tri_normals(self):
+        return None if self.normals is None else self._deindex(self.normals, 3)
+
+    def tri_texcoords(self):
+        return None if self.texcoords is None else self._deindex(self.texcoords, 2)
 
 
 @dataclass
@@ -52,6 +63,7 @@ class SceneSpec:
     env: Optional[np.ndarray] = None                # (h, w, 4) float32
     camera: dict = field(default_factory=dict)
     settings: dict = field(default_factory=dict)    # options() keywords
+    textures: list = field(default_factory=list)    # (h, w, 4) uint8, row 0 at v = 0
 
     @property
     def num_triangles(self):
@@ -218,6 +230,69 @@ def cornell(width=256, height=256, spp=16, seed=1):
     return SceneSpec("cornell", meshes, lights, [], None, cam, settings)
 
 
+def textured(width=128, height=128, spp=16, seed=1):
+    """The Cornell room with material textures: a checker albedo on the floor
+    (uv repeated 3x, wrap), a bump normal map on the back wall, a roughness
+    ramp on the conductor box and albedo + metallic maps on a metal-workflow
+    panel.  Every mesh carries per-vertex normals and texcoords."""
+    rng = np.random.default_rng(seed + 17)
+    n = 64
+    yy, xx = np.mgrid[0:n, 0:n]
+    checker = np.where(((xx // 8) + (yy // 8)) % 2 == 0, 0, 1)[..., None]
+    albedo_tex = np.where(checker == 0, np.uint8([200, 190, 170, 255]), np.uint8([40, 70, 140, 255])).astype(np.uint8)
+    ramp = np.zeros((32, 32, 4), np.uint8)
+    ramp[..., 0] = np.linspace(60, 230, 32, dtype=np.float64)[None, :].round().astype(np.uint8)
+    ramp[..., 3] = 255
+    # normal map: height field h = 0.15 sin(2pi x/16) sin(2pi y/16), n = normalize(-dh/dx, -dh/dy, 1)
+    ph = 2 * np.pi / 16.0
+    dhdx = 0.15 * ph * np.cos(ph * xx) * np.sin(ph * yy) * 8
+    dhdy = 0.15 * ph * np.sin(ph * xx) * np.cos(ph * yy) * 8
+    nrm = np.stack([-dhdx, -dhdy, np.ones_like(dhdx)], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    normal_tex = np.concatenate([np.clip((nrm * 0.5 + 0.5) * 255 + 0.5, 0, 255).astype(np.uint8),
+                                 np.full((n, n, 1), 255, np.uint8)], -1)
+    metal_tex = np.zeros((16, 16, 4), np.uint8)
+    metal_tex[..., 0] = rng.integers(0, 256, (16, 16))
+    metal_tex[..., 3] = 255
+    textures = [albedo_tex, ramp, normal_tex, metal_tex]
+
+    def tquad(p, u, v, mat, uv_scale=1.0):
+        verts, f = quad(p, u, v)
+        nr = np.cross(np.asarray(u, np.float64), np.asarray(v, np.float64))
+        nr = np.tile((nr / np.linalg.norm(nr)).astype(np.float32), (4, 1))
+        uv = np.float32([[0, 0], [1, 0], [1, 1], [0, 1]]) * uv_scale
+        return MeshSpec(verts, f, mat, normals=nr, texcoords=uv)
+
+    white = dict(type=MAT_DIFFUSE, albedo=(0.73, 0.73, 0.73), roughness=0.0)
+    floor = dict(type=MAT_DIFFUSE, albedo=(0.5, 0.5, 0.5), roughness=0.0, texture_ids=[0])
+    back = dict(type=MAT_DIFFUSE, albedo=(0.73, 0.73, 0.73), roughness=0.0, texture_ids=[-1] * 7 + [2])
+    red = dict(type=MAT_DIFFUSE, albedo=(0.65, 0.05, 0.05), roughness=0.0)
+    green = dict(type=MAT_DIFFUSE, albedo=(0.12, 0.45, 0.15), roughness=0.0)
+    copper = dict(type=MAT_CONDUCTOR, albedo=(1.0, 1.0, 1.0), roughness=0.2, texture_ids=[-1, 1])
+    panel = dict(type=MAT_METAL_WORKFLOW, albedo=(0.8, 0.8, 0.8), roughness=0.3, texture_ids=[0, -1, -1, -1, 3])
+    meshes = [tquad((0, 0, 0), (1, 0, 0), (0, 0, 1), floor, 3.0),
+              tquad((0, 1, 0), (0, 0, 1), (1, 0, 0), white),
+              tquad((0, 0, 1), (1, 0, 0), (0, 1, 0), back, 2.0),
+              tquad((0, 0, 0), (0, 0, 1), (0, 1, 0), red),
+              tquad((1, 0, 0), (0, 1, 0), (0, 0, 1), green),
+              tquad((0.1, 0.05, 0.35), (0.35, 0.0, -0.1), (0.0, 0.45, 0.1), panel)]
+    v, f = box((0.55, 0.0, 0.45), (0.85, 0.6, 0.75))
+    # de-indexed box with face normals and planar texcoords (x + y, z)
+    tv = v[f.reshape(-1)]
+    e1, e2 = tv[1::3] - tv[0::3], tv[2::3] - tv[0::3]
+    fn = np.cross(e1, e2)
+    fn /= np.linalg.norm(fn, axis=1, keepdims=True)
+    bn = np.repeat(fn, 3, axis=0).astype(np.float32)
+    buv = np.stack([(tv[:, 0] - 0.55) / 0.3 + tv[:, 1], (tv[:, 2] - 0.45) / 0.3], -1).astype(np.float32)
+    meshes.append(MeshSpec(tv.astype(np.float32), None, copper, normals=bn, texcoords=buv))
+    lights = [dict(type=LIGHT_QUAD, position=(0.375, 0.999, 0.375), u=(0.0, 0.0, 0.25), v=(0.25, 0.0, 0.0),
+                   radiance=(17.0, 12.0, 4.0), double_side=0)]
+    cam = dict(from_=(0.5, 0.5, -1.6), at=(0.5, 0.5, 0.5), up=(0, 1, 0))
+    settings = dict(width=width, height=height, spp=spp, max_depth=8, rr_depth=3, rng=RNG_PCG32, seed=seed,
+                    filter=FILTER_GAUSSIAN)
+    return SceneSpec("textured", meshes, lights, [], None, cam, settings, textures)
+
+
 def spheres(width=1920, height=1080, spp=64, seed=1, ico_level=8, sphere_tris=True, env_size=(2048, 1024)):
     rng = np.random.default_rng(seed)
     v, f = icosphere(ico_level)
@@ -307,9 +382,11 @@ def _material_obj(d):
 def build_scene(spec: SceneSpec) -> Scene:
     """A CUDA-library Scene holding the spec's meshes, lights, media and sky."""
     s = Scene()
+    for t in spec.textures:
+        s.add_texture(t)
     for m in spec.meshes:
-        s.add_mesh(m.positions, _material_obj(m.material), indices=m.indices, out_medium=m.out_medium,
-                   in_medium=m.in_medium)
+        s.add_mesh(m.positions, _material_obj(m.material), indices=m.indices, normals=m.normals,
+                   texcoords=m.texcoords, out_medium=m.out_medium, in_medium=m.in_medium)
     for l in spec.lights:
         s.add_light(light(**l))
     for md in spec.media:
@@ -328,4 +405,4 @@ def build_renderer(spec: SceneSpec, **overrides) -> tuple:
     return s, r
 
 
-SCENES = {"cornell": cornell, "spheres": spheres, "media": media}
+SCENES = {"cornell": cornell, "spheres": spheres, "media": media, "textured": textured}

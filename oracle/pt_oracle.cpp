@@ -21,6 +21,9 @@ template <class R>
 struct Scene {
     const float* tv = nullptr;
     const float* tn = nullptr;
+    const float* tuv = nullptr;
+    const uint32_t* tex = nullptr;      // all textures' texels
+    const int32_t* tex_info = nullptr;  // offset, width, height per texture
     const int32_t* tri_mesh = nullptr;
     int64_t ntri = 0;
     std::vector<Mat<R>> mats;
@@ -38,6 +41,8 @@ struct Scene {
 
 struct SceneHandle {
     std::vector<float> tv, tn, tuv;
+    std::vector<uint32_t> tex;
+    std::vector<int32_t> tex_info;
     std::vector<int32_t> tri_mesh;
     int64_t ntri = 0;
     std::vector<rt_material> mats;
@@ -90,6 +95,9 @@ Scene<R>* make_scene(SceneHandle* h) {
     s->env_h = h->env_h;
     s->tv = h->tv.data();
     s->tn = h->tn.data();
+    s->tuv = h->tuv.data();
+    s->tex = h->tex.empty() ? nullptr : h->tex.data();
+    s->tex_info = h->tex_info.empty() ? nullptr : h->tex_info.data();
     s->tri_mesh = h->tri_mesh.data();
     s->env = h->env.empty() ? nullptr : h->env.data();
     s->cache = h->cache.empty() ? nullptr : h->cache.data();
@@ -161,6 +169,7 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
     R pre_pdf = R(0), mult_trans_pdf = R(1), trans_pdf = R(1);
     V3<R> transmittance(R(0));
     Isect<R> it;
+    Mat<R> tex_mat;  // the textured copy of the last hit's material
     it.distance = FMAX;
     it.position = o;
     it.sn = V3<R>(R(0));
@@ -185,12 +194,33 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
             const float* vv = tv + size_t(p) * 9;
             R w0 = R(1) - u - v;
             V3<R> Ns = normalize(w0 * from3<R>(nn) + u * from3<R>(nn + 3) + v * from3<R>(nn + 6));
-            V3<R> P = w0 * from3<R>(vv) + u * from3<R>(vv + 3) + v * from3<R>(vv + 6);
             int mesh = sc.tri_mesh[size_t(p)];
+            const Mat<R>* mat = &sc.mats[size_t(mesh)];
+            if (mat->textured) {  // texture overrides, devicePrograms.cu:89-115
+                const float* uv = sc.tuv + size_t(p) * 6;
+                R tcx = w0 * R(uv[0]) + u * R(uv[2]) + v * R(uv[4]);
+                R tcy = w0 * R(uv[1]) + u * R(uv[3]) + v * R(uv[5]);
+                tex_mat = *mat;
+                R t4[4];
+                auto fetch = [&](int slot) {
+                    const int32_t* ti = sc.tex_info + 3 * mat->tex[slot];
+                    tex_rgba8(sc.tex + ti[0], ti[1], ti[2], tcx, tcy, t4);
+                };
+                if (mat->tex[0] >= 0) fetch(0), tex_mat.albedo = V3<R>(t4[0], t4[1], t4[2]);
+                if (mat->tex[1] >= 0) fetch(1), tex_mat.roughness = t4[0];
+                if (mat->tex[2] >= 0) fetch(2), tex_mat.anisotropy = t4[0];
+                if (mat->tex[3] >= 0) fetch(3), tex_mat.specular = V3<R>(t4[0], t4[1], t4[2]);
+                if (mat->tex[4] >= 0) fetch(4), tex_mat.metallic = t4[0];
+                if (mat->tex[5] >= 0) fetch(5), tex_mat.cru = t4[0];
+                if (mat->tex[6] >= 0) fetch(6), tex_mat.crv = t4[0];
+                if (mat->tex[7] >= 0) fetch(7), Ns = normal_from_tangent(Ns, V3<R>(t4[0], t4[1], t4[2]));
+                mat = &tex_mat;
+            }
+            V3<R> P = w0 * from3<R>(vv) + u * from3<R>(vv + 3) + v * from3<R>(vv + 6);
             it.set_face_normal(d, Ns);
             it.distance = length(P - it.position);
             it.position = P;
-            it.mat = &sc.mats[size_t(mesh)];
+            it.mat = mat;
             it.in_medium = sc.mesh_in[size_t(mesh)];
             it.out_medium = sc.mesh_out[size_t(mesh)];
             if (first) {
@@ -578,6 +608,17 @@ extern "C" {
 // ntri*9 positions, optional ntri*9 normals (NULL: face normals as in
 // Scene.cpp:150-158), optional ntri*6 texcoords, a mesh index per triangle,
 // one material and (out, in) medium pair per mesh.
+// Material textures: `texels` holds every texture's RGBA8 texels (row 0 at
+// v = 0), `info` offset / width / height per texture.  Call before the
+// first render.
+void orc_scene_set_textures(void* hp, const uint32_t* texels, int64_t ntexels, const int32_t* info, int32_t ntex) {
+    SceneHandle* h = static_cast<SceneHandle*>(hp);
+    h->tex.assign(texels, texels + ntexels);
+    h->tex_info.assign(info, info + 3 * ntex);
+    h->sf.reset(make_scene<float>(h));
+    h->sd.reset(make_scene<double>(h));
+}
+
 void* orc_scene_new(const float* tri_v, const float* tri_n, const float* tri_uv, const int32_t* tri_mesh, int64_t ntri,
                     const rt_material* mesh_mats, const int32_t* mesh_media, int32_t n_mesh, const rt_light* lights,
                     int32_t nl, const rt_medium* media, int32_t nm, const float* env_rgba, int32_t env_w, int32_t env_h) {

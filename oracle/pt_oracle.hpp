@@ -412,8 +412,15 @@ template <class R> struct Mat {
     V3<R> albedo, eta, k, specular;
     R roughness, anisotropy, int_ior, ext_ior, metallic, coat_weight, cru, crv;
     bool nonlinear;
+    int tex[8];      // texture ids (-1 = constant), rt_material.texture_ids order
+    bool textured;
     void set(const rt_material& m) {
         type = m.type;
+        textured = false;
+        for (int t = 0; t < 8; t++) {
+            tex[t] = m.texture_ids[t];
+            textured = textured || tex[t] >= 0;
+        }
         albedo = from3<R>(m.albedo);
         eta = from3<R>(m.eta);
         k = from3<R>(m.k);
@@ -1360,6 +1367,39 @@ template <class R> inline void tex_bilinear(const float* img, int w, int h, R u,
         out[c] = mixr(mixr(t00, t10, a), mixr(t01, t11, a), b);
     }
 }
+// tex2D<float4> of an RGBA8 material texture (core/src/Renderer.cpp:100-143:
+// uchar4 texels read as normalized floats, normalized coordinates, wrap
+// addressing, linear filtering), evaluated with float weights on texels
+// converted as byte * (1/255).
+template <class R> inline void tex_rgba8(const uint32_t* img, int w, int h, R u, R v, R out[4]) {
+    u = u - std::floor(u);
+    v = v - std::floor(v);
+    R x = u * R(w) - R(0.5f), y = v * R(h) - R(0.5f);
+    R fx = std::floor(x), fy = std::floor(y);
+    R a = x - fx, b = y - fy;
+    int x0 = int(fx), y0 = int(fy);
+    int x1 = x0 + 1, y1 = y0 + 1;
+    x0 = ((x0 % w) + w) % w;
+    x1 = ((x1 % w) + w) % w;
+    y0 = ((y0 % h) + h) % h;
+    y1 = ((y1 % h) + h) % h;
+    const uint32_t p00 = img[size_t(y0) * w + x0], p10 = img[size_t(y0) * w + x1];
+    const uint32_t p01 = img[size_t(y1) * w + x0], p11 = img[size_t(y1) * w + x1];
+    for (int c = 0; c < 4; ++c) {
+        auto texel = [c](uint32_t px) { return R(float((px >> (8 * c)) & 0xFFu) * (1.0f / 255.0f)); };
+        out[c] = mixr(mixr(texel(p00), texel(p10), a), mixr(texel(p01), texel(p11), a), b);
+    }
+}
+
+// NormalFromTangentToWorld, core/cuda/Utils.h:85-94.
+template <class R> inline V3<R> normal_from_tangent(const V3<R>& n, V3<R> t) {
+    t = normalize(t * R(2) - V3<R>(R(1)));
+    V3<R> up = std::abs(n.z) < R(0.9f) ? V3<R>(R(0), R(0), R(1)) : V3<R>(R(1), R(0), R(0));
+    V3<R> tx = normalize(cross(up, n));
+    V3<R> ty = normalize(cross(n, tx));
+    return normalize(tx * t.x + ty * t.y + n * t.z);
+}
+
 // HdrTexture::CalculateHdrCache, core/src/Scene.cpp:217-313 (float
 // arithmetic in the same order; the marginal index is clamped to width-1
 // where the reference would read past the table).

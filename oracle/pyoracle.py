@@ -30,6 +30,7 @@ def load():
         _lib.orc_scene_new.argtypes = [P(F), P(F), P(F), P(I32), I64, VP, P(I32), I32, VP, I32, VP, I32, P(F), I32,
                                        I32]
         _lib.orc_scene_free.argtypes = [VP]
+        _lib.orc_scene_set_textures.argtypes = [VP, P(C.c_uint32), I64, P(I32), I32]
         _lib.orc_render.restype = I32
         _lib.orc_render.argtypes = [VP, I32, VP, VP, I32, P(F), P(F), P(F), P(I64), I32, I32, I32]
         _lib.orc_camera.argtypes = [VP, I32, I32, P(F)]
@@ -47,6 +48,24 @@ def _f(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+def _normalize(v):
+    """float32 normalize with the library's operation order: v / sqrt((x*x + y*y) + z*z)."""
+    v = v.astype(np.float32)
+    x, y, z = v[..., 0], v[..., 1], v[..., 2]
+    ln = np.sqrt((x * x + y * y) + z * z)
+    return v / ln[..., None]
+
+
+def _face_normals(tris):
+    """Per-vertex face normals of de-indexed triangles (m, 9), as rt_scene_add_mesh computes them."""
+    t = tris.reshape(-1, 3, 3).astype(np.float32)
+    e1, e2 = _normalize(t[:, 1] - t[:, 0]), _normalize(t[:, 2] - t[:, 0])
+    c = np.stack([e1[:, 1] * e2[:, 2] - e2[:, 1] * e1[:, 2], e1[:, 2] * e2[:, 0] - e2[:, 2] * e1[:, 0],
+                  e1[:, 0] * e2[:, 1] - e2[:, 0] * e1[:, 1]], -1)
+    n = _normalize(c)
+    return np.repeat(n, 3, axis=0).reshape(-1, 9)
+
+
 class OracleScene:
     """The oracle's copy of a SceneSpec (optixrender_b200.scenes)."""
 
@@ -54,15 +73,27 @@ class OracleScene:
         import optixrender_b200 as rt
         lib = load()
         tris, tmesh = [], []
+        tnorm, tuv = [], []
         mats = []
         media_pairs = []
         for i, m in enumerate(spec.meshes):
             t = m.triangles()
             tris.append(t)
+            tn = m.tri_normals()
+            tnorm.append(None if tn is None else _normalize(tn.reshape(-1, 3)).reshape(-1, 9))
+            tuv.append(m.tri_texcoords())
             tmesh.append(np.full(t.shape[0], i, np.int32))
             mats.append(rt.material(**m.material))
             media_pairs += [m.out_medium, m.in_medium]
         self.tv = np.ascontiguousarray(np.concatenate(tris), np.float32)
+        self.tn = self.tuv = None
+        if any(n is not None for n in tnorm):
+            self.tn = np.ascontiguousarray(np.concatenate(
+                [n if n is not None else _face_normals(t) for n, t in zip(tnorm, tris)]), np.float32)
+        if any(u is not None for u in tuv):
+            self.tuv = np.ascontiguousarray(np.concatenate(
+                [u if u is not None else np.tile(np.float32([0, 0, 1, 0, 0, 1]), (t.shape[0], 1))
+                 for u, t in zip(tuv, tris)]), np.float32)
         self.tmesh = np.ascontiguousarray(np.concatenate(tmesh), np.int32)
         self.mats = (rt.Material * len(mats))(*mats)
         self.mm = np.asarray(media_pairs, np.int32)
@@ -71,11 +102,24 @@ class OracleScene:
         env = spec.env
         self.env = None if env is None else np.ascontiguousarray(env, np.float32)
         eh, ew = (0, 0) if env is None else env.shape[:2]
-        self.h = lib.orc_scene_new(_f(self.tv), None, None, self.tmesh.ctypes.data_as(C.POINTER(C.c_int32)),
+        self.h = lib.orc_scene_new(_f(self.tv), None if self.tn is None else _f(self.tn),
+                                   None if self.tuv is None else _f(self.tuv),
+                                   self.tmesh.ctypes.data_as(C.POINTER(C.c_int32)),
                                    self.tv.shape[0], C.cast(self.mats, C.c_void_p),
                                    self.mm.ctypes.data_as(C.POINTER(C.c_int32)), len(mats),
                                    C.cast(self.lights, C.c_void_p), len(spec.lights), C.cast(self.media, C.c_void_p),
                                    len(spec.media), None if env is None else _f(self.env), ew, eh)
+        if spec.textures:
+            texels, info, off = [], [], 0
+            for t in spec.textures:
+                a = np.ascontiguousarray(t, np.uint8)
+                texels.append(a.view(np.uint32).reshape(-1))
+                info += [off, a.shape[1], a.shape[0]]
+                off += a.shape[0] * a.shape[1]
+            self.texels = np.ascontiguousarray(np.concatenate(texels))
+            self.tex_info = np.asarray(info, np.int32)
+            lib.orc_scene_set_textures(self.h, self.texels.ctypes.data_as(C.POINTER(C.c_uint32)), self.texels.size,
+                                       self.tex_info.ctypes.data_as(C.POINTER(C.c_int32)), len(spec.textures))
         self.spec = spec
 
     def close(self):

@@ -1,0 +1,145 @@
+"""The continuous-batching render server (rt_server_*).
+
+Each job draws PCG32 streams keyed by (seed, path index) and sums every
+pixel's samples in sample order, so a job's image must be bit-identical to a
+Renderer::Render() with the same settings, whichever jobs shared its waves and
+however its paths were split across waves.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import optixrender_b200 as rt
+from optixrender_b200 import scenes
+
+
+def _specs():
+    return [
+        scenes.cornell(64, 48, 6, seed=7),
+        scenes.spheres(80, 45, 3, seed=3, ico_level=5, env_size=(256, 128)),
+        scenes.media(48, 40, 4, seed=5, grid_res=16, env_size=(256, 128)),
+    ]
+
+
+def _job_for(spec, scene_id, **over):
+    st = dict(spec.settings)
+    st.update(over)
+    return rt.job(scene_id, rt.camera(**spec.camera), st["width"], st["height"], st["spp"],
+                  max_depth=st["max_depth"], rr_depth=st["rr_depth"], filter=st.get("filter", rt.FILTER_BOX),
+                  tonemap=st.get("tonemap", rt.TONEMAP_REINHARD), seed=st["seed"])
+
+
+def _alone(spec, **over):
+    st = dict(spec.settings)
+    st.update(over)
+    st.setdefault("filter", rt.FILTER_BOX)
+    s, r = scenes.build_renderer(spec, **st)
+    r.render()
+    return r.download_linear(), r.download_pixels()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wave_paths,policy", [(4096, rt.SERVE_FAIR), (1 << 16, rt.SERVE_FAIR),
+                                               (4096, rt.SERVE_FIFO)])
+def test_jobs_in_a_mix_match_renders_alone_bitwise(wave_paths, policy):
+    specs = _specs()
+    srv = rt.Server(rt.server_options(wave_paths=wave_paths, max_jobs=8, max_depth=32, policy=policy))
+    keep = [scenes.build_scene(sp) for sp in specs]
+    ids = [srv.add_scene(s) for s in keep]
+    jobs = []
+    for rep in range(2):  # each scene twice, second time with another seed
+        for sp, sid in zip(specs, ids):
+            jobs.append((sp, rep, srv.submit(_job_for(sp, sid, seed=sp.settings["seed"] + rep))))
+    for sp, rep, jid in jobs:
+        st = srv.wait(jid, 120000.0)
+        assert st["state"] == rt.JOB_DONE
+        assert st["done_ms"] >= st["admit_ms"] >= st["submit_ms"]
+    stats = srv.stats()
+    print(stats)
+    assert stats["jobs_done"] == len(jobs)
+    assert stats["paths"] == sum(sp.settings["width"] * sp.settings["height"] * sp.settings["spp"]
+                                 for sp, _, _ in jobs)
+    assert stats["max_segments_in_a_wave"] >= 2  # jobs really shared waves
+    for sp, rep, jid in jobs:
+        lin, px = _alone(sp, seed=sp.settings["seed"] + rep)
+        got = srv.download(jid)
+        assert np.array_equal(got.view(np.uint32), lin.view(np.uint32)), sp.name
+        assert np.array_equal(srv.download_pixels(jid), px)
+        srv.release(jid)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_manual_mode_admits_within_the_memory_budget():
+    """With room for one job's buffers, jobs run one at a time; a finished job
+    holds its memory until it is released."""
+    spec = scenes.cornell(100, 100, 2, seed=11)
+    job_bytes = 100 * 100 * 104
+    srv = rt.Server(rt.server_options(background=0, hbm_budget_bytes=int(1.5 * job_bytes),
+                                      wave_paths=1 << 14, max_depth=8))
+    scene = scenes.build_scene(spec)
+    sid = srv.add_scene(scene)
+    ids = [srv.submit(_job_for(spec, sid, seed=20 + i)) for i in range(4)]
+    most_running = 0
+    images = {}
+    while srv.step():
+        st = srv.stats()
+        most_running = max(most_running, st["jobs_running"])
+        assert st["bytes_in_use"] <= st["bytes_budget"]
+        for i, jid in enumerate(ids):
+            if i not in images and srv.poll(jid)["state"] == rt.JOB_DONE:
+                images[i] = srv.download(jid)
+                srv.release(jid)
+    assert most_running == 1 and len(images) == 4
+    for i in range(4):
+        lin, _ = _alone(spec, seed=20 + i)
+        assert np.array_equal(images[i].view(np.uint32), lin.view(np.uint32))
+    srv.close()
+
+    # an unreleased finished job blocks the next one: waiting on it reports why
+    srv = rt.Server(rt.server_options(background=0, hbm_budget_bytes=int(1.5 * job_bytes),
+                                      wave_paths=1 << 14, max_depth=8))
+    sid = srv.add_scene(scene)
+    a, b = srv.submit(_job_for(spec, sid)), srv.submit(_job_for(spec, sid))
+    assert srv.wait(a)["state"] == rt.JOB_DONE
+    with pytest.raises(rt.RTError) as e:
+        srv.wait(b)
+    assert e.value.code == rt.RT_ERR_STATE
+    srv.release(a)
+    assert srv.wait(b)["state"] == rt.JOB_DONE
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_submit_errors_cancel_and_timeout():
+    spec = scenes.cornell(32, 32, 1)
+    srv = rt.Server(rt.server_options(background=0, hbm_budget_bytes=8 << 20, max_depth=8))
+    sid = srv.add_scene(scenes.build_scene(spec))
+    with pytest.raises(rt.RTError) as e:
+        srv.submit(_job_for(spec, sid, width=4096, height=4096))  # over the budget alone
+    assert e.value.code == rt.RT_ERR_OUT_OF_MEMORY
+    with pytest.raises(rt.RTError):
+        srv.submit(_job_for(spec, sid, max_depth=9))  # deeper than the server's launches
+    with pytest.raises(rt.RTError):
+        srv.submit(_job_for(spec, sid + 1))
+    a = srv.submit(_job_for(spec, sid))
+    b = srv.submit(_job_for(spec, sid))
+    srv.cancel(b)
+    assert srv.poll(b)["state"] == rt.JOB_CANCELLED
+    with pytest.raises(rt.RTError):
+        srv.download(a)  # not run yet
+    assert srv.wait(a)["state"] == rt.JOB_DONE
+    srv.release(a)
+    srv.release(b)
+    srv.close()
+
+    bg = rt.Server(rt.server_options(max_depth=8))
+    sid = bg.add_scene(scenes.build_scene(scenes.cornell(32, 32, 1)))
+    big = bg.submit(_job_for(spec, sid, width=512, height=512, spp=64))
+    t = time.perf_counter()
+    with pytest.raises(rt.RTError) as e:
+        bg.wait(big, 0.0)
+    assert e.value.code == rt.RT_ERR_TIMEOUT and time.perf_counter() - t < 1.0
+    assert bg.wait(big, 120000.0)["state"] == rt.JOB_DONE
+    bg.close()
