@@ -317,6 +317,23 @@ RT_API rt_status rt_renderer_frame_index(const rt_renderer* r, int32_t* frame);
 RT_API rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
                                    int32_t device_ptrs);
 
+/* rt_renderer_trace with host buffers, for callers that must not allocate
+ * device memory during the call (no counterpart in the reference).
+ * cudaMalloc and cudaFree, which rt_renderer_trace uses for its per-call
+ * buffers, can synchronise the whole device, stalling a render or serving
+ * loop's other streams, and they fail once the caller has taken the remaining
+ * device memory for its own pool.  This call allocates nothing: the rays and
+ * hits pass through one fixed device array per device (65,536 rays, 3 MiB),
+ * and larger batches are rejected with RT_ERR_INVALID_ARG.  Nothing in the
+ * array needs to start at zero.  The first call on each device looks up the
+ * array's address (cudaGetSymbolAddress); make that first call outside any
+ * stream capture.  Calls on one device share the array: calls that overlap
+ * in time (several host threads, or several renderers on one device) race on
+ * it and may return each other's hits, so serialise them.  Returns after the
+ * hits are in `hits` (the renderer's stream is synchronised). */
+RT_API rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n,
+                                           float* hits);
+
 /* ---------------------------------------------------------------------- */
 /* Serving: many render jobs batched into shared wavefront launches         */
 /* (no counterpart in the reference, which renders one frame at a time).    */

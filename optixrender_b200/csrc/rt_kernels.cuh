@@ -125,4 +125,8 @@ void launch_finalize_n(const rtd::JobDesc* dev_job, int64_t npix, cudaStream_t s
 void launch_trace(const rtd::SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st);
 void launch_verify(int op, const rtd::SceneView& sc, const rtd::DevLight* lights, const rtd::DevMedium* media,
                    const float* in, int64_t n, float* out, cudaStream_t st);
+// rt_trace_scratch.cu: ray queries staged in a fixed device array.
+int64_t trace_scratch_rays();
+cudaError_t trace_scratch_address(void** ptr);
+void launch_trace_scratch(const rtd::SceneView& sc, bool any_hit, void* scratch, int n, cudaStream_t st);
 }  // namespace rth

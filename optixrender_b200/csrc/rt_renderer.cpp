@@ -649,6 +649,29 @@ rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, 
     return RT_OK;
 }
 
+// Same queries as rt_renderer_trace with host buffers, staged in the fixed
+// device array of rt_trace_scratch.cu instead of buffers allocated per call.
+rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits) {
+    if (!r || n < 0 || (n > 0 && (!rays || !hits)))
+        return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace_noalloc: bad argument");
+    const int64_t cap = rth::trace_scratch_rays();
+    if (n > cap)
+        return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace_noalloc: " + std::to_string(n) + " rays exceed the " +
+                                            std::to_string(cap) +
+                                            " of the static scratch; split the batch or use rt_renderer_trace");
+    if (n == 0) return RT_OK;
+    void* scratch = nullptr;
+    RT_CUDA(rth::trace_scratch_address(&scratch), "rt_renderer_trace_noalloc: scratch address");
+    float4* sc = static_cast<float4*>(scratch);
+    RT_CUDA(cudaMemcpyAsync(sc, rays, size_t(n) * 32, cudaMemcpyHostToDevice, r->stream), "rt_renderer_trace_noalloc");
+    rth::launch_trace_scratch(r->ds.view, any_hit != 0, scratch, int(n), r->stream);
+    RT_CUDA(cudaGetLastError(), "rt_renderer_trace_noalloc");
+    RT_CUDA(cudaMemcpyAsync(hits, sc + 2 * cap, size_t(n) * 16, cudaMemcpyDeviceToHost, r->stream),
+            "rt_renderer_trace_noalloc");
+    RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace_noalloc");
+    return RT_OK;
+}
+
 rt_status rt_verify_shading(int32_t op, const rt_material* materials, int32_t nmat, const rt_light* lights, int32_t nl,
                             const rt_medium* media, int32_t nm, const float* in, int64_t n, float* out) {
     if (!in || !out || n < 0) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: bad argument");
