@@ -335,6 +335,45 @@ RT_API rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, cons
                                            float* hits);
 
 /* ---------------------------------------------------------------------- */
+/* Path-guiding network (no counterpart in the reference): a multiresolution */
+/* hash encoding of the position (16 levels x 2 features, 2^19 entries per   */
+/* level) feeding a 32-64-64-64-32 MLP (FP16 weights, FP32 accumulation)      */
+/* whose outputs are an 8-lobe von Mises-Fisher mixture over directions.     */
+/* These calls expose the network on host buffers; the renderer trains and   */
+/* queries it on device buffers when rt_options.guided is set.               */
+/* ---------------------------------------------------------------------- */
+
+typedef struct rt_guide rt_guide;
+
+typedef struct rt_guide_options {
+    float learning_rate;       /* Adam step size (1e-2) */
+    int32_t pad;
+    uint64_t seed;             /* parameter initialisation */
+} rt_guide_options;
+
+RT_API void rt_guide_options_default(rt_guide_options* o);
+RT_API rt_status rt_guide_create(const rt_guide_options* o, rt_guide** out);
+RT_API rt_status rt_guide_destroy(rt_guide* g);
+/* Parameter counts: hash table (levels x 2^19 x 2 floats, level-major) and MLP
+ * (W0 64x32, W1 64x64, W2 64x64, W3 32x64, each row-major [out][in]). */
+RT_API void rt_guide_sizes(int64_t* table_params, int64_t* mlp_params);
+RT_API rt_status rt_guide_get_params(const rt_guide* g, float* table, float* mlp);
+RT_API rt_status rt_guide_set_params(rt_guide* g, const float* table, const float* mlp);
+/* Raw outputs (n x 32) of positions in [0,1]^3 (n x 3). */
+RT_API rt_status rt_guide_forward(rt_guide* g, const float* pos, int64_t n, float* raw);
+/* Loss (1/n) sum_i -weight_i log q(dir_i | pos_i) and its gradients (the
+ * gradients are not applied). */
+RT_API rt_status rt_guide_gradients(rt_guide* g, const float* pos, const float* dir, const float* weight, int64_t n,
+                                    float* loss, float* grad_table, float* grad_mlp);
+/* One Adam step on the loss with the weights normalised to sum 1. */
+RT_API rt_status rt_guide_train_step(rt_guide* g, const float* pos, const float* dir, const float* weight, int64_t n,
+                                     float* loss);
+/* Mixture pdf at (pos, dir) pairs; with `u` (n x 3 uniforms) instead, samples
+ * directions into `out_dir` and returns their pdf. */
+RT_API rt_status rt_guide_pdf(rt_guide* g, const float* pos, const float* dir, const float* u, int64_t n,
+                              float* out_dir, float* pdf);
+
+/* ---------------------------------------------------------------------- */
 /* Serving: many render jobs batched into shared wavefront launches         */
 /* (no counterpart in the reference, which renders one frame at a time).    */
 /* ---------------------------------------------------------------------- */

@@ -124,6 +124,10 @@ class ServerStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+class GuideOptions(C.Structure):
+    _fields_ = [("learning_rate", C.c_float), ("pad", C.c_int32), ("seed", C.c_uint64)]
+
+
 class RTError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"rt error {code}: {msg}")
@@ -183,6 +187,16 @@ def load_library():
         "rt_renderer_trace": (I32, [VP, I32, VP, I64, VP, I32]),
         "rt_verify_shading": (I32, [I32, P(Material), I32, P(Light), I32, P(Medium), I32, P(F), I64, P(F)]),
         "rt_kulla_conty_lut": (I32, [P(F), P(F)]),
+        "rt_guide_options_default": (None, [P(GuideOptions)]),
+        "rt_guide_create": (I32, [P(GuideOptions), P(VP)]),
+        "rt_guide_destroy": (I32, [VP]),
+        "rt_guide_sizes": (None, [P(I64), P(I64)]),
+        "rt_guide_get_params": (I32, [VP, P(F), P(F)]),
+        "rt_guide_set_params": (I32, [VP, P(F), P(F)]),
+        "rt_guide_forward": (I32, [VP, P(F), I64, P(F)]),
+        "rt_guide_gradients": (I32, [VP, P(F), P(F), P(F), I64, P(F), P(F), P(F)]),
+        "rt_guide_train_step": (I32, [VP, P(F), P(F), P(F), I64, P(F)]),
+        "rt_guide_pdf": (I32, [VP, P(F), P(F), P(F), I64, P(F), P(F)]),
         "rt_server_options_default": (None, [P(ServerOptions)]),
         "rt_server_create": (I32, [P(ServerOptions), P(VP)]),
         "rt_server_destroy": (I32, [VP]),
@@ -600,6 +614,82 @@ class Server:
         st = ServerStats()
         _check(self._lib.rt_server_get_stats(self._h, C.byref(st)))
         return st.as_dict()
+
+
+class Guide:
+    """The path-guiding network on host buffers: hash grid + MLP + 8-lobe vMF mixture."""
+
+    def __init__(self, learning_rate=1e-2, seed=1):
+        self._lib = load_library()
+        o = GuideOptions()
+        self._lib.rt_guide_options_default(C.byref(o))
+        o.learning_rate, o.seed = learning_rate, seed
+        self._h = C.c_void_p()
+        _check(self._lib.rt_guide_create(C.byref(o), C.byref(self._h)))
+        t, m = C.c_int64(), C.c_int64()
+        self._lib.rt_guide_sizes(C.byref(t), C.byref(m))
+        self.table_size, self.mlp_size = t.value, m.value
+
+    def close(self):
+        if self._h:
+            self._lib.rt_guide_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _f32(a, cols=None):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        return a if cols is None else a.reshape(-1, cols)
+
+    def get_params(self):
+        t = np.empty(self.table_size, np.float32)
+        m = np.empty(self.mlp_size, np.float32)
+        _check(self._lib.rt_guide_get_params(self._h, _fptr(t), _fptr(m)))
+        return t, m
+
+    def set_params(self, table=None, mlp=None):
+        t = None if table is None else self._f32(table).reshape(-1)
+        m = None if mlp is None else self._f32(mlp).reshape(-1)
+        _check(self._lib.rt_guide_set_params(self._h, None if t is None else _fptr(t), None if m is None else _fptr(m)))
+
+    def forward(self, pos):
+        p = self._f32(pos, 3)
+        out = np.empty((p.shape[0], 32), np.float32)
+        _check(self._lib.rt_guide_forward(self._h, _fptr(p), p.shape[0], _fptr(out)))
+        return out
+
+    def gradients(self, pos, dirs, weights):
+        p, d, w = self._f32(pos, 3), self._f32(dirs, 3), self._f32(weights).reshape(-1)
+        loss = np.zeros(1, np.float32)
+        gt = np.empty(self.table_size, np.float32)
+        gm = np.empty(self.mlp_size, np.float32)
+        _check(self._lib.rt_guide_gradients(self._h, _fptr(p), _fptr(d), _fptr(w), p.shape[0], _fptr(loss),
+                                            _fptr(gt), _fptr(gm)))
+        return float(loss[0]), gt, gm
+
+    def train_step(self, pos, dirs, weights):
+        p, d, w = self._f32(pos, 3), self._f32(dirs, 3), self._f32(weights).reshape(-1)
+        loss = np.zeros(1, np.float32)
+        _check(self._lib.rt_guide_train_step(self._h, _fptr(p), _fptr(d), _fptr(w), p.shape[0], _fptr(loss)))
+        return float(loss[0])
+
+    def pdf(self, pos, dirs):
+        p, d = self._f32(pos, 3), self._f32(dirs, 3)
+        out = np.empty(p.shape[0], np.float32)
+        _check(self._lib.rt_guide_pdf(self._h, _fptr(p), _fptr(d), None, p.shape[0], None, _fptr(out)))
+        return out
+
+    def sample(self, pos, u):
+        p, uu = self._f32(pos, 3), self._f32(u, 3)
+        d = np.empty((p.shape[0], 3), np.float32)
+        out = np.empty(p.shape[0], np.float32)
+        _check(self._lib.rt_guide_pdf(self._h, _fptr(p), None, _fptr(uu), p.shape[0], _fptr(d), _fptr(out)))
+        return d, out
 
 
 def verify_shading(op, inputs, materials=(), lights=(), media=()):

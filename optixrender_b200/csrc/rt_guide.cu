@@ -1,0 +1,519 @@
+// rt_guide.cu - fused kernels of the path-guiding network.
+//
+// One warp runs 16 queries at a time through the whole network with
+// mma.sync.m16n8k16 (FP16 operands, FP32 accumulation): the hash-grid
+// features are gathered straight into the A fragments of the first layer,
+// every layer's accumulators are repacked in registers as the next layer's A
+// fragments, and the weights sit in shared memory (rows padded by 8 halves so
+// that a fragment load hits 32 different banks).  Training runs forward, loss
+// gradient, backward and weight gradients in the same kernel: deltas stay in
+// registers, the weight gradients are products of transposed fragments
+// (movmatrix), accumulated in shared memory and added to global memory once
+// per block, and the hash-grid gradient is scattered with float2 atomics.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rt_guide.cuh"
+#include "rt_guide_host.h"
+
+namespace rtg {
+
+__constant__ int c_res[kLevels];
+
+namespace {
+
+constexpr int kWarps = 4;
+constexpr int kBlock = kWarps * 32;
+// padded shared-memory rows (halves)
+constexpr int kS32 = kIn + 8;   // rows of 32 inputs
+constexpr int kS64 = kHid + 8;  // rows of 64 inputs
+// forward weights: W0 [64][40], W1 [64][72], W2 [64][72], W3 [32][72]
+constexpr int kOffW0 = 0, kOffW1 = kOffW0 + kHid * kS32, kOffW2 = kOffW1 + kHid * kS64, kOffW3 = kOffW2 + kHid * kS64;
+constexpr int kFwdHalves = kOffW3 + kOut * kS64;
+// transposed weights for the backward pass: W3T [64][40], W2T [64][72], W1T [64][72], W0T [32][72]
+constexpr int kOffT3 = 0, kOffT2 = kOffT3 + kHid * kS32, kOffT1 = kOffT2 + kHid * kS64, kOffT0 = kOffT1 + kHid * kS64;
+constexpr int kBwdHalves = kOffT0 + kIn * kS64;
+constexpr int kTileStride = kOut + 1;  // per-warp 16 x 33 float staging tile
+
+RT_D void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+RT_D uint32_t pack_h2(float lo, float hi) {
+    __half2 h = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+RT_D float2 unpack_h2(uint32_t x) { return __half22float2(*reinterpret_cast<__half2*>(&x)); }
+
+RT_D uint32_t trans8x8(uint32_t x) {
+    uint32_t y;
+    asm volatile("movmatrix.sync.aligned.m8n8.trans.b16 %0, %1;\n" : "=r"(y) : "r"(x));
+    return y;
+}
+
+// d[j] = A (16 x K) * W^T (K x N) for the weight W [N][K] in shared memory, row stride S.
+template <int K, int N, int S>
+RT_D void layer(const uint32_t (&a)[K / 16][4], const __half* W, float (&d)[N / 8][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+#pragma unroll
+    for (int j = 0; j < N / 8; j++) {
+        d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.0f;
+        const __half* row = W + (8 * j + g) * S + 2 * tig;
+#pragma unroll
+        for (int t = 0; t < K / 16; t++) {
+            uint32_t b0 = *reinterpret_cast<const uint32_t*>(row + 16 * t);
+            uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + 16 * t + 8);
+            mma16816(d[j], a[t], b0, b1);
+        }
+    }
+}
+
+// Accumulators of N columns -> A fragments (N / 16 k-tiles), with ReLU.
+template <int N>
+RT_D void pack_relu(const float (&d)[N / 8][4], uint32_t (&a)[N / 16][4]) {
+#pragma unroll
+    for (int t = 0; t < N / 16; t++) {
+        a[t][0] = pack_h2(fmaxf(d[2 * t][0], 0.f), fmaxf(d[2 * t][1], 0.f));
+        a[t][1] = pack_h2(fmaxf(d[2 * t][2], 0.f), fmaxf(d[2 * t][3], 0.f));
+        a[t][2] = pack_h2(fmaxf(d[2 * t + 1][0], 0.f), fmaxf(d[2 * t + 1][1], 0.f));
+        a[t][3] = pack_h2(fmaxf(d[2 * t + 1][2], 0.f), fmaxf(d[2 * t + 1][3], 0.f));
+    }
+}
+
+// Deltas masked by the ReLU of the forward activations `h` (A fragments), packed to A fragments.
+template <int N>
+RT_D void pack_masked(const float (&d)[N / 8][4], const uint32_t (&h)[N / 16][4], uint32_t (&a)[N / 16][4]) {
+#pragma unroll
+    for (int t = 0; t < N / 16; t++) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const float* src = d[2 * t + (r >> 1)] + 2 * (r & 1);
+            float2 hv = unpack_h2(h[t][r]);
+            a[t][r] = pack_h2(hv.x > 0.f ? src[0] : 0.f, hv.y > 0.f ? src[1] : 0.f);
+        }
+    }
+}
+
+// Weight gradient dW [M][N] += E^T X for deltas E (16 rows x M, A fragments)
+// and inputs X (16 rows x N, A fragments), added into shared memory.
+template <int M, int N>
+RT_D void weight_grad(const uint32_t (&e)[M / 16][4], const uint32_t (&x)[N / 16][4], float* gW) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    uint32_t bt[N / 8][2];
+#pragma unroll
+    for (int j = 0; j < N / 8; j++) {
+        const int t = j >> 1, hi = j & 1;
+        bt[j][0] = trans8x8(x[t][hi ? 2 : 0]);
+        bt[j][1] = trans8x8(x[t][hi ? 3 : 1]);
+    }
+#pragma unroll
+    for (int mt = 0; mt < M / 16; mt++) {
+        uint32_t at[4] = {trans8x8(e[mt][0]), trans8x8(e[mt][2]), trans8x8(e[mt][1]), trans8x8(e[mt][3])};
+#pragma unroll
+        for (int j = 0; j < N / 8; j++) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            mma16816(d, at, bt[j][0], bt[j][1]);
+            float* p = gW + (16 * mt + g) * N + 8 * j + 2 * tig;
+            atomicAdd(p, d[0]);
+            atomicAdd(p + 1, d[1]);
+            atomicAdd(p + 8 * N, d[2]);
+            atomicAdd(p + 8 * N + 1, d[3]);
+        }
+    }
+}
+
+struct Corners {
+    uint32_t idx[8];
+    float w[8];
+};
+
+RT_D void level_corners(int l, float3 x, Corners& c) {
+    const int res = c_res[l];
+    const float fr = float(res);
+    float px = x.x * fr, py = x.y * fr, pz = x.z * fr;
+    float cx = fminf(floorf(px), fr - 1.0f), cy = fminf(floorf(py), fr - 1.0f), cz = fminf(floorf(pz), fr - 1.0f);
+    const float fx = px - cx, fy = py - cy, fz = pz - cz;
+    const uint32_t ix = uint32_t(cx), iy = uint32_t(cy), iz = uint32_t(cz);
+    const uint32_t r1 = uint32_t(res) + 1u;
+    const bool dense = uint64_t(r1) * r1 * r1 <= uint64_t(kT);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const uint32_t gx = ix + (k & 1), gy = iy + ((k >> 1) & 1), gz = iz + ((k >> 2) & 1);
+        c.idx[k] = dense ? gx + gy * r1 + gz * r1 * r1 : ((gx * 1u) ^ (gy * kPrime1) ^ (gz * kPrime2)) & uint32_t(kT - 1);
+        c.w[k] = ((k & 1) ? fx : 1.0f - fx) * (((k >> 1) & 1) ? fy : 1.0f - fy) * (((k >> 2) & 1) ? fz : 1.0f - fz);
+    }
+}
+
+RT_D uint32_t encode_level(const __half2* __restrict__ table, int l, float3 x) {
+    Corners c;
+    level_corners(l, x, c);
+    const __half2* t = table + size_t(l) * kT;
+    float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        float2 v = __half22float2(__ldg(t + c.idx[k]));
+        f0 += c.w[k] * v.x;
+        f1 += c.w[k] * v.y;
+    }
+    return pack_h2(f0, f1);
+}
+
+// A fragments of the 16 x 32 input: this thread's rows g and g + 8, levels
+// tig, tig + 4, tig + 8, tig + 12 (feature pairs 2l, 2l + 1).
+RT_D void encode_tile(const __half2* table, float3 xg, float3 xg8, bool vg, bool vg8, uint32_t (&a)[2][4]) {
+    const int tig = threadIdx.x & 3;
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int l0 = 8 * t + tig, l1 = 8 * t + 4 + tig;
+        a[t][0] = vg ? encode_level(table, l0, xg) : 0u;
+        a[t][1] = vg8 ? encode_level(table, l0, xg8) : 0u;
+        a[t][2] = vg ? encode_level(table, l1, xg) : 0u;
+        a[t][3] = vg8 ? encode_level(table, l1, xg8) : 0u;
+    }
+}
+
+RT_D void load_weights(const __half* __restrict__ mlp, __half* fw, __half* bw) {
+    const __half* W0 = mlp;
+    const __half* W1 = W0 + kW0;
+    const __half* W2 = W1 + kW1;
+    const __half* W3 = W2 + kW2;
+    for (int i = threadIdx.x; i < kW0; i += blockDim.x) {
+        int o = i / kIn, k = i % kIn;
+        fw[kOffW0 + o * kS32 + k] = W0[i];
+        if (bw) bw[kOffT0 + k * kS64 + o] = W0[i];
+    }
+    for (int i = threadIdx.x; i < kW1; i += blockDim.x) {
+        int o = i / kHid, k = i % kHid;
+        fw[kOffW1 + o * kS64 + k] = W1[i];
+        fw[kOffW2 + o * kS64 + k] = W2[i];
+        if (bw) {
+            bw[kOffT1 + k * kS64 + o] = W1[i];
+            bw[kOffT2 + k * kS64 + o] = W2[i];
+        }
+    }
+    for (int i = threadIdx.x; i < kW3; i += blockDim.x) {
+        int o = i / kHid, k = i % kHid;
+        fw[kOffW3 + o * kS64 + k] = W3[i];
+        if (bw) bw[kOffT3 + k * kS32 + o] = W3[i];
+    }
+}
+
+RT_D float3 ld_pos(const float* p, int64_t i) { return make_float3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+// Forward of 16 rows: returns the output accumulators (4 n-tiles of 8 outputs).
+RT_D void forward_tile(const __half* sw, const uint32_t (&ax)[2][4], float (&out)[4][4]) {
+    float d64[8][4];
+    uint32_t h[4][4];
+    layer<kIn, kHid, kS32>(ax, sw + kOffW0, d64);
+    pack_relu<kHid>(d64, h);
+    layer<kHid, kHid, kS64>(h, sw + kOffW1, d64);
+    pack_relu<kHid>(d64, h);
+    layer<kHid, kHid, kS64>(h, sw + kOffW2, d64);
+    pack_relu<kHid>(d64, h);
+    layer<kHid, kOut, kS64>(h, sw + kOffW3, out);
+}
+
+RT_D void stage_outputs(const float (&out)[4][4], float* tile) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float* p = tile + g * kTileStride + 8 * j + 2 * tig;
+        p[0] = out[j][0];
+        p[1] = out[j][1];
+        p[8 * kTileStride] = out[j][2];
+        p[8 * kTileStride + 1] = out[j][3];
+    }
+}
+
+}  // namespace
+
+// Raw outputs (mode 0) or mixtures (mode 1) of n normalised positions.
+__global__ void __launch_bounds__(kBlock) k_guide_forward(NetView net, const float* __restrict__ pos, int n, int mode,
+                                                          float* __restrict__ raw, Mixture* __restrict__ mix) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __half* sw = reinterpret_cast<__half*>(smem);
+    float* tiles = reinterpret_cast<float*>(smem + kFwdHalves * sizeof(__half));
+    load_weights(net.mlp, sw, nullptr);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2;
+    float* tile = tiles + warp * 16 * kTileStride;
+    const int tiles_total = (n + 15) / 16;
+    for (int tt = blockIdx.x * kWarps + warp; tt < tiles_total; tt += gridDim.x * kWarps) {
+        const int r0 = tt * 16 + g, r1 = r0 + 8;
+        const bool v0 = r0 < n, v1 = r1 < n;
+        float3 x0 = v0 ? ld_pos(pos, r0) : make_float3(0.f, 0.f, 0.f);
+        float3 x1 = v1 ? ld_pos(pos, r1) : make_float3(0.f, 0.f, 0.f);
+        uint32_t ax[2][4];
+        encode_tile(net.table, x0, x1, v0, v1, ax);
+        float out[4][4];
+        forward_tile(sw, ax, out);
+        stage_outputs(out, tile);
+        __syncwarp();
+        if (lane < 16 && tt * 16 + lane < n) {
+            const int64_t row = int64_t(tt) * 16 + lane;
+            const float* o = tile + lane * kTileStride;
+            if (mode == 0) {
+                for (int k = 0; k < kOut; k++) raw[row * kOut + k] = o[k];
+            } else {
+                Mixture m;
+                head_from_outputs(o, m);
+                mix[row] = m;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Loss gradient of one row with respect to its 32 raw outputs (in place),
+// for -s * log q(d); returns the row's loss term.
+RT_D float loss_grad_row(float* o, float3 d, float s) {
+    float w[kLobes], kap[kLobes], dens[kLobes];
+    float3 mu[kLobes], dth[kLobes], dph[kLobes];
+    float st[kLobes], sp[kLobes];
+    bool inr[kLobes];
+    float mx = o[0];
+    for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, o[4 * k]);
+    float sum = 0.f;
+    for (int k = 0; k < kLobes; k++) {
+        w[k] = expf(o[4 * k] - mx);
+        sum += w[k];
+    }
+    float q = 0.f;
+    for (int k = 0; k < kLobes; k++) {
+        w[k] /= sum;
+        const float kr = o[4 * k + 1];
+        inr[k] = kr >= kKappaLo && kr <= kKappaHi;
+        kap[k] = expf(fminf(fmaxf(kr, kKappaLo), kKappaHi));
+        st[k] = 1.f / (1.f + expf(-o[4 * k + 2]));
+        sp[k] = 1.f / (1.f + expf(-o[4 * k + 3]));
+        const float th = 3.14159265358979f * st[k], ph = 6.28318530717959f * sp[k];
+        const float s_t = sinf(th), c_t = cosf(th), s_p = sinf(ph), c_p = cosf(ph);
+        mu[k] = make_float3(s_t * c_p, s_t * s_p, c_t);
+        dth[k] = make_float3(c_t * c_p, c_t * s_p, -s_t);
+        dph[k] = make_float3(-s_t * s_p, s_t * c_p, 0.f);
+        const float c = mu[k].x * d.x + mu[k].y * d.y + mu[k].z * d.z;
+        dens[k] = kap[k] / (6.28318530717959f * -expm1f(-2.f * kap[k])) * expf(kap[k] * (c - 1.f));
+        q += w[k] * dens[k];
+    }
+    q = fmaxf(q, 1e-30f);
+    for (int k = 0; k < kLobes; k++) {
+        const float r = w[k] * dens[k] / q;
+        const float c = mu[k].x * d.x + mu[k].y * d.y + mu[k].z * d.z;
+        const float dlogk = 1.f / kap[k] - 2.f / expm1f(2.f * kap[k]) + (c - 1.f);
+        o[4 * k] = s * (w[k] - r);
+        o[4 * k + 1] = inr[k] ? s * -r * dlogk * kap[k] : 0.f;
+        o[4 * k + 2] = s * -r * kap[k] * (dth[k].x * d.x + dth[k].y * d.y + dth[k].z * d.z) * 3.14159265358979f *
+                       st[k] * (1.f - st[k]);
+        o[4 * k + 3] = s * -r * kap[k] * (dph[k].x * d.x + dph[k].y * d.y + dph[k].z * d.z) * 6.28318530717959f *
+                       sp[k] * (1.f - sp[k]);
+    }
+    return -s * logf(q);
+}
+
+// Forward + loss + backward of n samples (position, unit direction, weight);
+// `scale` multiplies every sample weight (1 / batch).  Adds the gradients to
+// grad_table / grad_mlp and the loss to *loss.
+__global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const float* __restrict__ pos,
+                                                           const float* __restrict__ dir,
+                                                           const float* __restrict__ weight, int n, float scale,
+                                                           float* __restrict__ grad_table,
+                                                           float* __restrict__ grad_mlp, float* __restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __half* sw = reinterpret_cast<__half*>(smem);
+    __half* sb = sw + kFwdHalves;
+    float* gW = reinterpret_cast<float*>(smem + (kFwdHalves + kBwdHalves) * sizeof(__half));
+    float* tiles = gW + kMlpParams;
+    load_weights(net.mlp, sw, sb);
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) gW[i] = 0.f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    float* tile = tiles + warp * 16 * kTileStride;
+    float lsum = 0.f;
+    const int tiles_total = (n + 15) / 16;
+    for (int tt = blockIdx.x * kWarps + warp; tt < tiles_total; tt += gridDim.x * kWarps) {
+        const int r0 = tt * 16 + g, r1 = r0 + 8;
+        const bool v0 = r0 < n, v1 = r1 < n;
+        const float3 x0 = v0 ? ld_pos(pos, r0) : make_float3(0.f, 0.f, 0.f);
+        const float3 x1 = v1 ? ld_pos(pos, r1) : make_float3(0.f, 0.f, 0.f);
+        uint32_t ax[2][4], h1[4][4], h2[4][4], h3[4][4];
+        encode_tile(net.table, x0, x1, v0, v1, ax);
+        float d64[8][4], out[4][4];
+        layer<kIn, kHid, kS32>(ax, sw + kOffW0, d64);
+        pack_relu<kHid>(d64, h1);
+        layer<kHid, kHid, kS64>(h1, sw + kOffW1, d64);
+        pack_relu<kHid>(d64, h2);
+        layer<kHid, kHid, kS64>(h2, sw + kOffW2, d64);
+        pack_relu<kHid>(d64, h3);
+        layer<kHid, kOut, kS64>(h3, sw + kOffW3, out);
+        stage_outputs(out, tile);
+        __syncwarp();
+        if (lane < 16) {
+            const int row = tt * 16 + lane;
+            float* o = tile + lane * kTileStride;
+            if (row < n) {
+                const float3 dd = ld_pos(dir, row);
+                lsum += loss_grad_row(o, dd, weight[row] * scale);
+            } else {
+                for (int k = 0; k < kOut; k++) o[k] = 0.f;
+            }
+        }
+        __syncwarp();
+        // dO as A fragments (fp16)
+        uint32_t ado[2][4];
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const float* p = tile + g * kTileStride + 16 * t + 2 * tig;
+            ado[t][0] = pack_h2(p[0], p[1]);
+            ado[t][1] = pack_h2(p[8 * kTileStride], p[8 * kTileStride + 1]);
+            ado[t][2] = pack_h2(p[8], p[9]);
+            ado[t][3] = pack_h2(p[8 * kTileStride + 8], p[8 * kTileStride + 9]);
+        }
+        __syncwarp();
+        uint32_t e[4][4];
+        weight_grad<kOut, kHid>(ado, h3, gW + kW0 + kW1 + kW2);
+        layer<kOut, kHid, kS32>(ado, sb + kOffT3, d64);
+        pack_masked<kHid>(d64, h3, e);
+        weight_grad<kHid, kHid>(e, h2, gW + kW0 + kW1);
+        layer<kHid, kHid, kS64>(e, sb + kOffT2, d64);
+        pack_masked<kHid>(d64, h2, e);
+        weight_grad<kHid, kHid>(e, h1, gW + kW0);
+        layer<kHid, kHid, kS64>(e, sb + kOffT1, d64);
+        pack_masked<kHid>(d64, h1, e);
+        weight_grad<kHid, kIn>(e, ax, gW);
+        float dx[4][4];
+        layer<kHid, kIn, kS64>(e, sb + kOffT0, dx);
+        // hash-grid gradient: this thread's levels 4j + tig for rows g (dx[j][0..1]) and g + 8 (dx[j][2..3])
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int l = 4 * j + tig;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                if (!(h ? v1 : v0)) continue;
+                Corners c;
+                level_corners(l, h ? x1 : x0, c);
+                float2* gt = reinterpret_cast<float2*>(grad_table) + size_t(l) * kT;
+                const float g0 = dx[j][2 * h], g1 = dx[j][2 * h + 1];
+#pragma unroll
+                for (int k = 0; k < 8; k++) atomicAdd(gt + c.idx[k], make_float2(c.w[k] * g0, c.w[k] * g1));
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
+        if (gW[i] != 0.f) atomicAdd(grad_mlp + i, gW[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
+    if (lane == 0 && lsum != 0.f) atomicAdd(loss, lsum);
+}
+
+// Adam over one parameter array: p -= lr * mhat / (sqrt(vhat) + eps); the
+// gradient is cleared and the fp16 copy refreshed.
+__global__ void k_adam(float* __restrict__ p, __half* __restrict__ p16, float* __restrict__ grad,
+                       float* __restrict__ m, float* __restrict__ v, int64_t n, float lr, float b1, float b2, float c1,
+                       float c2, float eps) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const float gr = grad[i];
+        grad[i] = 0.f;
+        const float mi = b1 * m[i] + (1.f - b1) * gr;
+        const float vi = b2 * v[i] + (1.f - b2) * gr * gr;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+        p[i] = pi;
+        p16[i] = __float2half_rn(pi);
+    }
+}
+
+__global__ void k_to_half(const float* __restrict__ p, __half* __restrict__ p16, int64_t n) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        p16[i] = __float2half_rn(p[i]);
+}
+
+// Mixture pdf of (position, direction) pairs and samples from (position, u0..u2).
+__global__ void k_guide_pdf_sample(const Mixture* __restrict__ mix, const float* __restrict__ dir,
+                                   const float* __restrict__ u, int n, float* __restrict__ out_dir,
+                                   float* __restrict__ pdf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Mixture m = mix[i];
+    rtd::v3 d;
+    if (u) {
+        d = mixture_sample(m, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+        out_dir[3 * i] = d.x;
+        out_dir[3 * i + 1] = d.y;
+        out_dir[3 * i + 2] = d.z;
+    } else {
+        d = rtd::v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+    }
+    pdf[i] = mixture_pdf(m, d);
+}
+
+}  // namespace rtg
+
+namespace rtgh {
+
+size_t forward_smem() { return size_t(rtg::kFwdHalves) * 2 + size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4; }
+size_t backward_smem() {
+    return size_t(rtg::kFwdHalves + rtg::kBwdHalves) * 2 + size_t(rtg::kMlpParams) * 4 +
+           size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4;
+}
+
+cudaError_t set_resolutions(const int* res) { return cudaMemcpyToSymbol(rtg::c_res, res, sizeof(int) * rtg::kLevels); }
+
+cudaError_t prepare_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(rtg::k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(forward_smem()));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(rtg::k_guide_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(backward_smem()));
+}
+
+static int grid_for_tiles(int n, int sms) {
+    const int tiles = (n + 15) / 16;
+    const int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
+    return blocks < sms * 8 ? (blocks > 0 ? blocks : 1) : sms * 8;
+}
+
+void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, float* raw, rtg::Mixture* mix, int sms,
+                    cudaStream_t st) {
+    if (n <= 0) return;
+    rtg::k_guide_forward<<<grid_for_tiles(n, sms), rtg::kBlock, forward_smem(), st>>>(net, pos, n, mode, raw, mix);
+}
+
+void launch_backward(const rtg::NetView& net, const float* pos, const float* dir, const float* weight, int n,
+                     float scale, float* grad_table, float* grad_mlp, float* loss, int sms, cudaStream_t st) {
+    if (n <= 0) return;
+    const int tiles = (n + 15) / 16;
+    int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
+    if (blocks > sms * 2) blocks = sms * 2;  // one block per SM pair keeps the per-block gradient flush small
+    rtg::k_guide_backward<<<blocks, rtg::kBlock, backward_smem(), st>>>(net, pos, dir, weight, n, scale, grad_table,
+                                                                        grad_mlp, loss);
+}
+
+void launch_adam(float* p, __half* p16, float* grad, float* m, float* v, int64_t n, float lr, int step,
+                 cudaStream_t st) {
+    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-10f;
+    const float c1 = 1.0f / (1.0f - powf(b1, float(step))), c2 = 1.0f / (1.0f - powf(b2, float(step)));
+    int blocks = int((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    rtg::k_adam<<<blocks, 256, 0, st>>>(p, p16, grad, m, v, n, lr, b1, b2, c1, c2, eps);
+}
+
+void launch_to_half(const float* p, __half* p16, int64_t n, cudaStream_t st) {
+    int blocks = int((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    rtg::k_to_half<<<blocks, 256, 0, st>>>(p, p16, n);
+}
+
+void launch_pdf_sample(const rtg::Mixture* mix, const float* dir, const float* u, int n, float* out_dir, float* pdf,
+                       cudaStream_t st) {
+    if (n <= 0) return;
+    rtg::k_guide_pdf_sample<<<(n + 127) / 128, 128, 0, st>>>(mix, dir, u, n, out_dir, pdf);
+}
+
+}  // namespace rtgh

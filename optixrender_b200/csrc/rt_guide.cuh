@@ -1,0 +1,110 @@
+// rt_guide.cuh - the path-guiding network: constants, the per-query mixture
+// record, and the von Mises-Fisher mixture used by the shade kernel.
+//
+// Network (no counterpart in the reference renderer): a multiresolution hash
+// encoding of the position (Mueller et al., "Instant Neural Graphics
+// Primitives", 2022: 16 levels x 2 features, 2^19 entries per level) feeding a
+// 32-64-64-64-32 MLP without biases (ReLU hidden layers, FP16 weights, FP32
+// accumulation), whose 32 outputs are an 8-lobe vMF mixture over incident
+// directions: lobe k reads (weight logit, log concentration, polar angle,
+// azimuth) from outputs 4k..4k+3.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "rt_device.cuh"
+
+namespace rtg {
+
+constexpr int kLevels = 16;
+constexpr int kFeats = 2;
+constexpr int kLog2T = 19;
+constexpr int kT = 1 << kLog2T;
+constexpr int kIn = kLevels * kFeats;  // 32
+constexpr int kHid = 64;
+constexpr int kOut = 32;
+constexpr int kLobes = 8;
+constexpr int kW0 = kHid * kIn, kW1 = kHid * kHid, kW2 = kHid * kHid, kW3 = kOut * kHid;
+constexpr int kMlpParams = kW0 + kW1 + kW2 + kW3;  // 12288
+constexpr int64_t kTableParams = int64_t(kLevels) * kT * kFeats;
+constexpr float kKappaLo = -2.0f, kKappaHi = 9.0f;  // log-concentration range
+constexpr uint32_t kPrime1 = 2654435761u, kPrime2 = 805459861u;
+
+// Mixture of one query: lobe k = (mu.xyz, kappa) and the normalised weights.
+struct __align__(16) Mixture {
+    float4 lobe[kLobes];
+    float w[kLobes];
+};
+
+// Raw network outputs -> mixture (softmax weights, kappa = exp(clamped),
+// mu from theta = pi * sigmoid, phi = 2 pi * sigmoid).
+RT_D void head_from_outputs(const float* o, Mixture& m) {
+    float mx = o[0];
+#pragma unroll
+    for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, o[4 * k]);
+    float sum = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) {
+        m.w[k] = __expf(o[4 * k] - mx);
+        sum += m.w[k];
+    }
+    const float inv = 1.0f / sum;
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) {
+        m.w[k] *= inv;
+        float kap = __expf(fminf(fmaxf(o[4 * k + 1], kKappaLo), kKappaHi));
+        float th = 3.14159265358979f / (1.0f + __expf(-o[4 * k + 2]));
+        float ph = 6.28318530717959f / (1.0f + __expf(-o[4 * k + 3]));
+        float st, ct, sp, cp;
+        __sincosf(th, &st, &ct);
+        __sincosf(ph, &sp, &cp);
+        m.lobe[k] = make_float4(st * cp, st * sp, ct, kap);
+    }
+}
+
+// vMF density kappa / (2 pi (1 - e^{-2 kappa})) exp(kappa (mu.d - 1)).
+RT_D float vmf_pdf(float4 l, rtd::v3 d) {
+    const float c = l.x * d.x + l.y * d.y + l.z * d.z;
+    return l.w / (6.28318530717959f * -expm1f(-2.0f * l.w)) * __expf(l.w * (c - 1.0f));
+}
+
+RT_D float mixture_pdf(const Mixture& m, rtd::v3 d) {
+    float p = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) p += m.w[k] * vmf_pdf(m.lobe[k], d);
+    return p;
+}
+
+// Picks a lobe with u0 and samples it with (u1, u2): the cosine to mu is
+// 1 + log(u1 + (1 - u1) e^{-2 kappa}) / kappa (Jakob, "Numerically stable
+// sampling of the von Mises Fisher distribution on S2", 2012).
+RT_D rtd::v3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
+    int k = 0;
+    float acc = m.w[0];
+    while (k < kLobes - 1 && u0 >= acc) {
+        k++;
+        acc += m.w[k];
+    }
+    const float4 l = m.lobe[k];
+    float w = 1.0f + __logf(u1 + (1.0f - u1) * __expf(-2.0f * l.w)) / l.w;
+    w = fminf(fmaxf(w, -1.0f), 1.0f);
+    const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    float sp, cp;
+    __sincosf(6.28318530717959f * u2, &sp, &cp);
+    const rtd::v3 mu(l.x, l.y, l.z);
+    // orthonormal basis around mu (Duff et al., "Building an orthonormal basis, revisited", 2017)
+    const float sg = copysignf(1.0f, mu.z);
+    const float a = -1.0f / (sg + mu.z), b = mu.x * mu.y * a;
+    const rtd::v3 t1(1.0f + sg * mu.x * mu.x * a, sg * b, -sg * mu.x);
+    const rtd::v3 t2(b, sg + mu.y * mu.y * a, -mu.y);
+    return normalize(t1 * (s * cp) + t2 * (s * sp) + mu * w);
+}
+
+// Device view of the network's parameters.
+struct NetView {
+    const __half2* table;  // kLevels * kT entries (fp16 features)
+    const __half* mlp;     // kMlpParams, W0 W1 W2 W3 row-major [out][in]
+    float3 lo, inv_ext;    // position normalisation: (x - lo) * inv_ext in [0, 1]
+};
+
+}  // namespace rtg
