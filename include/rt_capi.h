@@ -176,6 +176,18 @@ typedef struct rt_options {
                                  free device memory; at most 2^26) */
     int32_t collect_stats;    /* count rays, nodes and triangles */
     float exposure;           /* multiplier before tonemapping (1) */
+    /* Learned proposal (PCG32 streams only): the first guide_train_spp samples
+     * per pixel (counted over Render() calls) are rendered one sample per pixel
+     * per wave, and after each of those waves the guiding network takes
+     * guide_steps Adam steps on up to 2^18 radiance samples from it; from then
+     * on the trained mixture is sampled with probability guide_prob at every
+     * non-dielectric surface vertex and combined with BSDF sampling by
+     * one-sample MIS, so the estimate stays unbiased. */
+    int32_t guided;           /* 0: plain BSDF + NEE (the reference method) */
+    int32_t guide_train_spp;  /* 32 */
+    float guide_prob;         /* 0.5 */
+    int32_t guide_steps;      /* 4 */
+    int32_t bvh_build;        /* RT_BVH_GPU (default): built on the device; RT_BVH_HOST: on the host */
 } rt_options;
 
 /* Per-render statistics. */
@@ -261,6 +273,11 @@ RT_API rt_status rt_scene_set_env(rt_scene* s, const float* rgba, int32_t width,
 RT_API rt_status rt_scene_get_bounds(const rt_scene* s, float lo[3], float hi[3]);
 RT_API rt_status rt_scene_counts(const rt_scene* s, int64_t* triangles, int32_t* meshes, int32_t* lights,
                                  int32_t* media);
+enum { RT_BVH_GPU = 0, RT_BVH_HOST = 1 };
+
+/* The same acceleration structure built on the current device (binned SAH on
+ * all SMs, then the collapse), copied back and validated on the host. */
+RT_API rt_status rt_scene_build_bvh_gpu(const rt_scene* s, int64_t* num_nodes, int32_t* depth);
 /* Builds the acceleration structure (the work of optixAccelBuild,
  * core/src/Renderer.cpp:146-285) on the host and validates it: every child and
  * triangle index in range, every quantised box containing what it bounds.
@@ -308,6 +325,16 @@ RT_API rt_status rt_renderer_get_stats(const rt_renderer* r, rt_render_stats* st
 /* Frame counter of progressive accumulation (LaunchParams::frame.frameID). */
 RT_API rt_status rt_renderer_frame_index(const rt_renderer* r, int32_t* frame);
 
+/* The renderer's guiding network, created on first use; it stays owned by
+ * the renderer.  Positions it takes are normalised to the scene bounds grown
+ * by 1% on each side. */
+typedef struct rt_guide rt_guide;
+RT_API rt_status rt_renderer_guide(rt_renderer* r, rt_guide** guide);
+/* Training samples collected by the last training wave: `count` of them, up to
+ * `max_samples` copied as 8 floats each (network input position, weight,
+ * direction, 1). */
+RT_API rt_status rt_renderer_guide_samples(rt_renderer* r, float* out, int64_t max_samples, int64_t* count);
+
 /* Ray queries against the renderer's scene: the equivalent of optixTrace,
  * core/cuda/devicePrograms.cu:258-269 (closest hit) and :303-319 (shadow /
  * any hit, terminate on first hit).  rays: n x 8 floats (ox oy oz tmin dx dy dz
@@ -343,12 +370,12 @@ RT_API rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, cons
 /* queries it on device buffers when rt_options.guided is set.               */
 /* ---------------------------------------------------------------------- */
 
-typedef struct rt_guide rt_guide;
-
 typedef struct rt_guide_options {
     float learning_rate;       /* Adam step size (1e-2) */
-    int32_t pad;
+    int32_t max_resolution;    /* grid resolution of the finest level (64); the coarsest is min(16, it) */
     uint64_t seed;             /* parameter initialisation */
+    float max_log_kappa;       /* log of the highest lobe concentration (4) */
+    int32_t pad;
 } rt_guide_options;
 
 RT_API void rt_guide_options_default(rt_guide_options* o);
@@ -368,6 +395,13 @@ RT_API rt_status rt_guide_gradients(rt_guide* g, const float* pos, const float* 
 /* One Adam step on the loss with the weights normalised to sum 1. */
 RT_API rt_status rt_guide_train_step(rt_guide* g, const float* pos, const float* dir, const float* weight, int64_t n,
                                      float* loss);
+/* Learning rate, finest grid resolution and highest log-concentration; a
+ * value <= 0 (0 for the concentration) keeps the current one.  The hash table
+ * is kept, so a new resolution re-indexes the trained features. */
+RT_API rt_status rt_guide_set_hyperparameters(rt_guide* g, float learning_rate, int32_t max_resolution,
+                                              float max_log_kappa);
+/* Loss of the last training step and the number of steps taken. */
+RT_API rt_status rt_guide_last_loss(rt_guide* g, float* loss, int64_t* steps);
 /* Mixture pdf at (pos, dir) pairs; with `u` (n x 3 uniforms) instead, samples
  * directions into `out_dir` and returns their pdf. */
 RT_API rt_status rt_guide_pdf(rt_guide* g, const float* pos, const float* dir, const float* u, int64_t n,
@@ -383,17 +417,18 @@ typedef struct rt_server rt_server;
 typedef struct rt_server_options {
     int64_t hbm_budget_bytes;  /* device memory for resident scenes + admitted jobs (0 = 80% of free) */
     int32_t wave_paths;        /* paths per shared wave (0 = 2^23) */
-    int32_t max_jobs;          /* jobs resident at once (<= 256; 0 = 64) */
+    int32_t max_jobs;          /* jobs resident at once (<= 256; 0 = 256) */
     int32_t max_depth;         /* bounce budget of the shared launches (>= every job's max_depth; 0 = 32) */
     int32_t background;        /* nonzero: a server thread runs the loop; zero: call rt_server_step */
     int32_t waves_in_flight;   /* waves queued ahead on the device (0 = 2) */
-    int32_t policy;            /* RT_SERVE_FAIR (default) or RT_SERVE_FIFO */
+    int32_t policy;            /* RT_SERVE_FAIR (default), RT_SERVE_FIFO or RT_SERVE_SRPT */
 } rt_server_options;
 
 /* How a wave's path slots are split among admitted jobs.  FAIR: up to 16 jobs,
- * taken round-robin, share each wave evenly (small jobs finish early, latency
- * grows with job size).  FIFO: the oldest job takes all it can. */
-enum { RT_SERVE_FAIR = 0, RT_SERVE_FIFO = 1 };
+ * taken round-robin, share each wave evenly (latency grows with job size).
+ * FIFO: the oldest job takes all it can.  SRPT: the jobs with the fewest paths
+ * left go first (shortest remaining work; lowest mean time-to-image). */
+enum { RT_SERVE_FAIR = 0, RT_SERVE_FIFO = 1, RT_SERVE_SRPT = 2 };
 
 /* One request: a resident scene, a camera and the renderer settings of one
  * Render() (PCG32 streams seeded by `seed`). */

@@ -30,6 +30,7 @@ PHASE_ISOTROPIC, PHASE_HG = 0, 1
 MEDIUM_HOMOGENEOUS, MEDIUM_GRID = 0, 1
 FILTER_BOX, FILTER_TENT, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2, 3
 RNG_LCG, RNG_PCG32 = 0, 1
+BVH_GPU, BVH_HOST = 0, 1
 TONEMAP_REINHARD, TONEMAP_ACES_SRGB, TONEMAP_CLAMP = 0, 1, 2
 AOV_COLOR, AOV_ALBEDO, AOV_NORMAL = 0, 1, 2
 VERIFY_BSDF_EVAL, VERIFY_BSDF_SAMPLE, VERIFY_LIGHT_SAMPLE, VERIFY_LIGHT_EVAL = 0, 1, 2, 3
@@ -75,7 +76,9 @@ class Options(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
                 ("filter", C.c_int32), ("rng", C.c_int32), ("rr_depth", C.c_int32), ("progressive", C.c_int32),
                 ("seed", C.c_uint64), ("tonemap", C.c_int32), ("wave_paths", C.c_int32),
-                ("collect_stats", C.c_int32), ("exposure", C.c_float)]
+                ("collect_stats", C.c_int32), ("exposure", C.c_float), ("guided", C.c_int32),
+                ("guide_train_spp", C.c_int32), ("guide_prob", C.c_float), ("guide_steps", C.c_int32),
+                ("bvh_build", C.c_int32)]
 
 
 class RenderStats(C.Structure):
@@ -103,7 +106,7 @@ class JobDesc(C.Structure):
 
 
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
-SERVE_FAIR, SERVE_FIFO = 0, 1
+SERVE_FAIR, SERVE_FIFO, SERVE_SRPT = 0, 1, 2
 
 
 class JobStatus(C.Structure):
@@ -125,7 +128,8 @@ class ServerStats(C.Structure):
 
 
 class GuideOptions(C.Structure):
-    _fields_ = [("learning_rate", C.c_float), ("pad", C.c_int32), ("seed", C.c_uint64)]
+    _fields_ = [("learning_rate", C.c_float), ("max_resolution", C.c_int32), ("seed", C.c_uint64),
+                ("max_log_kappa", C.c_float), ("pad", C.c_int32)]
 
 
 class RTError(RuntimeError):
@@ -168,6 +172,7 @@ def load_library():
         "rt_scene_counts": (I32, [VP, P(I64), P(I32), P(I32), P(I32)]),
         "rt_scene_load_json": (I32, [VP, C.c_char_p, P(Options), P(Camera)]),
         "rt_scene_build_bvh": (I32, [VP, P(I64), P(I32)]),
+        "rt_scene_build_bvh_gpu": (I32, [VP, P(I64), P(I32)]),
         "rt_scene_load_json_string": (I32, [VP, C.c_char_p, C.c_char_p, P(Options), P(Camera)]),
         "rt_renderer_create": (I32, [VP, P(Options), P(VP)]),
         "rt_renderer_destroy": (I32, [VP]),
@@ -197,6 +202,10 @@ def load_library():
         "rt_guide_gradients": (I32, [VP, P(F), P(F), P(F), I64, P(F), P(F), P(F)]),
         "rt_guide_train_step": (I32, [VP, P(F), P(F), P(F), I64, P(F)]),
         "rt_guide_pdf": (I32, [VP, P(F), P(F), P(F), I64, P(F), P(F)]),
+        "rt_guide_last_loss": (I32, [VP, P(F), P(I64)]),
+        "rt_guide_set_hyperparameters": (I32, [VP, F, I32, F]),
+        "rt_renderer_guide": (I32, [VP, P(VP)]),
+        "rt_renderer_guide_samples": (I32, [VP, P(F), I64, P(I64)]),
         "rt_server_options_default": (None, [P(ServerOptions)]),
         "rt_server_create": (I32, [P(ServerOptions), P(VP)]),
         "rt_server_destroy": (I32, [VP]),
@@ -412,6 +421,12 @@ class Scene:
         _check(self._lib.rt_scene_build_bvh(self._h, C.byref(n), C.byref(d)))
         return n.value, d.value
 
+    def build_bvh_gpu(self):
+        """Builds the wide BVH on the device and validates it on the host: (nodes, depth)."""
+        n, d = C.c_int64(), C.c_int32()
+        _check(self._lib.rt_scene_build_bvh_gpu(self._h, C.byref(n), C.byref(d)))
+        return n.value, d.value
+
     def bounds(self):
         lo = (C.c_float * 3)()
         hi = (C.c_float * 3)()
@@ -524,6 +539,21 @@ class Renderer:
                                            out.ctypes.data, 0))
         return out
 
+    def guide_samples(self, max_samples=1 << 22):
+        """The last training wave's samples: (n, 8) = input position, weight, direction, 1."""
+        n = C.c_int64()
+        _check(self._lib.rt_renderer_guide_samples(self._h, None, 0, C.byref(n)))
+        k = min(n.value, max_samples)
+        out = np.empty((k, 8), np.float32)
+        _check(self._lib.rt_renderer_guide_samples(self._h, _fptr(out), k, C.byref(n)))
+        return out
+
+    def guide(self):
+        """The renderer's guiding network (borrowed; created on first use)."""
+        h = C.c_void_p()
+        _check(self._lib.rt_renderer_guide(self._h, C.byref(h)))
+        return Guide(handle=h.value, owner=self)
+
     def trace_device(self, rays_ptr, n, hits_ptr, any_hit=False):
         _check(self._lib.rt_renderer_trace(self._h, 1 if any_hit else 0, rays_ptr, n, hits_ptr, 1))
 
@@ -619,27 +649,46 @@ class Server:
 class Guide:
     """The path-guiding network on host buffers: hash grid + MLP + 8-lobe vMF mixture."""
 
-    def __init__(self, learning_rate=1e-2, seed=1):
+    def __init__(self, learning_rate=1e-2, seed=1, handle=None, owner=None, max_resolution=None,
+                 max_log_kappa=None):
         self._lib = load_library()
-        o = GuideOptions()
-        self._lib.rt_guide_options_default(C.byref(o))
-        o.learning_rate, o.seed = learning_rate, seed
-        self._h = C.c_void_p()
-        _check(self._lib.rt_guide_create(C.byref(o), C.byref(self._h)))
+        self._owned = handle is None
+        self._owner = owner  # keeps a borrowed handle's renderer alive
+        if handle is None:
+            o = GuideOptions()
+            self._lib.rt_guide_options_default(C.byref(o))
+            o.learning_rate, o.seed = learning_rate, seed
+            if max_resolution is not None:
+                o.max_resolution = max_resolution
+            if max_log_kappa is not None:
+                o.max_log_kappa = max_log_kappa
+            self._h = C.c_void_p()
+            _check(self._lib.rt_guide_create(C.byref(o), C.byref(self._h)))
+        else:
+            self._h = C.c_void_p(handle)
         t, m = C.c_int64(), C.c_int64()
         self._lib.rt_guide_sizes(C.byref(t), C.byref(m))
         self.table_size, self.mlp_size = t.value, m.value
 
     def close(self):
-        if self._h:
+        if self._h and self._owned:
             self._lib.rt_guide_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
             self.close()
         except Exception:
             pass
+
+    def set_hyperparameters(self, learning_rate=0.0, max_resolution=0, max_log_kappa=0.0):
+        _check(self._lib.rt_guide_set_hyperparameters(self._h, float(learning_rate), int(max_resolution),
+                                                      float(max_log_kappa)))
+
+    def last_loss(self):
+        loss, steps = C.c_float(), C.c_int64()
+        _check(self._lib.rt_guide_last_loss(self._h, C.byref(loss), C.byref(steps)))
+        return loss.value, steps.value
 
     @staticmethod
     def _f32(a, cols=None):

@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-ftz=true", "-prec-div=false", 
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fopenmp", "-Wall", "-Wno-unused-function", "-Wno-unknown-pragmas",
              "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["rt_kernels.cu", "rt_trace_scratch.cu", "rt_guide.cu", "rt_guide_api.cu"]
+CU_SOURCES = ["rt_kernels.cu", "rt_trace_scratch.cu", "rt_guide.cu", "rt_guide_api.cu", "rt_bvh_gpu.cu"]
 CPP_SOURCES = ["rt_capi.cpp", "rt_renderer.cpp", "rt_bvh.cpp", "rt_tables.cpp", "rt_scene_io.cpp", "rt_server.cpp"]
 HEADERS = ["rt_device.cuh", "rt_shading.cuh", "rt_traverse.cuh", "rt_kernels.cuh", "rt_internal.h", "rt_bvh.h",
            "rt_media.cuh", "rt_guide.cuh", "rt_guide_host.h"]

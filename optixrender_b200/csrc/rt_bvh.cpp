@@ -410,7 +410,79 @@ bool validate(const std::vector<rtd::CwNode>& nodes, const std::vector<int>& ord
     return true;
 }
 
+// True bounds of wide node i from its triangles and children (post-order).
+void wide_bounds(const std::vector<rtd::CwNode>& nodes, const std::vector<int>& order, const float* tv, size_t i,
+                 std::vector<Box>& wbox, std::vector<char>& done, int depth, bool& ok) {
+    if (depth > 64 || i >= nodes.size()) {
+        ok = false;
+        return;
+    }
+    const rtd::CwNode& n = nodes[i];
+    Box b;
+    b.reset();
+    int rank = 0;
+    for (int s = 0; s < 8; s++) {
+        if (n.meta[s] == 0) continue;
+        if ((n.imask >> s) & 1u) {
+            size_t c = size_t(n.child_base) + size_t(rank++);
+            if (c >= nodes.size() || c == i) {
+                ok = false;
+                return;
+            }
+            if (!done[c]) wide_bounds(nodes, order, tv, c, wbox, done, depth + 1, ok);
+            if (!ok) return;
+            b.grow(wbox[c]);
+        } else {
+            uint32_t unary = n.meta[s] >> 5, off = n.meta[s] & 31u;
+            int cnt = unary == 1 ? 1 : unary == 3 ? 2 : unary == 7 ? 3 : 0;
+            for (int k = 0; k < cnt; k++) {
+                size_t slot = size_t(n.tri_base) + off + size_t(k);
+                if (slot >= order.size()) {
+                    ok = false;
+                    return;
+                }
+                const float* t = tv + size_t(order[slot]) * 9;
+                b.grow(t);
+                b.grow(t + 3);
+                b.grow(t + 6);
+            }
+        }
+    }
+    wbox[i] = b;
+    done[i] = 1;
+}
+
 }  // namespace
+
+bool validate_cwbvh(const BuiltBvh& bvh, const float* tv, int64_t ntri, std::string& err) {
+    if (int64_t(bvh.order.size()) != ntri) {
+        err = "triangle count mismatch";
+        return false;
+    }
+    std::vector<char> seen(size_t(ntri), 0);
+    for (int t : bvh.order) {
+        if (t < 0 || t >= ntri || seen[size_t(t)]) {
+            err = "triangle order is not a permutation";
+            return false;
+        }
+        seen[size_t(t)] = 1;
+    }
+    if (bvh.nodes.empty()) return ntri == 0;
+    std::vector<Box> wbox(bvh.nodes.size());
+    std::vector<char> done(bvh.nodes.size(), 0);
+    bool ok = true;
+    wide_bounds(bvh.nodes, bvh.order, tv, 0, wbox, done, 0, ok);
+    if (!ok) {
+        err = "child or triangle index out of range";
+        return false;
+    }
+    for (size_t i = 0; i < done.size(); i++)
+        if (!done[i]) {
+            err = "unreachable wide node";
+            return false;
+        }
+    return validate(bvh.nodes, bvh.order, wbox, tv, err);
+}
 
 bool build_cwbvh(const float* tv, int64_t ntri, BuiltBvh& res, std::string& err) {
     res.nodes.clear();

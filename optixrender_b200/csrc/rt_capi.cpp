@@ -241,6 +241,11 @@ void rt_options_default(rt_options* o) {
     o->wave_paths = 0;
     o->collect_stats = 0;
     o->exposure = 1.0f;
+    o->guided = 0;
+    o->guide_train_spp = 32;
+    o->guide_prob = 0.5f;
+    o->guide_steps = 4;
+    o->bvh_build = RT_BVH_GPU;
 }
 
 // ====================================================================== scene
@@ -393,6 +398,18 @@ rt_status rt_scene_build_bvh(const rt_scene* s, int64_t* num_nodes, int32_t* dep
     std::string err;
     if (!rth::build_cwbvh(s->tv.data(), int64_t(s->tri_mesh.size()), bvh, err))
         return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
+    if (num_nodes) *num_nodes = int64_t(bvh.nodes.size());
+    if (depth) *depth = bvh.depth;
+    return RT_OK;
+}
+
+rt_status rt_scene_build_bvh_gpu(const rt_scene* s, int64_t* num_nodes, int32_t* depth) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_scene_build_bvh_gpu: NULL scene");
+    rth::BuiltBvh bvh;
+    std::string err;
+    const int64_t nt = int64_t(s->tri_mesh.size());
+    if (!rth::build_cwbvh_gpu(s->tv.data(), nt, bvh, err, nullptr)) return fail(RT_ERR_CUDA, err);
+    if (!rth::validate_cwbvh(bvh, s->tv.data(), nt, err)) return fail(RT_ERR_UNSUPPORTED, "GPU BVH invalid: " + err);
     if (num_nodes) *num_nodes = int64_t(bvh.nodes.size());
     if (depth) *depth = bvh.depth;
     return RT_OK;

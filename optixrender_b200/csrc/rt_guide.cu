@@ -16,10 +16,9 @@
 
 #include "rt_guide.cuh"
 #include "rt_guide_host.h"
+#include "rt_kernels.cuh"
 
 namespace rtg {
-
-__constant__ int c_res[kLevels];
 
 namespace {
 
@@ -35,6 +34,7 @@ constexpr int kFwdHalves = kOffW3 + kOut * kS64;
 constexpr int kOffT3 = 0, kOffT2 = kOffT3 + kHid * kS32, kOffT1 = kOffT2 + kHid * kS64, kOffT0 = kOffT1 + kHid * kS64;
 constexpr int kBwdHalves = kOffT0 + kIn * kS64;
 constexpr int kTileStride = kOut + 1;  // per-warp 16 x 33 float staging tile
+constexpr int kShadeBucketsG = 6;      // shade buckets of guided material types
 
 RT_D void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
@@ -132,8 +132,8 @@ struct Corners {
     float w[8];
 };
 
-RT_D void level_corners(int l, float3 x, Corners& c) {
-    const int res = c_res[l];
+RT_D void level_corners(const int* res_table, int l, float3 x, Corners& c) {
+    const int res = res_table[l];
     const float fr = float(res);
     float px = x.x * fr, py = x.y * fr, pz = x.z * fr;
     float cx = fminf(floorf(px), fr - 1.0f), cy = fminf(floorf(py), fr - 1.0f), cz = fminf(floorf(pz), fr - 1.0f);
@@ -149,9 +149,9 @@ RT_D void level_corners(int l, float3 x, Corners& c) {
     }
 }
 
-RT_D uint32_t encode_level(const __half2* __restrict__ table, int l, float3 x) {
+RT_D uint32_t encode_level(const __half2* __restrict__ table, const int* res, int l, float3 x) {
     Corners c;
-    level_corners(l, x, c);
+    level_corners(res, l, x, c);
     const __half2* t = table + size_t(l) * kT;
     float f0 = 0.f, f1 = 0.f;
 #pragma unroll
@@ -165,15 +165,15 @@ RT_D uint32_t encode_level(const __half2* __restrict__ table, int l, float3 x) {
 
 // A fragments of the 16 x 32 input: this thread's rows g and g + 8, levels
 // tig, tig + 4, tig + 8, tig + 12 (feature pairs 2l, 2l + 1).
-RT_D void encode_tile(const __half2* table, float3 xg, float3 xg8, bool vg, bool vg8, uint32_t (&a)[2][4]) {
+RT_D void encode_tile(const NetView& net, float3 xg, float3 xg8, bool vg, bool vg8, uint32_t (&a)[2][4]) {
     const int tig = threadIdx.x & 3;
 #pragma unroll
     for (int t = 0; t < 2; t++) {
         const int l0 = 8 * t + tig, l1 = 8 * t + 4 + tig;
-        a[t][0] = vg ? encode_level(table, l0, xg) : 0u;
-        a[t][1] = vg8 ? encode_level(table, l0, xg8) : 0u;
-        a[t][2] = vg ? encode_level(table, l1, xg) : 0u;
-        a[t][3] = vg8 ? encode_level(table, l1, xg8) : 0u;
+        a[t][0] = vg ? encode_level(net.table, net.res, l0, xg) : 0u;
+        a[t][1] = vg8 ? encode_level(net.table, net.res, l0, xg8) : 0u;
+        a[t][2] = vg ? encode_level(net.table, net.res, l1, xg) : 0u;
+        a[t][3] = vg8 ? encode_level(net.table, net.res, l1, xg8) : 0u;
     }
 }
 
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_forward(NetView net, const flo
         float3 x0 = v0 ? ld_pos(pos, r0) : make_float3(0.f, 0.f, 0.f);
         float3 x1 = v1 ? ld_pos(pos, r1) : make_float3(0.f, 0.f, 0.f);
         uint32_t ax[2][4];
-        encode_tile(net.table, x0, x1, v0, v1, ax);
+        encode_tile(net, x0, x1, v0, v1, ax);
         float out[4][4];
         forward_tile(sw, ax, out);
         stage_outputs(out, tile);
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_forward(NetView net, const flo
                 for (int k = 0; k < kOut; k++) raw[row * kOut + k] = o[k];
             } else {
                 Mixture m;
-                head_from_outputs(o, m);
+                head_from_outputs(o, m, net.kappa_hi);
                 mix[row] = m;
             }
         }
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_forward(NetView net, const flo
 
 // Loss gradient of one row with respect to its 32 raw outputs (in place),
 // for -s * log q(d); returns the row's loss term.
-RT_D float loss_grad_row(float* o, float3 d, float s) {
+RT_D float loss_grad_row(float* o, float3 d, float s, float kappa_hi) {
     float w[kLobes], kap[kLobes], dens[kLobes];
     float3 mu[kLobes], dth[kLobes], dph[kLobes];
     float st[kLobes], sp[kLobes];
@@ -287,8 +287,8 @@ RT_D float loss_grad_row(float* o, float3 d, float s) {
     for (int k = 0; k < kLobes; k++) {
         w[k] /= sum;
         const float kr = o[4 * k + 1];
-        inr[k] = kr >= kKappaLo && kr <= kKappaHi;
-        kap[k] = expf(fminf(fmaxf(kr, kKappaLo), kKappaHi));
+        inr[k] = kr >= kKappaLo && kr <= kappa_hi;
+        kap[k] = expf(fminf(fmaxf(kr, kKappaLo), kappa_hi));
         st[k] = 1.f / (1.f + expf(-o[4 * k + 2]));
         sp[k] = 1.f / (1.f + expf(-o[4 * k + 3]));
         const float th = 3.14159265358979f * st[k], ph = 6.28318530717959f * sp[k];
@@ -321,9 +321,14 @@ RT_D float loss_grad_row(float* o, float3 d, float s) {
 __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const float* __restrict__ pos,
                                                            const float* __restrict__ dir,
                                                            const float* __restrict__ weight, int n, float scale,
+                                                           const float* __restrict__ weight_sum,
                                                            float* __restrict__ grad_table,
                                                            float* __restrict__ grad_mlp, float* __restrict__ loss) {
     extern __shared__ __align__(16) unsigned char smem[];
+    if (weight_sum) {  // scale = 1 / (sum of the batch's weights), computed on the device
+        const float ws = *weight_sum;
+        scale = ws > 0.f ? 1.0f / ws : 0.f;
+    }
     __half* sw = reinterpret_cast<__half*>(smem);
     __half* sb = sw + kFwdHalves;
     float* gW = reinterpret_cast<float*>(smem + (kFwdHalves + kBwdHalves) * sizeof(__half));
@@ -341,7 +346,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
         const float3 x0 = v0 ? ld_pos(pos, r0) : make_float3(0.f, 0.f, 0.f);
         const float3 x1 = v1 ? ld_pos(pos, r1) : make_float3(0.f, 0.f, 0.f);
         uint32_t ax[2][4], h1[4][4], h2[4][4], h3[4][4];
-        encode_tile(net.table, x0, x1, v0, v1, ax);
+        encode_tile(net, x0, x1, v0, v1, ax);
         float d64[8][4], out[4][4];
         layer<kIn, kHid, kS32>(ax, sw + kOffW0, d64);
         pack_relu<kHid>(d64, h1);
@@ -357,7 +362,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
             float* o = tile + lane * kTileStride;
             if (row < n) {
                 const float3 dd = ld_pos(dir, row);
-                lsum += loss_grad_row(o, dd, weight[row] * scale);
+                lsum += loss_grad_row(o, dd, weight[row] * scale, net.kappa_hi);
             } else {
                 for (int k = 0; k < kOut; k++) o[k] = 0.f;
             }
@@ -395,7 +400,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
             for (int h = 0; h < 2; h++) {
                 if (!(h ? v1 : v0)) continue;
                 Corners c;
-                level_corners(l, h ? x1 : x0, c);
+                level_corners(net.res, l, h ? x1 : x0, c);
                 float2* gt = reinterpret_cast<float2*>(grad_table) + size_t(l) * kT;
                 const float g0 = dx[j][2 * h], g1 = dx[j][2 * h + 1];
 #pragma unroll
@@ -409,6 +414,167 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
     if (lane == 0 && lsum != 0.f) atomicAdd(loss, lsum);
+}
+
+// ------------------------------------------------------------------ renderer side
+// Items of the sorted shade queue whose material type is guided, in bucket order.
+struct GuidedItems {
+    int bucket[kShadeBucketsG], count[kShadeBucketsG], n;
+};
+
+RT_D GuidedItems guided_items(const rtd::WaveCtl* ctl) {
+    GuidedItems gi;
+    int m = 0;
+    gi.n = 0;
+    for (int b = 0; b < rtd::kShadeBuckets; b++) {
+        if (b == rtd::kMissBucket || !guided_type(b)) continue;
+        gi.bucket[m] = b;
+        gi.count[m] = ctl->bucket[b];
+        gi.n += gi.count[m];
+        m++;
+    }
+    for (; m < kShadeBucketsG; m++) gi.bucket[m] = gi.count[m] = 0;
+    return gi;
+}
+
+RT_D int guided_slot(const GuidedItems& gi, const rtd::WaveBufs& B, int i) {
+    int m = 0, base = 0;
+    while (m < kShadeBucketsG - 1 && i >= base + gi.count[m]) base += gi.count[m++];
+    return B.sorted[size_t(gi.bucket[m]) * size_t(B.capacity) + size_t(i - base)];
+}
+
+RT_D float3 hit_position(const rtd::Ctx& c, int slot) {
+    const rtd::WaveBufs& B = c.wb;
+    const float4 o = B.ray_o[slot], d = B.ray_d[slot], h = B.hit[slot];
+    const rtd::WaveParams& W = c.waves[*c.wave_index];
+    const rtd::SceneView& sc = c.jobs[W.seg[rtd::find_segment(W, slot)].job].sc;
+    const float4* tv = sc.tri_v + size_t(__float_as_int(h.w)) * 3;
+    const float4 p0 = __ldg(tv), p1 = __ldg(tv + 1), p2 = __ldg(tv + 2);
+    const rtd::v3 dd(d.x, d.y, d.z);
+    const rtd::v3 p(o.x + h.x * d.x, o.y + h.x * d.y, o.z + h.x * d.z);
+    return guide_input(p, rtd::v3(p0.x, p0.y, p0.z), rtd::v3(p1.x, p1.y, p1.z), rtd::v3(p2.x, p2.y, p2.z), dd, c.G);
+}
+
+// Mixtures of this bounce's guided vertices (surface hits of guided material
+// types), written per slot for the shade kernel.
+__global__ void __launch_bounds__(kBlock) k_guide_infer(rtd::Ctx c, NetView net) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __half* sw = reinterpret_cast<__half*>(smem);
+    float* tiles = reinterpret_cast<float*>(smem + kFwdHalves * sizeof(__half));
+    load_weights(net.mlp, sw, nullptr);
+    __syncthreads();
+    const rtd::WaveBufs& B = c.wb;
+    const GuidedItems gi = guided_items(B.ctl);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2;
+    float* tile = tiles + warp * 16 * kTileStride;
+    const int n = gi.n;
+    const int tiles_total = (n + 15) / 16;
+    for (int tt = blockIdx.x * kWarps + warp; tt < tiles_total; tt += gridDim.x * kWarps) {
+        const int r0 = tt * 16 + g, r1 = r0 + 8;
+        const bool v0 = r0 < n, v1 = r1 < n;
+        const int s0 = v0 ? guided_slot(gi, B, r0) : 0, s1 = v1 ? guided_slot(gi, B, r1) : 0;
+        const float3 x0 = v0 ? hit_position(c, s0) : make_float3(0.f, 0.f, 0.f);
+        const float3 x1 = v1 ? hit_position(c, s1) : make_float3(0.f, 0.f, 0.f);
+        uint32_t ax[2][4];
+        encode_tile(net, x0, x1, v0, v1, ax);
+        float out[4][4];
+        forward_tile(sw, ax, out);
+        stage_outputs(out, tile);
+        __syncwarp();
+        if (lane < 16 && tt * 16 + lane < n) {
+            const int slot = guided_slot(gi, B, tt * 16 + lane);
+            Mixture m;
+            head_from_outputs(tile + lane * kTileStride, m, net.kappa_hi);
+            c.G.mix[slot] = m;
+        }
+        __syncwarp();
+    }
+}
+
+// End of a training wave: turns each path's records into training samples
+// (position, direction, weight = luminance of the incident-radiance estimate
+// (R_end - R_i) / T_i times |cos| over the sampling pdf: the mixture is fitted
+// to incident radiance times the cosine), appended to `buf`.
+__global__ void k_guide_collect(rtd::Ctx c, float4* __restrict__ buf, int* __restrict__ count, int cap) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const rtd::WaveParams& W = c.waves[*c.wave_index];
+    const rtd::WaveBufs& B = c.wb;
+    const int lane = threadIdx.x & 31;
+    const bool in_wave = slot < W.wave_count;
+    float4 re = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (in_wave) {
+        const float4 a = B.rad[slot], e = B.nee0[slot], l = B.nee1[slot];
+        re = make_float4(a.x + e.x + l.x, a.y + e.y + l.y, a.z + e.z + l.z, 0.f);
+    }
+    const size_t C = size_t(B.capacity);
+    for (int r = 0; r < kGuideRec; r++) {
+        bool ok = false;
+        float4 xp = make_float4(0.f, 0.f, 0.f, 0.f), dv = xp;
+        float wgt = 0.f;
+        if (in_wave) {
+            const float4* R = c.G.rec + size_t(r) * 4 * C + slot;
+            dv = R[C];
+            if (dv.w != 0.f) {
+                xp = R[0];
+                const float4 t = R[2 * C], rr = R[3 * C];
+                const float lx = t.x > 0.f ? (re.x - rr.x) / t.x : 0.f;
+                const float ly = t.y > 0.f ? (re.y - rr.y) / t.y : 0.f;
+                const float lz = t.z > 0.f ? (re.z - rr.z) / t.z : 0.f;
+                wgt = (lx + ly + lz) * (1.0f / 3.0f) * dv.w / xp.w;  // target: L_in |cos|
+                ok = wgt > 0.f && wgt < 3.0e38f;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (!m) continue;
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        const int pos = base + __popc(m & ((1u << lane) - 1u));
+        if (ok && pos < cap) {
+            buf[2 * size_t(pos)] = make_float4(xp.x, xp.y, xp.z, wgt);
+            buf[2 * size_t(pos) + 1] = make_float4(dv.x, dv.y, dv.z, 1.0f);
+        }
+    }
+}
+
+// A training batch of `n` samples: all collected ones when they fit, else a
+// uniform random subset (with replacement); accumulates the batch's weight sum
+// for the loss scale.
+__global__ void k_guide_batch(const float4* __restrict__ buf, const int* __restrict__ count, int cap, int n,
+                              uint32_t seed, float* __restrict__ pos, float* __restrict__ dir, float* __restrict__ w,
+                              float* __restrict__ weight_sum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cnt = min(*count, cap);
+    float wi = 0.f;
+    if (i < n) {
+        float4 a = make_float4(0.5f, 0.5f, 0.5f, 0.f), b = make_float4(0.f, 0.f, 1.f, 0.f);
+        if (cnt > n) {  // a random subset (with replacement)
+            uint32_t h = uint32_t(i) * 0x9E3779B9u ^ seed;
+            h ^= h >> 16;
+            h *= 0x85EBCA6Bu;
+            h ^= h >> 13;
+            h *= 0xC2B2AE35u;
+            h ^= h >> 16;
+            const int j = int(uint64_t(h) * uint64_t(cnt) >> 32);
+            a = buf[2 * size_t(j)];
+            b = buf[2 * size_t(j) + 1];
+        } else if (i < cnt) {  // every sample once; the rest of the batch weighs nothing
+            a = buf[2 * size_t(i)];
+            b = buf[2 * size_t(i) + 1];
+        }
+        pos[3 * i] = a.x;
+        pos[3 * i + 1] = a.y;
+        pos[3 * i + 2] = a.z;
+        dir[3 * i] = b.x;
+        dir[3 * i + 1] = b.y;
+        dir[3 * i + 2] = b.z;
+        wi = a.w;
+        w[i] = wi;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wi += __shfl_down_sync(0xffffffffu, wi, o);
+    if ((threadIdx.x & 31) == 0 && wi != 0.f) atomicAdd(weight_sum, wi);
 }
 
 // Adam over one parameter array: p -= lr * mhat / (sqrt(vhat) + eps); the
@@ -463,11 +629,11 @@ size_t backward_smem() {
            size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4;
 }
 
-cudaError_t set_resolutions(const int* res) { return cudaMemcpyToSymbol(rtg::c_res, res, sizeof(int) * rtg::kLevels); }
-
 cudaError_t prepare_kernels() {
     cudaError_t e = cudaFuncSetAttribute(rtg::k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(forward_smem()));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(rtg::k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(forward_smem()));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(rtg::k_guide_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(backward_smem()));
@@ -486,13 +652,27 @@ void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, 
 }
 
 void launch_backward(const rtg::NetView& net, const float* pos, const float* dir, const float* weight, int n,
-                     float scale, float* grad_table, float* grad_mlp, float* loss, int sms, cudaStream_t st) {
+                     float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss, int sms,
+                     cudaStream_t st) {
     if (n <= 0) return;
     const int tiles = (n + 15) / 16;
     int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
-    if (blocks > sms * 2) blocks = sms * 2;  // one block per SM pair keeps the per-block gradient flush small
-    rtg::k_guide_backward<<<blocks, rtg::kBlock, backward_smem(), st>>>(net, pos, dir, weight, n, scale, grad_table,
-                                                                        grad_mlp, loss);
+    if (blocks > sms * 2) blocks = sms * 2;  // two blocks per SM keep the per-block gradient flush small
+    rtg::k_guide_backward<<<blocks, rtg::kBlock, backward_smem(), st>>>(net, pos, dir, weight, n, scale, weight_sum,
+                                                                        grad_table, grad_mlp, loss);
+}
+
+void launch_infer(const rtd::Ctx& c, const rtg::NetView& net, int sms, cudaStream_t st) {
+    rtg::k_guide_infer<<<sms * 4, rtg::kBlock, forward_smem(), st>>>(c, net);
+}
+
+void launch_collect(const rtd::Ctx& c, float4* buf, int* count, int cap, cudaStream_t st) {
+    rtg::k_guide_collect<<<(c.wb.capacity + 255) / 256, 256, 0, st>>>(c, buf, count, cap);
+}
+
+void launch_batch(const float4* buf, const int* count, int cap, int n, uint32_t seed, float* pos, float* dir,
+                  float* w, float* weight_sum, cudaStream_t st) {
+    rtg::k_guide_batch<<<(n + 255) / 256, 256, 0, st>>>(buf, count, cap, n, seed, pos, dir, w, weight_sum);
 }
 
 void launch_adam(float* p, __half* p16, float* grad, float* m, float* v, int64_t n, float lr, int step,

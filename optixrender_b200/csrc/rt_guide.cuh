@@ -27,7 +27,7 @@ constexpr int kLobes = 8;
 constexpr int kW0 = kHid * kIn, kW1 = kHid * kHid, kW2 = kHid * kHid, kW3 = kOut * kHid;
 constexpr int kMlpParams = kW0 + kW1 + kW2 + kW3;  // 12288
 constexpr int64_t kTableParams = int64_t(kLevels) * kT * kFeats;
-constexpr float kKappaLo = -2.0f, kKappaHi = 9.0f;  // log-concentration range
+constexpr float kKappaLo = -2.0f;  // lowest log-concentration (the highest is per network)
 constexpr uint32_t kPrime1 = 2654435761u, kPrime2 = 805459861u;
 
 // Mixture of one query: lobe k = (mu.xyz, kappa) and the normalised weights.
@@ -36,9 +36,29 @@ struct __align__(16) Mixture {
     float w[kLobes];
 };
 
+// Device view of the network's parameters.
+struct NetView {
+    const __half2* table;  // kLevels * kT entries (fp16 features)
+    const __half* mlp;     // kMlpParams, W0 W1 W2 W3 row-major [out][in]
+    float3 lo, inv_ext;    // position normalisation: (x - lo) * inv_ext in [0, 1]
+    int res[kLevels];      // grid resolution of each level
+    float kappa_hi;        // highest log-concentration of a lobe
+};
+
+// Guiding state of a wave, read by the wavefront kernels.
+constexpr int kGuideRec = 3;  // training records per path (the first bounces)
+struct GuideCtx {
+    Mixture* mix;        // per slot: this bounce's mixture (null: the wave is not guided)
+    float4* rec;         // training records, [kGuideRec][4][capacity] float4 (null: no training)
+    float prob;          // probability of sampling the mixture at a guided vertex
+    float min_rough;     // conductors and clear coats rougher than this are guided
+    float3 lo, inv_ext;  // position normalisation of the scene
+};
+
+#ifdef __CUDACC__
 // Raw network outputs -> mixture (softmax weights, kappa = exp(clamped),
 // mu from theta = pi * sigmoid, phi = 2 pi * sigmoid).
-RT_D void head_from_outputs(const float* o, Mixture& m) {
+RT_D void head_from_outputs(const float* o, Mixture& m, float kappa_hi) {
     float mx = o[0];
 #pragma unroll
     for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, o[4 * k]);
@@ -52,7 +72,7 @@ RT_D void head_from_outputs(const float* o, Mixture& m) {
 #pragma unroll
     for (int k = 0; k < kLobes; k++) {
         m.w[k] *= inv;
-        float kap = __expf(fminf(fmaxf(o[4 * k + 1], kKappaLo), kKappaHi));
+        float kap = __expf(fminf(fmaxf(o[4 * k + 1], kKappaLo), kappa_hi));
         float th = 3.14159265358979f / (1.0f + __expf(-o[4 * k + 2]));
         float ph = 6.28318530717959f / (1.0f + __expf(-o[4 * k + 3]));
         float st, ct, sp, cp;
@@ -100,11 +120,47 @@ RT_D rtd::v3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
     return normalize(t1 * (s * cp) + t2 * (s * sp) + mu * w);
 }
 
-// Device view of the network's parameters.
-struct NetView {
-    const __half2* table;  // kLevels * kT entries (fp16 features)
-    const __half* mlp;     // kMlpParams, W0 W1 W2 W3 row-major [out][in]
-    float3 lo, inv_ext;    // position normalisation: (x - lo) * inv_ext in [0, 1]
-};
+// The same on a mixture in global memory (read-only for the kernel).
+RT_D float mixture_pdf(const Mixture* m, rtd::v3 d) {
+    const float4* w4 = reinterpret_cast<const float4*>(m->w);
+    const float4 wa = __ldg(w4), wb = __ldg(w4 + 1);
+    const float w[kLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    float p = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) p += w[k] * vmf_pdf(__ldg(m->lobe + k), d);
+    return p;
+}
+RT_D rtd::v3 mixture_sample(const Mixture* m, float u0, float u1, float u2) {
+    Mixture c;
+#pragma unroll
+    for (int k = 0; k < kLobes; k++) c.lobe[k] = __ldg(m->lobe + k);
+    const float4* w4 = reinterpret_cast<const float4*>(m->w);
+    const float4 wa = __ldg(w4), wb = __ldg(w4 + 1);
+    c.w[0] = wa.x, c.w[1] = wa.y, c.w[2] = wa.z, c.w[3] = wa.w;
+    c.w[4] = wb.x, c.w[5] = wb.y, c.w[6] = wb.z, c.w[7] = wb.w;
+    return mixture_sample(c, u0, u1, u2);
+}
+
+// Network input of a surface point: the position moved by kSideOffset (in
+// normalised scene units) along the geometric normal turned towards the
+// incoming ray, so that the two sides of a thin wall read different hash
+// cells at the fine levels; then normalised and clamped to [0, 1]^3.
+constexpr float kSideOffset = 1.0f / 512.0f;
+RT_D float3 guide_input(rtd::v3 p, rtd::v3 p0, rtd::v3 p1, rtd::v3 p2, rtd::v3 d, const GuideCtx& G) {
+    rtd::v3 ng = cross(p1 - p0, p2 - p0);
+    const float len = sqrtf(dot(ng, ng));
+    ng = len > 0.0f ? ng * (1.0f / len) : rtd::v3(0.0f);
+    if (dot(ng, d) > 0.0f) ng = -ng;
+    float3 x;
+    x.x = fminf(fmaxf((p.x - G.lo.x) * G.inv_ext.x + kSideOffset * ng.x, 0.f), 1.f);
+    x.y = fminf(fmaxf((p.y - G.lo.y) * G.inv_ext.y + kSideOffset * ng.y, 0.f), 1.f);
+    x.z = fminf(fmaxf((p.z - G.lo.z) * G.inv_ext.z + kSideOffset * ng.z, 0.f), 1.f);
+    return x;
+}
+
+// Material types whose vertices are guided (dielectrics never; conductors and
+// clear coats only above the roughness threshold).
+RT_D bool guided_type(int type) { return type != RT_MAT_DIELECTRIC && type != RT_MAT_THIN_DIELECTRIC; }
+#endif
 
 }  // namespace rtg

@@ -3,6 +3,7 @@
 // The renderer drives the same kernels on device buffers.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -15,9 +16,10 @@ using namespace rti;
 
 namespace rtgh {
 
-void level_resolutions(int* res) {
-    const double b = std::exp((std::log(2048.0) - std::log(16.0)) / double(rtg::kLevels - 1));
-    for (int l = 0; l < rtg::kLevels; l++) res[l] = int(std::floor(16.0 * std::pow(b, double(l))));
+void level_resolutions(int n_max, int* res) {
+    const double lo = std::min(16.0, double(n_max));
+    const double b = std::exp((std::log(double(n_max)) - std::log(lo)) / double(rtg::kLevels - 1));
+    for (int l = 0; l < rtg::kLevels; l++) res[l] = int(std::floor(lo * std::pow(b, double(l)) + 1e-6));
 }
 
 }  // namespace rtgh
@@ -29,6 +31,7 @@ struct rt_guide {
     rt_guide_options opt{};
     DevBuf table, table16, mlp, mlp16, gtable, gmlp, mt, vt, mm, vm, loss;
     int step = 0;
+    int res[rtg::kLevels];
 };
 
 namespace {
@@ -53,6 +56,8 @@ rtg::NetView view(const rt_guide* g) {
     v.mlp = g->mlp16.as<__half>();
     v.lo = make_float3(0.f, 0.f, 0.f);
     v.inv_ext = make_float3(1.f, 1.f, 1.f);
+    for (int l = 0; l < rtg::kLevels; l++) v.res[l] = g->res[l];
+    v.kappa_hi = g->opt.max_log_kappa;
     return v;
 }
 
@@ -86,13 +91,15 @@ rt_status guide_create(const rt_guide_options* o, rt_guide** out) {
         delete g;
         return cuda_fail(e, "rt_guide_create");
     }
-    int res[rtg::kLevels];
-    rtgh::level_resolutions(res);
+    if (g->opt.max_resolution < 2 || g->opt.max_resolution > (1 << 20) || !(g->opt.max_log_kappa > rtg::kKappaLo)) {
+        rt_guide_destroy(g);
+        return fail(RT_ERR_INVALID_ARG, "rt_guide_create: max_resolution in [2, 2^20], max_log_kappa > -2");
+    }
+    rtgh::level_resolutions(g->opt.max_resolution, g->res);
     rt_status st = RT_OK;
     auto check = [&](cudaError_t ce, const char* what) {
         if (st == RT_OK && ce != cudaSuccess) st = cuda_fail(ce, what);
     };
-    check(rtgh::set_resolutions(res), "rt_guide_create: level table");
     check(rtgh::prepare_kernels(), "rt_guide_create: kernel attributes");
     const size_t tb = size_t(rtg::kTableParams) * 4, mb = size_t(rtg::kMlpParams) * 4;
     check(g->table.alloc(tb), "rt_guide_create: allocate");
@@ -142,8 +149,9 @@ rtg::NetView guide_view(const rt_guide* g, float3 lo, float3 inv_ext) {
 // Gradient of `n` device samples (scale multiplies every weight) followed by
 // one Adam step, all on `st`.
 rt_status guide_train_device(rt_guide* g, const float* pos, const float* dir, const float* weight, int n, float scale,
-                             cudaStream_t st) {
-    rtgh::launch_backward(view(g), pos, dir, weight, n, scale, g->gtable.as<float>(), g->gmlp.as<float>(),
+                             const float* weight_sum, cudaStream_t st) {
+    GD_CUDA(cudaMemsetAsync(g->loss.ptr, 0, 4, st), "guide training step");
+    rtgh::launch_backward(view(g), pos, dir, weight, n, scale, weight_sum, g->gtable.as<float>(), g->gmlp.as<float>(),
                           g->loss.as<float>(), g->sms, st);
     g->step++;
     rtgh::launch_adam(g->table.as<float>(), g->table16.as<__half>(), g->gtable.as<float>(), g->mt.as<float>(),
@@ -164,7 +172,9 @@ void rt_guide_options_default(rt_guide_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->learning_rate = 1e-2f;
+    o->max_resolution = 64;
     o->seed = 1;
+    o->max_log_kappa = 4.0f;
 }
 
 rt_status rt_guide_create(const rt_guide_options* o, rt_guide** out) {
@@ -234,7 +244,7 @@ rt_status rt_guide_gradients(rt_guide* g, const float* pos, const float* dir, co
     GD_CUDA(cudaMemsetAsync(g->gtable.ptr, 0, g->gtable.bytes, g->stream), "rt_guide_gradients");
     GD_CUDA(cudaMemsetAsync(g->gmlp.ptr, 0, g->gmlp.bytes, g->stream), "rt_guide_gradients");
     GD_CUDA(cudaMemsetAsync(g->loss.ptr, 0, 4, g->stream), "rt_guide_gradients");
-    rtgh::launch_backward(view(g), dp.as<float>(), dd.as<float>(), dw.as<float>(), int(n), 1.0f / float(n),
+    rtgh::launch_backward(view(g), dp.as<float>(), dd.as<float>(), dw.as<float>(), int(n), 1.0f / float(n), nullptr,
                           g->gtable.as<float>(), g->gmlp.as<float>(), g->loss.as<float>(), g->sms, g->stream);
     GD_CUDA(cudaGetLastError(), "rt_guide_gradients");
     if (loss) GD_CUDA(cudaMemcpyAsync(loss, g->loss.ptr, 4, cudaMemcpyDeviceToHost, g->stream), "rt_guide_gradients");
@@ -263,10 +273,33 @@ rt_status rt_guide_train_step(rt_guide* g, const float* pos, const float* dir, c
     if (!st) st = upload(g, dw, weight, n, "rt_guide_train_step");
     if (st) return st;
     GD_CUDA(cudaMemsetAsync(g->loss.ptr, 0, 4, g->stream), "rt_guide_train_step");
-    st = guide_train_device(g, dp.as<float>(), dd.as<float>(), dw.as<float>(), int(n), float(1.0 / sum), g->stream);
+    st = guide_train_device(g, dp.as<float>(), dd.as<float>(), dw.as<float>(), int(n), float(1.0 / sum), nullptr,
+                            g->stream);
     if (st) return st;
     if (loss) GD_CUDA(cudaMemcpyAsync(loss, g->loss.ptr, 4, cudaMemcpyDeviceToHost, g->stream), "rt_guide_train_step");
     GD_CUDA(cudaStreamSynchronize(g->stream), "rt_guide_train_step");
+    return RT_OK;
+}
+
+rt_status rt_guide_set_hyperparameters(rt_guide* g, float lr, int32_t max_resolution, float max_log_kappa) {
+    if (!g) return fail(RT_ERR_INVALID_ARG, "rt_guide_set_hyperparameters: NULL guide");
+    if (max_resolution > (1 << 20) || (max_resolution > 0 && max_resolution < 2) ||
+        (max_log_kappa != 0.0f && !(max_log_kappa > rtg::kKappaLo)))
+        return fail(RT_ERR_INVALID_ARG, "rt_guide_set_hyperparameters: max_resolution in [2, 2^20], max_log_kappa > -2");
+    if (lr > 0.0f) g->opt.learning_rate = lr;
+    if (max_resolution > 0) {
+        g->opt.max_resolution = max_resolution;
+        rtgh::level_resolutions(max_resolution, g->res);
+    }
+    if (max_log_kappa != 0.0f) g->opt.max_log_kappa = max_log_kappa;
+    return RT_OK;
+}
+
+rt_status rt_guide_last_loss(rt_guide* g, float* loss, int64_t* steps) {
+    if (!g || !loss) return fail(RT_ERR_INVALID_ARG, "rt_guide_last_loss: NULL argument");
+    GD_CUDA(cudaDeviceSynchronize(), "rt_guide_last_loss");
+    GD_CUDA(cudaMemcpy(loss, g->loss.ptr, 4, cudaMemcpyDeviceToHost), "rt_guide_last_loss");
+    if (steps) *steps = g->step;
     return RT_OK;
 }
 

@@ -4,25 +4,43 @@
 #include <cuda_runtime.h>
 
 #include "rt_guide.cuh"
+#include "rt_kernels.cuh"
 
 namespace rtgh {
 
 size_t forward_smem();
 size_t backward_smem();
-cudaError_t set_resolutions(const int* res);
 cudaError_t prepare_kernels();
 // mode 0: raw outputs (n x 32 floats); mode 1: one Mixture per position.
 void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, float* raw, rtg::Mixture* mix, int sms,
                     cudaStream_t st);
+// `weight_sum` (device, may be null) replaces `scale` by 1 / *weight_sum.
 void launch_backward(const rtg::NetView& net, const float* pos, const float* dir, const float* weight, int n,
-                     float scale, float* grad_table, float* grad_mlp, float* loss, int sms, cudaStream_t st);
+                     float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss, int sms,
+                     cudaStream_t st);
+// Renderer side: mixtures of a bounce's guided vertices, training samples of
+// a wave, random training batches.
+void launch_infer(const rtd::Ctx& c, const rtg::NetView& net, int sms, cudaStream_t st);
+void launch_collect(const rtd::Ctx& c, float4* buf, int* count, int cap, cudaStream_t st);
+void launch_batch(const float4* buf, const int* count, int cap, int n, uint32_t seed, float* pos, float* dir,
+                  float* w, float* weight_sum, cudaStream_t st);
 void launch_adam(float* p, __half* p16, float* grad, float* m, float* v, int64_t n, float lr, int step,
                  cudaStream_t st);
 void launch_to_half(const float* p, __half* p16, int64_t n, cudaStream_t st);
 void launch_pdf_sample(const rtg::Mixture* mix, const float* dir, const float* u, int n, float* out_dir, float* pdf,
                        cudaStream_t st);
 
-// Level resolutions floor(16 * b^l), b = exp((ln 2048 - ln 16) / 15).
-void level_resolutions(int* res);
+// Level resolutions floor(n_min * b^l + 1e-6), b = exp((ln n_max - ln n_min) / 15), n_min = min(16, n_max).
+void level_resolutions(int n_max, int* res);
 
 }  // namespace rtgh
+
+namespace rti {
+rt_status guide_create(const rt_guide_options* o, rt_guide** out);
+rtg::NetView guide_view(const rt_guide* g, float3 lo, float3 inv_ext);
+// Gradient of n device samples (scale multiplies every weight; a non-null
+// weight_sum replaces it by 1 / *weight_sum) followed by one Adam step.
+rt_status guide_train_device(rt_guide* g, const float* pos, const float* dir, const float* weight, int n, float scale,
+                             const float* weight_sum, cudaStream_t st);
+int guide_sms(const rt_guide* g);
+}  // namespace rti

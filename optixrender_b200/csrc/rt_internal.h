@@ -67,7 +67,8 @@ struct DeviceScene {
     size_t bytes = 0;
     ~DeviceScene();
 };
-rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st);
+// Builds the wide BVH (on the device unless host_build) and uploads everything.
+rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st, bool host_build = false);
 void grid_majorants(const float* dens, const int res[3], int mres, std::vector<float>& out);
 
 }  // namespace rti

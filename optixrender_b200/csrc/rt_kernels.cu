@@ -27,13 +27,6 @@ namespace rtd {
 constexpr int kBlock = 128;
 constexpr int kStaleTextured = 1 << 30;  // stale.w flag: the slot's mat_tex holds the last hit's material
 
-RT_D const WaveParams& wave_of(const Ctx& c) { return c.waves[*c.wave_index]; }
-
-RT_D int find_segment(const WaveParams& w, int slot) {
-    int s = w.num_seg - 1;
-    while (s > 0 && slot < w.seg[s].slot_begin) s--;
-    return s;
-}
 
 RT_D int warp_fetch(int* counter, int lane) {
     int base = 0;
@@ -116,6 +109,9 @@ __global__ void k_raygen(Ctx c) {
     b.stale[slot] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
     b.rng[slot] = make_uint2(uint32_t(rng.state), uint32_t(rng.state >> 32));
     b.queue[0][slot] = slot;
+    if (c.G.rec != nullptr)
+        for (int r = 0; r < rtg::kGuideRec; r++)
+            c.G.rec[(size_t(r) * 4 + 1) * size_t(b.capacity) + slot] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // ------------------------------------------------------------------ extend
@@ -279,7 +275,14 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
             v3 radiance = xyz(r4);
             radiance += xyz(n0);
             radiance += xyz(n1);
+            const rtg::GuideCtx& G = c.G;
+            const size_t cap = size_t(B.capacity);
+            if (G.rec != nullptr && bounce >= 1 && bounce - 1 < rtg::kGuideRec)  // radiance before the next vertex
+                G.rec[(size_t(bounce - 1) * 4 + 3) * cap + slot] = f4(radiance, 0.0f);
             v3 V = -d, L = d;
+            float gp = 0.0f;  // probability of sampling the guiding mixture at this vertex
+            float rec_pdf = 0.0f, rec_cos = 0.0f;
+            float3 gin = make_float3(0.f, 0.f, 0.f);  // network input of this vertex
             // ---- closest hit / miss programs (devicePrograms.cu:71-132, 148-159)
             int tri = __float_as_int(h4.w);
             Surf s;
@@ -327,6 +330,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                     stale_mesh = mesh | kStaleTextured;
                 }
                 v3 P = w0 * xyz(p0) + u * xyz(p1) + v * xyz(p2);
+                if (G.rec != nullptr) gin = rtg::guide_input(o + h4.x * d, xyz(p0), xyz(p1), xyz(p2), d, G);
                 s.front = dot(d, Ns) < 0.0f;
                 s.sn = s.front ? Ns : -Ns;
                 closest = length(P - o);
@@ -354,6 +358,16 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 if (bounce == 0) {
                     B.aov_a[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
                     B.aov_n[slot] = make_float2(0.f, 0.f);
+                }
+            }
+            const rtg::Mixture* gmix = nullptr;
+            if (G.mix != nullptr && tri >= 0 && s.mat != nullptr) {
+                const float* mw = reinterpret_cast<const float*>(s.mat);  // type, roughness (plain loads)
+                const int mtype = __float_as_int(mw[0]);
+                const bool glossy = mtype == RT_MAT_CONDUCTOR || mtype == RT_MAT_CLEARCOATED_CONDUCTOR;
+                if (rtg::guided_type(mtype) && (!glossy || mw[4] >= G.min_rough)) {
+                    gp = G.prob;
+                    gmix = G.mix + slot;
                 }
             }
             // ---- analytic lights (devicePrograms.cu:270-271)
@@ -452,6 +466,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                         if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
                             float bpdf;
                             v3 f = eval_material(sc, s, V, sd, bpdf);
+                            if (gp > 0.0f) bpdf = gp * rtg::mixture_pdf(gmix, sd) + (1.0f - gp) * bpdf;
                             float ct = fabsf(dot(s.sn, sd));
                             float w = power_heuristic(lp, bpdf);
                             v3 thh(1.0f);
@@ -486,6 +501,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                         if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
                             float bpdf;
                             v3 f = eval_material(sc, s, V, sd, bpdf);
+                            if (gp > 0.0f) bpdf = gp * rtg::mixture_pdf(gmix, sd) + (1.0f - gp) * bpdf;
                             float ct = fabsf(dot(s.sn, sd));
                             float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, bpdf);
                             v3 thh(1.0f);
@@ -506,10 +522,30 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                     }
                     // BSDF sampling, devicePrograms.cu:474-477
                     float bpdf = 0.0f;
-                    v3 f = sample_material(sc, s, rng, V, L, bpdf);
-                    float ct = fabsf(dot(s.sn, L));
-                    history *= (f * ct / bpdf);
-                    pre_pdf = bpdf;
+                    if (gp > 0.0f) {
+                        // one-sample MIS of the mixture and the BSDF: the direction comes
+                        // from the mixture with probability gp, and is weighted by the
+                        // combined density gp * q + (1 - gp) * p_bsdf
+                        if (rng.next() < gp) {
+                            float u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+                            L = rtg::mixture_sample(gmix, u0, u1, u2);
+                        } else {
+                            float unused;
+                            sample_material(sc, s, rng, V, L, unused);
+                        }
+                        v3 f = eval_material(sc, s, V, L, bpdf);
+                        const float pm = gp * rtg::mixture_pdf(gmix, L) + (1.0f - gp) * bpdf;
+                        float ct = fabsf(dot(s.sn, L));
+                        history *= (f * ct / pm);
+                        pre_pdf = pm;
+                        rec_pdf = pm;
+                        rec_cos = ct;
+                    } else {
+                        v3 f = sample_material(sc, s, rng, V, L, bpdf);
+                        float ct = fabsf(dot(s.sn, L));
+                        history *= (f * ct / bpdf);
+                        pre_pdf = bpdf;
+                    }
                 }
             }
             if (alive) {
@@ -528,6 +564,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 }
             }
             cont = alive && (bounce + 1 < jp.max_depth);
+            if (G.rec != nullptr && cont && rec_pdf > 0.0f && rec_cos > 0.0f && bounce < rtg::kGuideRec) {
+                // training record: network input, pdf, direction, |cos|, throughput after this vertex
+                float4* R = G.rec + size_t(bounce) * 4 * cap + slot;
+                R[0] = make_float4(gin.x, gin.y, gin.z, rec_pdf);
+                R[cap] = f4(L, rec_cos);
+                R[2 * cap] = f4(history, 0.0f);
+            }
             B.rad[slot] = f4(radiance, 0.0f);
             B.nee0[slot] = f4(nee_e, 0.0f);
             B.nee1[slot] = f4(nee_l, 0.0f);

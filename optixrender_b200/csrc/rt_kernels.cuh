@@ -7,6 +7,7 @@
 #pragma once
 
 #include "rt_device.cuh"
+#include "rt_guide.cuh"
 
 namespace rtd {
 
@@ -101,7 +102,19 @@ struct Ctx {
     int wave_ring;    // number of WaveParams entries; the index wraps around
     int bounce;
     int max_depth;  // largest max_depth of the jobs in the wave
+    rtg::GuideCtx G;  // path guiding (G.mix null: not guided)
 };
+
+#ifdef __CUDACC__
+RT_D const WaveParams& wave_of(const Ctx& c) { return c.waves[*c.wave_index]; }
+
+// The segment of a wave that holds `slot`.
+RT_D int find_segment(const WaveParams& w, int slot) {
+    int s = w.num_seg - 1;
+    while (s > 0 && slot < w.seg[s].slot_begin) s--;
+    return s;
+}
+#endif
 
 }  // namespace rtd
 

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "rt_bvh.h"
+#include "rt_guide_host.h"
 #include "rt_internal.h"
 
 using namespace rtd;
@@ -50,11 +51,15 @@ void grid_majorants(const float* dens, const int res[3], int mres, std::vector<f
             }
 }
 
-rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st) {
+rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st, bool host_build) {
     const int64_t nt = int64_t(s.tri_mesh.size());
     rth::BuiltBvh bvh;
     std::string err;
-    if (!rth::build_cwbvh(s.tv.data(), nt, bvh, err)) return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
+    if (host_build) {
+        if (!rth::build_cwbvh(s.tv.data(), nt, bvh, err)) return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
+    } else if (!rth::build_cwbvh_gpu(s.tv.data(), nt, bvh, err, st)) {
+        return fail(RT_ERR_CUDA, err);
+    }
     if (bvh.depth > kStackSize)
         return fail(RT_ERR_UNSUPPORTED, "BVH too deep for the traversal stack (" + std::to_string(bvh.depth) + " levels)");
     ds.bvh_depth = bvh.depth;
@@ -222,9 +227,21 @@ struct rt_renderer {
     int waves = 0;
     int extend_launches = 0;
     int64_t paths = 0;
+    // path guiding
+    float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {1.f, 1.f, 1.f};  // scene bounds
+    rt_guide* guide = nullptr;
+    DevBuf g_mix, g_rec, g_buf, g_count, g_bpos, g_bdir, g_bw, g_wsum;
+    int g_cap = 0;             // slots covered by g_mix
+    int64_t guide_trained = 0; // samples per pixel rendered while training
+    uint32_t guide_seed = 1;
+    bool graph_guided = false;
+    const void* graph_mix = nullptr;
 };
 
 namespace {
+
+constexpr int kGuideBatch = 1 << 18;
+constexpr int kGuidedWaveMax = 1 << 24;
 
 rt_status ensure_pixels(rt_renderer* r, int w, int h) {
     if (r->pw == w && r->ph == h) return RT_OK;
@@ -279,11 +296,47 @@ int auto_capacity(const rt_options& o, int64_t npix, int64_t total) {
     return int(std::max<int64_t>(cap, 1));
 }
 
+// Guiding network and its per-slot buffers: mixtures for `cap` slots, and
+// for training waves of `train_slots` paths the records, the sample buffer
+// and one batch.
+rt_status ensure_guide(rt_renderer* r, int cap, int64_t train_slots) {
+    if (!r->guide) {
+        rt_guide_options go;
+        rt_guide_options_default(&go);
+        go.seed = r->opt.seed;
+        rt_status st = guide_create(&go, &r->guide);
+        if (st) return st;
+    }
+    if (r->g_cap < cap) {
+        RT_CUDA(r->g_mix.alloc(size_t(cap) * sizeof(rtg::Mixture)), "allocate guide mixtures");
+        r->g_cap = cap;
+    }
+    if (train_slots > 0) {
+        const size_t rec = size_t(rtg::kGuideRec) * 4 * size_t(r->capacity) * sizeof(float4);
+        if (r->g_rec.bytes < rec) RT_CUDA(r->g_rec.alloc(rec), "allocate guide records");
+        const size_t buf = size_t(rtg::kGuideRec) * size_t(train_slots) * 32;
+        if (r->g_buf.bytes < buf) RT_CUDA(r->g_buf.alloc(buf), "allocate guide samples");
+        if (!r->g_count.ptr) RT_CUDA(r->g_count.alloc(sizeof(int)), "allocate guide samples");
+        if (!r->g_wsum.ptr) RT_CUDA(r->g_wsum.alloc(sizeof(float)), "allocate guide batch");
+        if (!r->g_bw.ptr) {
+            RT_CUDA(r->g_bpos.alloc(size_t(kGuideBatch) * 12), "allocate guide batch");
+            RT_CUDA(r->g_bdir.alloc(size_t(kGuideBatch) * 12), "allocate guide batch");
+            RT_CUDA(r->g_bw.alloc(size_t(kGuideBatch) * 4), "allocate guide batch");
+        }
+    }
+    return RT_OK;
+}
+
 rt_status check_options(const rt_options* o) {
     if (o->spp < 1 || o->max_depth < 1) return fail(RT_ERR_INVALID_ARG, "spp and max_depth must be >= 1");
     if (o->width < 0 || o->height < 0) return fail(RT_ERR_INVALID_ARG, "negative frame size");
     if (int64_t(o->width) * o->height > (int64_t(1) << 28)) return fail(RT_ERR_INVALID_ARG, "frame too large");
     if (o->rng != RT_RNG_LCG && o->rng != RT_RNG_PCG32) return fail(RT_ERR_INVALID_ARG, "unknown rng");
+    if (o->bvh_build != RT_BVH_GPU && o->bvh_build != RT_BVH_HOST) return fail(RT_ERR_INVALID_ARG, "unknown bvh_build");
+    if (o->guided && o->rng != RT_RNG_PCG32)
+        return fail(RT_ERR_INVALID_ARG, "guided rendering needs PCG32 streams (rng = RT_RNG_PCG32)");
+    if (o->guided && (!(o->guide_prob > 0.0f) || o->guide_prob > 1.0f || o->guide_train_spp < 0 || o->guide_steps < 0))
+        return fail(RT_ERR_INVALID_ARG, "guide_prob must be in (0, 1], guide_train_spp and guide_steps >= 0");
     if (o->filter < RT_FILTER_BOX || o->filter > RT_FILTER_GAUSSIAN) return fail(RT_ERR_INVALID_ARG, "unknown filter");
     return RT_OK;
 }
@@ -311,7 +364,11 @@ rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_rende
     r->opt = o;
     if (const char* v = std::getenv("RT_SORT_SHADE")) r->sort_shade = std::atoi(v) != 0;
     rt_camera_default(&r->cam);
-    st = upload_scene(*s, r->ds, r->stream);
+    st = upload_scene(*s, r->ds, r->stream, o.bvh_build == RT_BVH_HOST);
+    for (int a = 0; a < 3; a++) {
+        r->lo[a] = s->lo[a];
+        r->hi[a] = s->hi[a];
+    }
     if (st == RT_OK) {
         e = cudaEventCreate(&r->ev0);
         if (e == cudaSuccess) e = cudaEventCreate(&r->ev1);
@@ -337,6 +394,7 @@ rt_status rt_renderer_destroy(rt_renderer* r) {
     if (!r) return RT_OK;
     if (r->stream) cudaStreamSynchronize(r->stream);
     if (r->graph) cudaGraphExecDestroy(r->graph);
+    if (r->guide) rt_guide_destroy(r->guide);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
     if (r->own_stream && r->stream) cudaStreamDestroy(r->stream);
@@ -402,10 +460,22 @@ rt_status rt_renderer_render(rt_renderer* r) {
     if (st) return st;
     const int64_t npix = int64_t(o.width) * o.height;
     const int64_t total = npix * o.spp;
-    const int cap = auto_capacity(o, npix, total);
+    const bool guided = o.guided != 0;
+    int cap = auto_capacity(o, npix, total);
+    if (guided) cap = std::min(cap, kGuidedWaveMax);
+    // guided: the first training samples run one sample per pixel per wave
+    const int64_t train_waves =
+        guided && npix <= int64_t(kGuidedWaveMax)
+            ? std::min<int64_t>(o.spp, std::max<int64_t>(0, int64_t(o.guide_train_spp) - r->guide_trained))
+            : 0;
+    const int wave_cap = train_waves > 0 ? std::max<int>(cap, int(npix)) : cap;
     r->wave_paths = cap;
-    st = ensure_waves(r, cap);
+    st = ensure_waves(r, wave_cap);
     if (st) return st;
+    if (guided) {
+        st = ensure_guide(r, wave_cap, train_waves > 0 ? npix : 0);
+        if (st) return st;
+    }
     if (!o.progressive) r->frame = 0;  // Renderer.cpp:642-644
     JobDesc hj;
     std::memset(&hj, 0, sizeof(hj));
@@ -435,17 +505,20 @@ rt_status rt_renderer_render(rt_renderer* r) {
     r->frame++;
     cudaStream_t s = r->stream;
     RT_CUDA(cudaMemcpyAsync(r->job.ptr, &hj, sizeof(hj), cudaMemcpyHostToDevice, s), "upload launch parameters");
-    const int64_t nwaves = (total + cap - 1) / cap;
+    const int64_t trained_paths = train_waves * npix;
+    const int64_t nwaves = train_waves + (total - trained_paths + cap - 1) / cap;
     std::vector<WaveParams> waves(static_cast<size_t>(nwaves));
+    int64_t begin = 0;
     for (int64_t w = 0; w < nwaves; w++) {
         WaveParams& wp = waves[size_t(w)];
         std::memset(&wp, 0, sizeof(wp));
         wp.num_seg = 1;
-        wp.wave_count = int(std::min<int64_t>(cap, total - w * cap));
+        wp.wave_count = int(std::min<int64_t>(w < train_waves ? npix : cap, total - begin));
         wp.seg[0].job = 0;
         wp.seg[0].slot_begin = 0;
         wp.seg[0].count = wp.wave_count;
-        wp.seg[0].path_begin = w * cap;
+        wp.seg[0].path_begin = begin;
+        begin += wp.wave_count;
     }
     RT_CUDA(r->segs.alloc(waves.size() * sizeof(WaveParams)), "allocate wave table");
     RT_CUDA(cudaMemcpyAsync(r->segs.ptr, waves.data(), waves.size() * sizeof(WaveParams), cudaMemcpyHostToDevice, s),
@@ -487,7 +560,25 @@ rt_status rt_renderer_render(rt_renderer* r) {
     c.wave_index = r->wave_index.as<int>();
     c.wave_ring = int(nwaves);
     c.max_depth = o.max_depth;
-    auto issue_wave = [&](bool timed) {
+    rtg::NetView net{};
+    if (guided) {
+        float3 lo, inv;
+        for (int a = 0; a < 3; a++) {  // 1% margin around the scene bounds
+            const float ext = std::max(r->hi[a] - r->lo[a], 1e-6f);
+            (&lo.x)[a] = r->lo[a] - 0.01f * ext;
+            (&inv.x)[a] = 1.0f / (1.02f * ext);
+        }
+        net = guide_view(r->guide, lo, inv);
+        c.G.mix = r->g_mix.as<rtg::Mixture>();
+        c.G.prob = o.guide_prob;
+        c.G.min_rough = 0.3f;
+        c.G.lo = lo;
+        c.G.inv_ext = inv;
+    }
+    const int gsms = guided ? guide_sms(r->guide) : 0;
+    auto issue_wave = [&](bool timed, bool training) {
+        c.G.rec = training ? r->g_rec.as<float4>() : nullptr;
+        if (training) cudaMemsetAsync(r->g_count.ptr, 0, sizeof(int), s);
         c.bounce = 0;
         rth::launch_raygen(c, s);
         for (int bnc = 0; bnc < o.max_depth; bnc++) {
@@ -496,6 +587,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
             if (timed) cudaEventRecord(r->timer.next(), s);
             rth::launch_extend(c, r->shape, timed, s);
             if (timed) cudaEventRecord(r->timer.next(), s);
+            if (guided) rtgh::launch_infer(c, net, gsms, s);
             rth::launch_shade(c, r->shape, timed, s);
             if (timed) cudaEventRecord(r->timer.next(), s);
             rth::launch_shadow(c, r->shape, timed, s);
@@ -507,19 +599,36 @@ rt_status rt_renderer_render(rt_renderer* r) {
             }
         }
         rth::launch_resolve(c, s);
+        if (training) rtgh::launch_collect(c, r->g_buf.as<float4>(), r->g_count.as<int>(), int(r->g_buf.bytes / 32), s);
         rth::launch_next_wave(c, s);
     };
+    // training waves, each followed by guide_steps Adam steps on batches of its samples
+    for (int64_t w = 0; w < train_waves; w++) {
+        issue_wave(stats, true);
+        for (int k = 0; k < o.guide_steps; k++) {
+            RT_CUDA(cudaMemsetAsync(r->g_wsum.ptr, 0, sizeof(float), s), "guide batch");
+            rtgh::launch_batch(r->g_buf.as<float4>(), r->g_count.as<int>(), int(r->g_buf.bytes / 32), kGuideBatch,
+                               r->guide_seed++ * 0x9E3779B9u, r->g_bpos.as<float>(), r->g_bdir.as<float>(),
+                               r->g_bw.as<float>(), r->g_wsum.as<float>(), s);
+            st = guide_train_device(r->guide, r->g_bpos.as<float>(), r->g_bdir.as<float>(), r->g_bw.as<float>(),
+                                    kGuideBatch, 1.0f, r->g_wsum.as<float>(), s);
+            if (st) return st;
+        }
+    }
+    r->guide_trained += train_waves;
+    const int64_t plain_waves = nwaves - train_waves;
     // graph capture is not possible on the legacy default stream
     if (stats || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
-        for (int64_t w = 0; w < nwaves; w++) issue_wave(stats);
-    } else {
+        for (int64_t w = 0; w < plain_waves; w++) issue_wave(stats, false);
+    } else if (plain_waves > 0) {
         if (!r->graph || r->graph_capacity != r->capacity || r->graph_depth != o.max_depth ||
-            r->graph_waves != r->segs.ptr || r->graph_ring != int(nwaves)) {
+            r->graph_waves != r->segs.ptr || r->graph_ring != int(nwaves) || r->graph_guided != guided ||
+            r->graph_mix != r->g_mix.ptr) {
             if (r->graph) cudaGraphExecDestroy(r->graph);
             r->graph = nullptr;
             cudaGraph_t g = nullptr;
             RT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin graph capture");
-            issue_wave(false);
+            issue_wave(false, false);
             RT_CUDA(cudaStreamEndCapture(s, &g), "end graph capture");
             cudaError_t e = cudaGraphInstantiate(&r->graph, g, 0);
             cudaGraphDestroy(g);
@@ -528,10 +637,13 @@ rt_status rt_renderer_render(rt_renderer* r) {
             r->graph_depth = o.max_depth;
             r->graph_waves = r->segs.ptr;
             r->graph_ring = int(nwaves);
+            r->graph_guided = guided;
+            r->graph_mix = r->g_mix.ptr;
         }
-        for (int64_t w = 0; w < nwaves; w++) RT_CUDA(cudaGraphLaunch(r->graph, s), "launch wave graph");
+        for (int64_t w = 0; w < plain_waves; w++) RT_CUDA(cudaGraphLaunch(r->graph, s), "launch wave graph");
     }
-    launches += int(nwaves) * (3 * o.max_depth + 3);
+    launches += int(nwaves) * (3 * o.max_depth + 3) + (guided ? int(nwaves) * o.max_depth : 0) +
+                int(train_waves) * (1 + 3 * o.guide_steps);
     ext = int(nwaves) * o.max_depth;
     rth::launch_finalize(hj, dj, s);
     launches++;
@@ -542,6 +654,33 @@ rt_status rt_renderer_render(rt_renderer* r) {
     r->waves = int(nwaves);
     r->extend_launches = ext;
     r->paths = total;
+    return RT_OK;
+}
+
+rt_status rt_renderer_guide(rt_renderer* r, rt_guide** guide) {
+    if (!r || !guide) return fail(RT_ERR_INVALID_ARG, "rt_renderer_guide: NULL argument");
+    if (!r->guide) {
+        rt_status st = ensure_guide(r, 0, 0);
+        if (st) return st;
+    }
+    *guide = r->guide;
+    return RT_OK;
+}
+
+rt_status rt_renderer_guide_samples(rt_renderer* r, float* out, int64_t max_samples, int64_t* count) {
+    if (!r || !count) return fail(RT_ERR_INVALID_ARG, "rt_renderer_guide_samples: NULL argument");
+    *count = 0;
+    if (!r->g_count.ptr) return RT_OK;
+    int n = 0;
+    RT_CUDA(cudaMemcpyAsync(&n, r->g_count.ptr, sizeof(int), cudaMemcpyDeviceToHost, r->stream), "guide samples");
+    RT_CUDA(cudaStreamSynchronize(r->stream), "guide samples");
+    const int64_t cap = int64_t(r->g_buf.bytes / 32);
+    *count = std::min<int64_t>(n, cap);
+    const int64_t k = std::min<int64_t>(*count, max_samples);
+    if (out && k > 0) {
+        RT_CUDA(cudaMemcpyAsync(out, r->g_buf.ptr, size_t(k) * 32, cudaMemcpyDeviceToHost, r->stream), "guide samples");
+        RT_CUDA(cudaStreamSynchronize(r->stream), "guide samples");
+    }
     return RT_OK;
 }
 

@@ -697,6 +697,12 @@ rt_status load_json(rt_scene* s, const std::string& text, const std::string& bas
             std::string r = str(in->get("rng"), "lcg");
             opts->rng = r == "pcg32" ? RT_RNG_PCG32 : RT_RNG_LCG;
             opts->rr_depth = int(num(in->get("rr_depth"), opts->rr_depth));
+            // learned proposal: {"guided": true, "guide_train_spp": 32, "guide_prob": 0.5, "guide_steps": 4}
+            if (const Json* gd = in->get("guided")) opts->guided = gd->kind == Json::Bool ? gd->b : int(num(gd, 0)) != 0;
+            opts->guide_train_spp = int(num(in->get("guide_train_spp"), opts->guide_train_spp));
+            opts->guide_prob = float(num(in->get("guide_prob"), opts->guide_prob));
+            opts->guide_steps = int(num(in->get("guide_steps"), opts->guide_steps));
+            if (opts->guided) opts->rng = RT_RNG_PCG32;
         }
     }
     // media first, so shapes can refer to them by name

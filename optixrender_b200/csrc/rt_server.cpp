@@ -310,7 +310,11 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
     }
     std::vector<std::pair<Job*, int64_t>> plan;
     if (!active.empty()) {
-        if (s->opt.policy == RT_SERVE_FIFO) {
+        if (s->opt.policy == RT_SERVE_FIFO || s->opt.policy == RT_SERVE_SRPT) {
+            if (s->opt.policy == RT_SERVE_SRPT)  // fewest paths left first, ties by admission
+                std::stable_sort(active.begin(), active.end(), [](const Job* a, const Job* b) {
+                    return a->total - a->issued < b->total - b->issued;
+                });
             int64_t left = s->capacity;
             for (Job* j : active) {
                 if (left == 0 || int(plan.size()) == kMaxSegments) break;
@@ -446,7 +450,7 @@ void rt_server_options_default(rt_server_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->wave_paths = 1 << 23;
-    o->max_jobs = 64;
+    o->max_jobs = 256;
     o->max_depth = 32;
     o->background = 1;
     o->waves_in_flight = 2;
@@ -460,11 +464,11 @@ rt_status rt_server_create(const rt_server_options* o, rt_server** out) {
     if (o) {
         s->opt = *o;
         if (s->opt.wave_paths <= 0) s->opt.wave_paths = 1 << 23;
-        if (s->opt.max_jobs <= 0) s->opt.max_jobs = 64;
+        if (s->opt.max_jobs <= 0) s->opt.max_jobs = 256;
         if (s->opt.max_depth <= 0) s->opt.max_depth = 32;
         if (s->opt.waves_in_flight <= 0) s->opt.waves_in_flight = 2;
     }
-    if (s->opt.policy != RT_SERVE_FAIR && s->opt.policy != RT_SERVE_FIFO) {
+    if (s->opt.policy != RT_SERVE_FAIR && s->opt.policy != RT_SERVE_FIFO && s->opt.policy != RT_SERVE_SRPT) {
         delete s;
         return fail(RT_ERR_INVALID_ARG, "rt_server_create: unknown policy");
     }

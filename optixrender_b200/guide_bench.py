@@ -1,0 +1,103 @@
+"""Time to a relative MSE, guided vs plain (the learned proposal's benchmark).
+
+relMSE = mean over pixels and channels of (I - I_ref)^2 / (I_ref^2 + 1e-2),
+where I_ref is a plain render of `--ref-spp` samples per pixel accumulated in
+FP64 on the host (frames of 256 spp with independent seeds).  Each method
+renders progressively, `--step` spp per Render() call, up to `--max-spp`; the
+time is the renderer's device time (CUDA events around every Render(), the
+guided method's training steps included).  The time to reach `--target` is
+interpolated log-log between the two checkpoints around it.
+
+    python -m optixrender_b200.guide_bench                    # 1920x1080 spheres, target 1e-3
+    python -m optixrender_b200.guide_bench --scene portal --width 256 --height 256
+"""
+import argparse
+import json
+import math
+
+import numpy as np
+
+from optixrender_b200 import scenes
+
+
+def relmse(img, ref):
+    a, b = img[..., :3].astype(np.float64), ref[..., :3].astype(np.float64)
+    return float(np.mean((a - b) ** 2 / (b * b + 1e-2)))
+
+
+def reference(spec, spp, frame_spp=256, seed=1000):
+    """Plain render of `spp` samples per pixel, FP64-accumulated over frames."""
+    s, r = scenes.build_renderer(spec, spp=min(frame_spp, spp), progressive=0)
+    acc = None
+    frames = max(1, spp // frame_spp)
+    ms = 0.0
+    for f in range(frames):
+        o = r.options
+        o.seed = seed + f
+        r.set_options(o)
+        r.render()
+        img = r.download_linear()[..., :3].astype(np.float64)
+        ms += r.stats()["ms_total"]
+        acc = img if acc is None else acc + img
+    return acc / frames, frames * min(frame_spp, spp), ms
+
+
+def curve(spec, ref, guided, step, max_spp, seed, train_spp):
+    over = dict(spp=step, progressive=1, seed=seed)
+    if guided:
+        over.update(guided=1, guide_train_spp=train_spp)
+    s, r = scenes.build_renderer(spec, **over)
+    pts = []
+    ms = 0.0
+    spp = 0
+    next_check = step
+    while spp < max_spp:
+        r.render()
+        ms += r.stats()["ms_total"]
+        spp += step
+        if spp >= next_check or spp >= max_spp:
+            pts.append({"spp": spp, "ms": ms, "relmse": relmse(r.download_linear(), ref)})
+            next_check *= 2
+    return pts
+
+
+def time_to(pts, target):
+    """Device milliseconds to reach `target`, log-log interpolated; None when not reached."""
+    prev = None
+    for p in pts:
+        if p["relmse"] <= target:
+            if prev is None:
+                return p["ms"]
+            t = (math.log(target) - math.log(prev["relmse"])) / (math.log(p["relmse"]) - math.log(prev["relmse"]))
+            return math.exp(math.log(prev["ms"]) + t * (math.log(p["ms"]) - math.log(prev["ms"])))
+        prev = p
+    return None
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scene", default="spheres", choices=sorted(scenes.SCENES))
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--ref-spp", type=int, default=65536)
+    ap.add_argument("--max-spp", type=int, default=4096)
+    ap.add_argument("--step", type=int, default=16)
+    ap.add_argument("--train-spp", type=int, default=32)
+    ap.add_argument("--target", type=float, default=1e-3)
+    a = ap.parse_args(argv)
+    spec = scenes.SCENES[a.scene](a.width, a.height, 1)
+    ref, ref_spp, ref_ms = reference(spec, a.ref_spp)
+    plain = curve(spec, ref, False, a.step, a.max_spp, 7, a.train_spp)
+    guided = curve(spec, ref, True, a.step, a.max_spp, 8, a.train_spp)
+    tp, tg = time_to(plain, a.target), time_to(guided, a.target)
+    line = {"metric": f"time-to-relMSE {a.target:g}", "unit": "ms", "higher_is_better": False,
+            "plain_ms": tp, "guided_ms": tg, "speedup": (tp / tg) if (tp and tg) else None,
+            "scene": a.scene, "width": a.width, "height": a.height, "reference_spp": ref_spp,
+            "reference_ms": ref_ms, "train_spp": a.train_spp, "step_spp": a.step,
+            "plain": plain, "guided": guided, "data": "synthetic"}
+    print(json.dumps(line))
+    return line
+
+
+if __name__ == "__main__":
+    main()

@@ -23,7 +23,7 @@ from typing import Optional
 
 import numpy as np
 
-from . import (FILTER_GAUSSIAN, LIGHT_QUAD, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_DIFFUSE, MAT_METAL_WORKFLOW, MAT_PLASTIC,
+from . import (FILTER_BOX, FILTER_GAUSSIAN, LIGHT_QUAD, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_DIFFUSE, MAT_METAL_WORKFLOW, MAT_PLASTIC,
                MEDIUM_GRID, MEDIUM_HOMOGENEOUS, PHASE_HG, PHASE_ISOTROPIC, RNG_PCG32, Renderer, Scene, camera,
                light, material, medium, options)
 
@@ -230,6 +230,46 @@ def cornell(width=256, height=256, spp=16, seed=1):
     return SceneSpec("cornell", meshes, lights, [], None, cam, settings)
 
 
+def portal(width=96, height=96, spp=16, seed=1):
+    """A closed diffuse room split by a wall with a 0.2 x 0.2 opening; the only
+    light (a quad under the ceiling, facing down) is behind the wall, so the
+    camera's half of the room (dark grey surfaces) is lit through the opening
+    by the bright walls of the far half: next-event estimation rarely connects
+    and cosine-weighted BSDF sampling rarely finds the opening, the case a
+    learned proposal is for."""
+    bright = dict(type=MAT_DIFFUSE, albedo=(0.8, 0.8, 0.8), roughness=0.0)
+    warm = dict(type=MAT_DIFFUSE, albedo=(0.85, 0.65, 0.45), roughness=0.0)
+    dark = dict(type=MAT_DIFFUSE, albedo=(0.3, 0.3, 0.3), roughness=0.0)
+    meshes = []
+    # the camera's half (z < 0.5) is dark grey, the lit half bright
+    for z0, z1, m in [(0.0, 0.5, dark), (0.5, 1.0, bright)]:
+        dz = z1 - z0
+        for p, u, v in [((0, 0, z0), (1, 0, 0), (0, 0, dz)),      # floor (normal +y)
+                        ((0, 1, z0), (0, 0, dz), (1, 0, 0)),      # ceiling (-y)
+                        ((0, 0, z0), (0, 0, dz), (0, 1, 0)),      # left (+x)
+                        ((1, 0, z0), (0, 1, 0), (0, 0, dz))]:     # right (-x)
+            verts, f = quad(p, u, v)
+            meshes.append(MeshSpec(verts, f, m))
+    for p, u, v, m in [((0, 0, 1), (1, 0, 0), (0, 1, 0), warm),   # back wall, facing the room
+                       ((0, 0, 0), (0, 1, 0), (1, 0, 0), dark)]:  # front wall
+        verts, f = quad(p, u, v)
+        meshes.append(MeshSpec(verts, f, m))
+    # divider at z = 0.5 with an opening x in [0.4, 0.6], y in [0.4, 0.6]
+    z = 0.5
+    for (x0, x1, y0, y1) in [(0.0, 1.0, 0.0, 0.4), (0.0, 1.0, 0.6, 1.0), (0.0, 0.4, 0.4, 0.6), (0.6, 1.0, 0.4, 0.6)]:
+        verts, f = quad((x0, y0, z), (x1 - x0, 0, 0), (0, y1 - y0, 0))   # facing +z (the lit half)
+        meshes.append(MeshSpec(verts, f, bright))
+        verts, f = quad((x0, y0, z), (0, y1 - y0, 0), (x1 - x0, 0, 0))   # facing -z (the camera)
+        meshes.append(MeshSpec(verts, f, dark))
+    lights = [dict(type=LIGHT_QUAD, position=(0.35, 0.999, 0.7), u=(0.0, 0.0, 0.2), v=(0.3, 0.0, 0.0),
+                   radiance=(40.0, 36.0, 30.0), double_side=0)]
+    # looking down at the floor and walls of the dark half, which see the opening
+    cam = dict(from_=(0.5, 0.9, 0.03), at=(0.5, 0.0, 0.4), up=(0, 1, 0), fov_y_deg=0.0)
+    settings = dict(width=width, height=height, spp=spp, max_depth=8, rr_depth=3, rng=RNG_PCG32, seed=seed,
+                    filter=FILTER_BOX)
+    return SceneSpec("portal", meshes, lights, [], None, cam, settings)
+
+
 def textured(width=128, height=128, spp=16, seed=1):
     """The Cornell room with material textures: a checker albedo on the floor
     (uv repeated 3x, wrap), a bump normal map on the back wall, a roughness
@@ -405,4 +445,4 @@ def build_renderer(spec: SceneSpec, **overrides) -> tuple:
     return s, r
 
 
-SCENES = {"cornell": cornell, "spheres": spheres, "media": media, "textured": textured}
+SCENES = {"cornell": cornell, "spheres": spheres, "media": media, "textured": textured, "portal": portal}

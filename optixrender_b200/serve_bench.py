@@ -134,9 +134,9 @@ def main(argv=None):
     p.add_argument("--requests", type=int, default=1000)
     p.add_argument("--load", type=float, default=0.8)
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--policy", default="fair", choices=["fair", "fifo"])
+    p.add_argument("--policy", default="fair", choices=["fair", "fifo", "srpt"])
     p.add_argument("--wave-paths", type=int, default=1 << 23)
-    p.add_argument("--max-jobs", type=int, default=64)
+    p.add_argument("--max-jobs", type=int, default=256)
     p.add_argument("--small", action="store_true", help="small scenes and resolutions (tests)")
     a = p.parse_args(argv)
     specs, keep = build_scenes(a.small)
@@ -144,7 +144,8 @@ def main(argv=None):
     spps = [1, 2, 4, 8] if a.small else SPPS
     reqs = make_requests(a.requests, specs, a.seed, res, spps)
     srv = rt.Server(rt.server_options(wave_paths=a.wave_paths, max_jobs=a.max_jobs, max_depth=32,
-                                      policy=rt.SERVE_FAIR if a.policy == "fair" else rt.SERVE_FIFO))
+                                      policy={"fair": rt.SERVE_FAIR, "fifo": rt.SERVE_FIFO,
+                                              "srpt": rt.SERVE_SRPT}[a.policy]))
     ids = [srv.add_scene(s) for s in keep]
     warm = make_requests(4, specs, a.seed + 1, res[:1], spps[:1])
     run_stream(srv, warm, ids, [0.0] * len(warm))  # graphs captured, scenes touched

@@ -5,8 +5,9 @@ guiding kernels.  The network has no counterpart in the reference renderer;
 it restates published methods:
 
 * multiresolution hash encoding (Mueller, Evans, Schied, Keller, "Instant
-  Neural Graphics Primitives", SIGGRAPH 2022): 16 levels, 2 features per
-  level, 2^19 entries per level, trilinear interpolation of the 8 cell
+  Neural Graphics Primitives", SIGGRAPH 2022): 16 levels of geometrically
+  growing resolution from 16 to 64 (any finest resolution may be chosen), 2
+  features per level, 2^19 entries per level, trilinear interpolation of the 8 cell
   corners, dense indexing where the level's grid fits the table and the
   spatial hash (x * 1) ^ (y * 2654435761) ^ (z * 805459861) mod 2^19 elsewhere;
 * a 32 -> 64 -> 64 -> 64 -> 32 MLP without biases, ReLU on the hidden layers;
@@ -29,16 +30,18 @@ import numpy as np
 
 LEVELS, FEATS, LOG2_T = 16, 2, 19
 T = 1 << LOG2_T
-N_MIN, N_MAX = 16, 2048
+N_MIN, N_MAX = 16, 64   # coarsest level min(16, n_max), finest n_max
 LAYERS = [(64, 32), (64, 64), (64, 64), (32, 64)]  # (out, in)
 LOBES = 8
-KAPPA_LO, KAPPA_HI = -2.0, 9.0
+KAPPA_LO, KAPPA_HI = -2.0, 4.0
 PRIMES = (1, 2654435761, 805459861)
 
 
-def level_resolutions():
-    b = math.exp((math.log(N_MAX) - math.log(N_MIN)) / (LEVELS - 1))
-    return [int(math.floor(N_MIN * b ** l)) for l in range(LEVELS)]
+def level_resolutions(n_max=None):
+    n_max = N_MAX if n_max is None else n_max
+    lo = min(N_MIN, n_max)
+    b = math.exp((math.log(n_max) - math.log(lo)) / (LEVELS - 1))
+    return [int(math.floor(lo * b ** l + 1e-6)) for l in range(LEVELS)]
 
 
 def mlp_param_count():

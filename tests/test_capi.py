@@ -43,7 +43,7 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(rt.Material) == 120
     assert C.sizeof(rt.Light) == 64
     assert C.sizeof(rt.Medium) == 96
-    assert C.sizeof(rt.Options) == 56
+    assert C.sizeof(rt.Options) == 80
     assert C.sizeof(rt.Camera) == 44
     assert C.sizeof(rt.MeshDesc) == 48
 

@@ -41,7 +41,7 @@ def _alone(spec, **over):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("wave_paths,policy", [(4096, rt.SERVE_FAIR), (1 << 16, rt.SERVE_FAIR),
-                                               (4096, rt.SERVE_FIFO)])
+                                               (4096, rt.SERVE_FIFO), (4096, rt.SERVE_SRPT)])
 def test_jobs_in_a_mix_match_renders_alone_bitwise(wave_paths, policy):
     specs = _specs()
     srv = rt.Server(rt.server_options(wave_paths=wave_paths, max_jobs=8, max_depth=32, policy=policy))

@@ -83,33 +83,36 @@ def test_oracle_gradients_match_finite_differences(monkeypatch):
 
 
 def test_level_resolutions():
-    assert go.level_resolutions()[0] == 16 and go.level_resolutions()[-1] == 2048
+    assert go.level_resolutions()[0] == 16 and go.level_resolutions()[-1] == 64
+    assert go.level_resolutions(2048)[-1] == 2048 and go.level_resolutions(8)[0] == 8
 
 
 @pytest.mark.gpu
-def test_forward_matches_oracle():
+@pytest.mark.parametrize("n_max", [64, 2048])  # dense levels only / dense and hashed levels
+def test_forward_matches_oracle(n_max):
     import optixrender_b200 as rt
     table, ws = _params(11)
-    g = rt.Guide()
+    g = rt.Guide(max_resolution=n_max)
     g.set_params(table.reshape(-1), np.concatenate([w.reshape(-1) for w in ws]))
     pos, _, _ = _samples(2048, 12)
     out = g.forward(pos)
     t16, w16 = _to16(table, ws)
-    ref, _ = go.forward(t16, w16, pos, go.level_resolutions())
+    ref, _ = go.forward(t16, w16, pos, go.level_resolutions(n_max))
     print("forward rel", _rel(out, ref), "cos", _cos(out, ref))
     assert _rel(out, ref) < 2e-2 and _cos(out, ref) > 0.999
 
 
 @pytest.mark.gpu
-def test_gradients_match_oracle():
+@pytest.mark.parametrize("n_max", [64, 2048])
+def test_gradients_match_oracle(n_max):
     import optixrender_b200 as rt
     table, ws = _params(21, table_scale=0.5, out_scale=0.3)
-    g = rt.Guide()
+    g = rt.Guide(max_resolution=n_max)
     g.set_params(table.reshape(-1), np.concatenate([w.reshape(-1) for w in ws]))
     pos, d, w = _samples(1024, 22)
     loss, gt, gm = g.gradients(pos, d, w)
     t16, w16 = _to16(table, ws)
-    rloss, rgt, rgw, _ = go.loss_and_grads(t16, w16, pos, d, w.astype(np.float64), go.level_resolutions())
+    rloss, rgt, rgw, _ = go.loss_and_grads(t16, w16, pos, d, w.astype(np.float64), go.level_resolutions(n_max))
     print("loss", loss, rloss)
     assert abs(loss - rloss) <= 1e-2 * abs(rloss)
     off = 0

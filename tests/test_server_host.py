@@ -33,7 +33,7 @@ def test_server_struct_layouts_match_the_header(tmp_path):
 
 def test_server_defaults():
     o = rt.server_options()
-    assert (o.wave_paths, o.max_jobs, o.max_depth, o.background, o.waves_in_flight) == (1 << 23, 64, 32, 1, 2)
+    assert (o.wave_paths, o.max_jobs, o.max_depth, o.background, o.waves_in_flight) == (1 << 23, 256, 32, 1, 2)
     j = rt.job(0, rt.camera((0, 0, 1), (0, 0, 0)), 8, 8, 1)
     assert (j.max_depth, j.rr_depth, j.filter, j.seed) == (25, 0, rt.FILTER_GAUSSIAN, 1)
 
