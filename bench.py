@@ -286,8 +286,7 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = paths_per_step * world / (e2e_ms / 1e3) / 1e6
-    waves = int(np.ceil(paths_per_step / min(paths_per_step, max(W * H, 1 << 21))))
-    h2d = 296 + 24 * waves
+    h2d = int(r.stats()["h2d_bytes"])  # launch parameters + wave table uploaded by each Render()
 
     peak, peak_kind = measured_peak()
     ext_bytes = (counters["extend_nodes"] * NODE_BYTES + counters["extend_tris"] * TRI_BYTES +

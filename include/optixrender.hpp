@@ -106,6 +106,18 @@ public:
         check(rt_scene_add_mesh(h_, &d, &material, out_med, in_med, &id));
         return id;
     }
+    // Scene::AddTexture(fileName) (Scene.cpp:66-69): BMP or binary PGM/PPM.
+    int AddTexture(const std::string& fileName) {
+        int32_t id = -1;
+        check(rt_scene_add_texture_file(h_, fileName.c_str(), &id));
+        return id;
+    }
+    // A decoded RGBA8 image, row 0 at the bottom (v = 0).
+    int AddTexture(const std::vector<uint8_t>& rgba, int width, int height) {
+        int32_t id = -1;
+        check(rt_scene_add_texture(h_, rgba.data(), width, height, &id));
+        return id;
+    }
     void AddLight(const Light& l) { check(rt_scene_add_light(h_, &l)); }
     void AddMedium(const Medium& m) { check(rt_scene_add_medium(h_, &m)); }
     // Scene::AddEnv with an equirectangular RGBA float image (row 0 at the bottom).
@@ -172,6 +184,50 @@ public:
 
 private:
     rt_renderer* h_ = nullptr;
+};
+
+// The continuous-batching server over resident scenes (rt_server_*; the
+// reference renders one frame per Renderer and has no counterpart).
+class Server {
+public:
+    explicit Server(const rt_server_options* o = nullptr) { check(rt_server_create(o, &h_)); }
+    ~Server() { rt_server_destroy(h_); }
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    int AddScene(const Scene& scene) {
+        int32_t id = -1;
+        check(rt_server_add_scene(h_, scene.handle(), &id));
+        return id;
+    }
+    int64_t Submit(const rt_job_desc& job) {
+        int64_t id = -1;
+        check(rt_server_submit(h_, &job, &id));
+        return id;
+    }
+    rt_job_status Wait(int64_t job, double timeout_ms = -1.0) {
+        rt_job_status st{};
+        check(rt_server_wait(h_, job, timeout_ms, &st));
+        return st;
+    }
+    rt_job_status Poll(int64_t job) {
+        rt_job_status st{};
+        check(rt_server_poll(h_, job, &st));
+        return st;
+    }
+    void Cancel(int64_t job) { check(rt_server_cancel(h_, job)); }
+    void DownloadPixels(int64_t job, uint32_t* pixels) { check(rt_server_download_rgba8(h_, job, pixels)); }
+    void DownloadLinear(int64_t job, float* rgba) { check(rt_server_download(h_, job, rgba)); }
+    void Release(int64_t job) { check(rt_server_release(h_, job)); }
+    rt_server_stats Stats() {
+        rt_server_stats st{};
+        check(rt_server_get_stats(h_, &st));
+        return st;
+    }
+    rt_server* handle() { return h_; }
+
+private:
+    rt_server* h_ = nullptr;
 };
 
 }  // namespace rt

@@ -210,6 +210,7 @@ typedef struct rt_render_stats {
     int64_t extend_launches;
     int64_t nan_throughput_paths; /* paths ended by IsNan(history), devicePrograms.cu:487-489 */
     int64_t wave_paths;        /* path slots per wave of the last Render() */
+    int64_t h2d_bytes;         /* bytes copied host to device by the last Render() */
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */

@@ -214,6 +214,7 @@ struct rt_renderer {
     DevBuf mat_tex;           // per-slot textured materials (scenes with textures)
     bool sort_shade = true;   // RT_SORT_SHADE=0 keeps the shade queue in extend order
     int wave_paths = 0;       // slots per wave of the last render
+    int64_t h2d_bytes = 0;    // host-to-device bytes of the last render
     DevBuf wave_index;
     // one captured wave (raygen, (extend, shade, shadow) x depth, resolve, advance)
     cudaGraphExec_t graph = nullptr;
@@ -523,6 +524,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
     RT_CUDA(r->segs.alloc(waves.size() * sizeof(WaveParams)), "allocate wave table");
     RT_CUDA(cudaMemcpyAsync(r->segs.ptr, waves.data(), waves.size() * sizeof(WaveParams), cudaMemcpyHostToDevice, s),
             "upload wave table");
+    r->h2d_bytes = int64_t(sizeof(hj) + waves.size() * sizeof(WaveParams));
     if (!r->wave_index.ptr) RT_CUDA(r->wave_index.alloc(sizeof(int)), "allocate wave counter");
     RT_CUDA(cudaMemsetAsync(r->wave_index.ptr, 0, sizeof(int), s), "clear wave counter");
     RT_CUDA(cudaMemsetAsync(r->ctl.ptr, 0, sizeof(WaveCtl), s), "clear counters");
@@ -751,6 +753,7 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     out->launches = r->launches;
     out->extend_launches = r->extend_launches;
     out->wave_paths = r->wave_paths;
+    out->h2d_bytes = r->h2d_bytes;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, r->ev0, r->ev1);
     out->ms_total = ms;

@@ -20,15 +20,16 @@ def main(argv=None) -> int:
     p.add_argument("--spp", type=int, default=2)
     p.add_argument("--frames", type=int, default=2)
     p.add_argument("--stats", type=int, default=0)
+    p.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library's choice)")
     a = p.parse_args(argv)
     from . import scenes
     spec = scenes.SCENES[a.scene](width=a.width, height=a.height, spp=a.spp)
-    s, r = scenes.build_renderer(spec, collect_stats=a.stats)
+    s, r = scenes.build_renderer(spec, collect_stats=a.stats, wave_paths=a.wave_paths)
     for _ in range(a.frames):
         r.render()
     r.synchronize()
     st = r.stats()
-    print({k: st[k] for k in ("paths", "extend_rays", "shadow_rays", "launches", "ms_total")})
+    print({k: st[k] for k in ("paths", "extend_rays", "shadow_rays", "launches", "ms_total", "wave_paths")})
     return 0
 
 

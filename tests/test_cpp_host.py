@@ -84,3 +84,30 @@ def test_cli_matches_python_api(tmp_path):
     ref = px.view(np.uint8).reshape(px.shape + (4,))[::-1, :, :3]
     assert np.array_equal(img, ref)
     assert img.mean() > 5
+
+
+def test_facade_compiles_with_textures_and_server(tmp_path):
+    """Every wrapper of the C++ facade type-checks against the C ABI."""
+    src = tmp_path / "use.cpp"
+    src.write_text("""#include "optixrender.hpp"
+int main() {
+    rt::Scene s;
+    int t = s.AddTexture(std::vector<uint8_t>(16, 255), 2, 2);
+    rt::Material m(rt::Diffuse);
+    m.texture_ids[0] = t;
+    rt::Server srv;
+    int sid = srv.AddScene(s);
+    rt_job_desc j{};
+    j.scene = sid;
+    int64_t id = srv.Submit(j);
+    rt_job_status st = srv.Wait(id, 1000.0);
+    std::vector<uint32_t> px(16);
+    srv.DownloadPixels(id, px.data());
+    srv.Release(id);
+    return int(st.state) + int(srv.Stats().jobs_done);
+}
+""")
+    inc = Path(__file__).resolve().parents[1] / "include"
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", str(inc), str(src)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
