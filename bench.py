@@ -321,6 +321,10 @@ def main():
         "instrumented_ms_per_step": counters["ms"] / args.steps,
         "rays_per_step": {"extend": counters["extend_rays"] / args.steps,
                           "shadow": counters["shadow_rays"] / args.steps},
+        "per_ray": {"extend_nodes": counters["extend_nodes"] / max(1, counters["extend_rays"]),
+                    "extend_tris": counters["extend_tris"] / max(1, counters["extend_rays"]),
+                    "shadow_nodes": (counters["nodes"] - counters["extend_nodes"]) / max(1, counters["shadow_rays"]),
+                    "shadow_tris": (counters["tris"] - counters["extend_tris"]) / max(1, counters["shadow_rays"])},
         "nan_samples": counters["nan"], "paths_ended_by_nan_throughput": counters["nan_history"],
         "launches_per_step": launches_per_step,
         "clocks": clk.summary(),

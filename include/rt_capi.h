@@ -423,12 +423,22 @@ typedef struct rt_server_options {
     int32_t background;        /* nonzero: a server thread runs the loop; zero: call rt_server_step */
     int32_t waves_in_flight;   /* waves queued ahead on the device (0 = 2) */
     int32_t policy;            /* RT_SERVE_FAIR (default), RT_SERVE_FIFO or RT_SERVE_SRPT */
+    /* Guided jobs (rt_job_desc.guided): each resident scene has one guiding
+     * network, trained on the scene's first guide_train_waves guided waves
+     * (guide_steps Adam steps after each) and then shared by every guided
+     * job on that scene. */
+    int32_t guide_train_waves; /* 0 = 32 */
+    int32_t guide_steps;       /* 0 = 4 */
+    float guide_prob;          /* probability of sampling the mixture (0 = 0.5) */
+    int32_t pad;
 } rt_server_options;
 
 /* How a wave's path slots are split among admitted jobs.  FAIR: up to 16 jobs,
  * taken round-robin, share each wave evenly (latency grows with job size).
  * FIFO: the oldest job takes all it can.  SRPT: the jobs with the fewest paths
- * left go first (shortest remaining work; lowest mean time-to-image). */
+ * left go first (shortest remaining work; lowest mean time-to-image).
+ * A wave holds either plain jobs (of any scenes) or the guided jobs of one
+ * scene; the policy also picks which of these groups the next wave serves. */
 enum { RT_SERVE_FAIR = 0, RT_SERVE_FIFO = 1, RT_SERVE_SRPT = 2 };
 
 /* One request: a resident scene, a camera and the renderer settings of one
@@ -439,7 +449,8 @@ typedef struct rt_job_desc {
     int32_t width, height, spp, max_depth, rr_depth, filter, tonemap;
     uint64_t seed;
     float exposure;
-    int32_t guided;            /* reserved for the learned proposal; 0 = plain */
+    int32_t guided;            /* nonzero: sample with the scene's guiding network (unbiased; the
+                                  image then depends on the network's training, not only on seed) */
 } rt_job_desc;
 
 enum { RT_JOB_QUEUED = 0, RT_JOB_RUNNING = 1, RT_JOB_DONE = 2, RT_JOB_FAILED = 3, RT_JOB_CANCELLED = 4 };
@@ -460,6 +471,10 @@ typedef struct rt_server_stats {
     int64_t bytes_in_use, bytes_budget;
     int32_t max_segments_in_a_wave;
     int32_t pad;
+    double busy_ms;            /* device time of the finished waves (CUDA events) */
+    double mean_wave_depth;    /* bounces launched per wave, averaged */
+    int64_t guided_waves;      /* waves of guided jobs, training waves included */
+    int64_t training_waves;    /* guided waves followed by training steps */
 } rt_server_stats;
 
 RT_API void rt_server_options_default(rt_server_options* o);

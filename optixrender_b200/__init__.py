@@ -97,7 +97,8 @@ class RenderStats(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("wave_paths", C.c_int32), ("max_jobs", C.c_int32),
                 ("max_depth", C.c_int32), ("background", C.c_int32), ("waves_in_flight", C.c_int32),
-                ("policy", C.c_int32)]
+                ("policy", C.c_int32), ("guide_train_waves", C.c_int32), ("guide_steps", C.c_int32),
+                ("guide_prob", C.c_float), ("pad", C.c_int32)]
 
 
 class JobDesc(C.Structure):
@@ -122,7 +123,8 @@ class ServerStats(C.Structure):
     _fields_ = [("jobs_submitted", C.c_int64), ("jobs_done", C.c_int64), ("jobs_queued", C.c_int64),
                 ("jobs_running", C.c_int64), ("waves", C.c_int64), ("paths", C.c_int64),
                 ("bytes_in_use", C.c_int64), ("bytes_budget", C.c_int64), ("max_segments_in_a_wave", C.c_int32),
-                ("pad", C.c_int32)]
+                ("pad", C.c_int32), ("busy_ms", C.c_double), ("mean_wave_depth", C.c_double),
+                ("guided_waves", C.c_int64), ("training_waves", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
@@ -569,11 +571,12 @@ def server_options(**kw):
 
 
 def job(scene, cam, width, height, spp, max_depth=25, rr_depth=0, filter=FILTER_GAUSSIAN, tonemap=TONEMAP_REINHARD,
-        seed=1, exposure=1.0):
-    """One render request: the settings of a Renderer::Render() on a resident scene (PCG32 streams)."""
+        seed=1, exposure=1.0, guided=0):
+    """One render request: the settings of a Renderer::Render() on a resident scene (PCG32 streams);
+    `guided` samples with the scene's guiding network."""
     return JobDesc(scene=int(scene), camera=cam, width=int(width), height=int(height), spp=int(spp),
                    max_depth=int(max_depth), rr_depth=int(rr_depth), filter=int(filter), tonemap=int(tonemap),
-                   seed=int(seed), exposure=float(exposure), guided=0)
+                   seed=int(seed), exposure=float(exposure), guided=int(guided))
 
 
 class Server:

@@ -25,6 +25,9 @@
 namespace rtd {
 
 constexpr int kBlock = 128;
+static_assert(kBlock == kTravBlock, "the traversal stack is laid out for this block size");
+// 8 resident blocks per SM (64 registers) beat 6 (80 registers) by 11%.
+constexpr int kTravMinBlocks = 8;
 constexpr int kStaleTextured = 1 << 30;  // stale.w flag: the slot's mat_tex holds the last hit's material
 
 
@@ -150,7 +153,7 @@ struct ExtendSrc {
 };
 
 template <bool Stats>
-__global__ void __launch_bounds__(kBlock, 8) k_extend(Ctx c) {
+__global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_extend(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     const int cur = c.bounce & 1, nxt = cur ^ 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -621,7 +624,7 @@ struct ShadowSrc {
 };
 
 template <bool Stats>
-__global__ void __launch_bounds__(kBlock, 8) k_shadow(Ctx c) {
+__global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_shadow(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     if (blockIdx.x == 0 && threadIdx.x < kShadeBuckets) ctl->bucket[threadIdx.x] = 0;  // for the next extend
     const int total = ctl->shadow_count;

@@ -11,9 +11,21 @@
 // whose paths have all been issued gets its finalize kernel and an event; the
 // host marks it done when the event completes.
 //
+// Nothing on the job path synchronises the device: a job's buffers are one
+// stream-ordered allocation from the server's memory pool (freed the same
+// way, so a release never waits for waves in flight), its descriptor is
+// copied from pinned staging memory, and downloads use their own stream.
+//
 // Paths draw PCG32 streams keyed by (job seed, path index) and each pixel's
-// samples are summed in sample order, so a job's image does not depend on
-// which jobs share its waves.
+// samples are summed in sample order, so a plain job's image does not depend
+// on which jobs share its waves.
+//
+// Guided jobs: every resident scene owns one guiding network.  A wave holds
+// either plain jobs of any scenes or the guided jobs of one scene (the
+// network a wave samples is fixed while it runs, so the estimate stays
+// unbiased); the scene's first guide_train_waves guided waves record training
+// samples and are followed by guide_steps Adam steps, and every later guided
+// job on the scene samples the trained network without training again.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +39,7 @@
 #include <thread>
 #include <vector>
 
+#include "rt_guide_host.h"
 #include "rt_internal.h"
 
 using namespace rtd;
@@ -48,12 +61,26 @@ struct Job {
     int slot = -1;
     int64_t npix = 0, total = 0, issued = 0;
     int64_t bytes = 0;
-    DevBuf acc_color, acc_albedo, acc_normal, lcg, color, albedo, normal, rgba8;
+    // one pool allocation: acc_color, acc_albedo, acc_normal, color, albedo,
+    // normal (float4 per pixel), then lcg and rgba8 (4 bytes per pixel)
+    char* mem = nullptr;
     cudaEvent_t done_ev = nullptr;
+    float4* f4(int k) const { return reinterpret_cast<float4*>(mem) + size_t(k) * size_t(npix); }
+    uint32_t* u32(int k) const { return reinterpret_cast<uint32_t*>(mem + size_t(npix) * 96) + size_t(k) * size_t(npix); }
     bool finalize_issued = false;
 };
 
 int64_t job_bytes(int64_t npix) { return npix * (6 * 16 + 2 * 4); }
+
+constexpr int kGuideBatch = 1 << 18;  // training samples per Adam step
+
+// The guiding network of one resident scene.
+struct SceneGuide {
+    rt_guide* net = nullptr;
+    float3 lo{}, inv{};  // position normalisation: scene bounds with a 1% margin
+    int64_t train_waves = 0;
+    uint32_t seed = 1;
+};
 
 }  // namespace
 
@@ -61,8 +88,12 @@ struct rt_server {
     rt_server_options opt{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t dl_stream = nullptr;  // downloads of finished images
+    cudaMemPool_t pool = nullptr;      // job buffers, stream-ordered on `stream`
+    JobDesc* host_jobs = nullptr;      // pinned staging of the job table
     std::chrono::steady_clock::time_point t0;
     std::vector<std::unique_ptr<DeviceScene>> scenes;
+    std::vector<SceneGuide> guides;  // one per scene; networks created at the first guided wave
     int64_t scene_bytes = 0;
     std::map<int64_t, std::unique_ptr<Job>> jobs;
     std::deque<int64_t> queued;
@@ -75,16 +106,23 @@ struct rt_server {
     DevBuf job_table, ring, wave_index, ctl;
     DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, sorted;
     DevBuf mat_tex;  // per-slot textured materials, once a scene with textures is resident
+    // guiding: per-slot mixtures, training records and samples, one batch
+    DevBuf g_mix, g_rec, g_buf, g_count, g_wsum, g_bpos, g_bdir, g_bw;
+    int64_t guide_bytes = 0;
     int capacity = 0;
     int ring_size = 0;
     int ring_pos = 0;
     WaveParams* host_ring = nullptr;   // pinned
-    std::vector<cudaEvent_t> ring_ev;
-    std::map<int, cudaGraphExec_t> graphs;  // by bounce count
+    std::vector<cudaEvent_t> ring_ev;     // end of the wave in each ring slot
+    std::vector<cudaEvent_t> ring_start;  // its start, for the device-busy time
+    std::vector<char> ring_timed;         // slot holds a wave not yet added to busy_ms
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // by (bounce count, guided scene + 1 or 0)
     rth::LaunchShape shape{};
     // stats
-    int64_t waves = 0, paths = 0, done = 0, submitted = 0;
+    int64_t waves = 0, paths = 0, done = 0, submitted = 0, depth_sum = 0, guided_waves = 0, training_waves = 0;
+    size_t pool_rr = 0;  // rotation over job groups (plain, guided per scene) of the fair policy
     int max_segments = 0;
+    double busy_ms = 0.0;
     // background thread
     std::mutex mu;
     std::condition_variable cv;
@@ -102,7 +140,16 @@ namespace {
 rt_status setup(rt_server* s) {
     SV_CUDA(cudaGetDevice(&s->device), "rt_server_create");
     SV_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "rt_server_create");
+    SV_CUDA(cudaStreamCreateWithFlags(&s->dl_stream, cudaStreamNonBlocking), "rt_server_create");
+    cudaMemPoolProps pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = s->device;
+    SV_CUDA(cudaMemPoolCreate(&s->pool, &pp), "create job memory pool");
     const int n = s->opt.max_jobs;
+    SV_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s->host_jobs), size_t(n) * sizeof(JobDesc)),
+            "allocate pinned job table");
     SV_CUDA(s->job_table.alloc(size_t(n) * sizeof(JobDesc)), "allocate job table");
     SV_CUDA(cudaMemset(s->job_table.ptr, 0, size_t(n) * sizeof(JobDesc)), "clear job table");
     s->ring_size = std::max(2, s->opt.waves_in_flight + 1);
@@ -114,9 +161,12 @@ rt_status setup(rt_server* s) {
     SV_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s->host_ring), size_t(s->ring_size) * sizeof(WaveParams)),
             "allocate pinned wave ring");
     for (int i = 0; i < s->ring_size; i++) {
-        cudaEvent_t e;
-        SV_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
+        cudaEvent_t e, b;
+        SV_CUDA(cudaEventCreate(&e), "create event");
+        SV_CUDA(cudaEventCreate(&b), "create event");
         s->ring_ev.push_back(e);
+        s->ring_start.push_back(b);
+        s->ring_timed.push_back(0);
     }
     const size_t cap = size_t(s->opt.wave_paths);
     DevBuf* f4s[] = {&s->ray_o, &s->ray_d, &s->hit, &s->thr, &s->rad, &s->nee0, &s->nee1, &s->stale, &s->aov_a};
@@ -136,10 +186,40 @@ rt_status setup(rt_server* s) {
         SV_CUDA(cudaMemGetInfo(&fr, &tot), "query device memory");
         s->opt.hbm_budget_bytes = int64_t(double(fr) * 0.8);
     }
+    // freed job memory stays in the pool, up to the budget, for the next admissions
+    uint64_t keep = uint64_t(s->opt.hbm_budget_bytes);
+    SV_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep), "configure job memory pool");
     return RT_OK;
 }
 
-Ctx make_ctx(rt_server* s) {
+// Per-slot guiding buffers, allocated with the first guided job.
+rt_status ensure_guide_buffers(rt_server* s) {
+    if (s->g_mix.ptr) return RT_OK;
+    const size_t cap = size_t(s->capacity);
+    SV_CUDA(s->g_mix.alloc(cap * sizeof(rtg::Mixture)), "allocate guide mixtures");
+    SV_CUDA(s->g_rec.alloc(size_t(rtg::kGuideRec) * 4 * cap * sizeof(float4)), "allocate guide records");
+    SV_CUDA(s->g_buf.alloc(size_t(rtg::kGuideRec) * cap * 32), "allocate guide samples");
+    SV_CUDA(s->g_count.alloc(sizeof(int)), "allocate guide samples");
+    SV_CUDA(s->g_wsum.alloc(sizeof(float)), "allocate guide batch");
+    SV_CUDA(s->g_bpos.alloc(size_t(kGuideBatch) * 12), "allocate guide batch");
+    SV_CUDA(s->g_bdir.alloc(size_t(kGuideBatch) * 12), "allocate guide batch");
+    SV_CUDA(s->g_bw.alloc(size_t(kGuideBatch) * 4), "allocate guide batch");
+    s->guide_bytes = int64_t(s->g_mix.bytes + s->g_rec.bytes + s->g_buf.bytes + 3 * size_t(kGuideBatch) * 12);
+    return RT_OK;
+}
+
+// The network of scene `k`, created at its first guided wave.
+rt_status ensure_scene_guide(rt_server* s, int k) {
+    SceneGuide& g = s->guides[size_t(k)];
+    if (g.net) return RT_OK;
+    rt_guide_options go;
+    rt_guide_options_default(&go);
+    go.seed = uint64_t(k) + 1;
+    return guide_create(&go, &g.net);
+}
+
+// `gscene` >= 0: the wave samples the guiding network of that scene.
+Ctx make_ctx(rt_server* s, int gscene = -1) {
     Ctx c;
     std::memset(&c, 0, sizeof(c));
     c.jobs = s->job_table.as<JobDesc>();
@@ -167,38 +247,65 @@ Ctx make_ctx(rt_server* s) {
     c.wave_index = s->wave_index.as<int>();
     c.wave_ring = s->ring_size;
     c.max_depth = s->opt.max_depth;
+    if (gscene >= 0) {
+        const SceneGuide& g = s->guides[size_t(gscene)];
+        c.G.mix = s->g_mix.as<rtg::Mixture>();
+        c.G.prob = s->opt.guide_prob;
+        c.G.min_rough = 0.3f;
+        c.G.lo = g.lo;
+        c.G.inv_ext = g.inv;
+    }
     return c;
 }
 
-// One captured wave per bounce count: raygen, (extend, shade, shadow) x depth,
-// resolve, advance of the wave ring.  A wave uses the graph of the deepest
-// job in it; each path still stops at its own job's max_depth.
-rt_status wave_graph(rt_server* s, int depth, cudaGraphExec_t* out) {
-    auto it = s->graphs.find(depth);
-    if (it != s->graphs.end()) {
-        *out = it->second;
-        return RT_OK;
-    }
-    Ctx c = make_ctx(s);
+// One wave's launches: raygen, (extend, [guide inference,] shade, shadow) x
+// depth, resolve, [training samples,] advance of the wave ring.
+void issue_wave(rt_server* s, const Ctx& c0, int depth, int gscene, bool training) {
+    Ctx c = c0;
     c.max_depth = depth;
-    cudaGraph_t g = nullptr;
-    SV_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+    c.G.rec = training ? s->g_rec.as<float4>() : nullptr;
+    rtg::NetView net{};
+    int gsms = 0;
+    if (gscene >= 0) {
+        const SceneGuide& g = s->guides[size_t(gscene)];
+        net = guide_view(g.net, g.lo, g.inv);
+        gsms = guide_sms(g.net);
+    }
+    if (training) cudaMemsetAsync(s->g_count.ptr, 0, sizeof(int), s->stream);
     c.bounce = 0;
     rth::launch_raygen(c, s->stream);
     for (int b = 0; b < depth; b++) {
         c.bounce = b;
         rth::launch_extend(c, s->shape, false, s->stream);
+        if (gscene >= 0) rtgh::launch_infer(c, net, gsms, s->stream);
         rth::launch_shade(c, s->shape, false, s->stream);
         rth::launch_shadow(c, s->shape, false, s->stream);
     }
     rth::launch_resolve(c, s->stream);
+    if (training)
+        rtgh::launch_collect(c, s->g_buf.as<float4>(), s->g_count.as<int>(), int(s->g_buf.bytes / 32), s->stream);
     rth::launch_next_wave(c, s->stream);
+}
+
+// One captured wave per bounce count: raygen, (extend, shade, shadow) x depth,
+// resolve, advance of the wave ring.  A wave uses the graph of the deepest
+// job in it; each path still stops at its own job's max_depth.
+rt_status wave_graph(rt_server* s, int depth, int gscene, cudaGraphExec_t* out) {
+    const std::pair<int, int> key(depth, gscene + 1);
+    auto it = s->graphs.find(key);
+    if (it != s->graphs.end()) {
+        *out = it->second;
+        return RT_OK;
+    }
+    cudaGraph_t g = nullptr;
+    SV_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+    issue_wave(s, make_ctx(s, gscene), depth, gscene, false);
     SV_CUDA(cudaStreamEndCapture(s->stream, &g), "end graph capture");
     cudaGraphExec_t ge = nullptr;
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "instantiate wave graph");
-    s->graphs[depth] = ge;
+    s->graphs[key] = ge;
     *out = ge;
     return RT_OK;
 }
@@ -208,14 +315,14 @@ rt_status admit(rt_server* s, Job& j) {
     j.npix = int64_t(d.width) * d.height;
     j.total = j.npix * d.spp;
     j.bytes = job_bytes(j.npix);
-    DevBuf* f4s[] = {&j.acc_color, &j.acc_albedo, &j.acc_normal, &j.color, &j.albedo, &j.normal};
-    for (DevBuf* b : f4s) SV_CUDA(b->alloc(size_t(j.npix) * sizeof(float4)), "allocate job buffers");
-    SV_CUDA(j.lcg.alloc(size_t(j.npix) * 4), "allocate job buffers");
-    SV_CUDA(j.rgba8.alloc(size_t(j.npix) * 4), "allocate job buffers");
+    SV_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&j.mem), size_t(j.bytes), s->pool, s->stream),
+            "allocate job buffers");
     SV_CUDA(cudaEventCreateWithFlags(&j.done_ev, cudaEventDisableTiming), "create event");
     j.slot = s->free_slots.back();
     s->free_slots.pop_back();
-    JobDesc hj;
+    // A slot's staging entry is rewritten only after its previous job was
+    // released, i.e. after that job's upload and waves completed.
+    JobDesc& hj = s->host_jobs[j.slot];
     std::memset(&hj, 0, sizeof(hj));
     hj.sc = s->scenes[size_t(d.scene)]->view;
     hj.cam = camera_view(d.camera, d.width, d.height);
@@ -232,17 +339,16 @@ rt_status admit(rt_server* s, Job& j) {
     p.npix = j.npix;
     p.tonemap = d.tonemap;
     p.exposure = d.exposure;
-    p.acc_color = j.acc_color.as<float4>();
-    p.acc_albedo = j.acc_albedo.as<float4>();
-    p.acc_normal = j.acc_normal.as<float4>();
-    p.lcg_state = j.lcg.as<uint32_t>();
-    p.color = j.color.as<float4>();
-    p.albedo = j.albedo.as<float4>();
-    p.normal = j.normal.as<float4>();
-    p.rgba8 = j.rgba8.as<uint32_t>();
+    p.acc_color = j.f4(0);
+    p.acc_albedo = j.f4(1);
+    p.acc_normal = j.f4(2);
+    p.color = j.f4(3);
+    p.albedo = j.f4(4);
+    p.normal = j.f4(5);
+    p.lcg_state = j.u32(0);
+    p.rgba8 = j.u32(1);
     JobDesc* dj = s->job_table.as<JobDesc>() + j.slot;
     SV_CUDA(cudaMemcpyAsync(dj, &hj, sizeof(hj), cudaMemcpyHostToDevice, s->stream), "upload job");
-    SV_CUDA(cudaStreamSynchronize(s->stream), "upload job");  // hj is a stack object
     rth::launch_begin_n(dj, j.npix, s->stream);
     j.state = RT_JOB_RUNNING;
     j.admit_ms = s->now_ms();
@@ -250,9 +356,19 @@ rt_status admit(rt_server* s, Job& j) {
     return RT_OK;
 }
 
+// Adds the device time of every finished wave not yet counted.
+void account_busy(rt_server* s) {
+    for (size_t i = 0; i < s->ring_ev.size(); i++) {
+        if (!s->ring_timed[i] || cudaEventQuery(s->ring_ev[i]) != cudaSuccess) continue;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, s->ring_start[i], s->ring_ev[i]) == cudaSuccess) s->busy_ms += double(ms);
+        s->ring_timed[i] = 0;
+    }
+}
+
 void free_job(rt_server* s, Job& j) {
-    DevBuf* all[] = {&j.acc_color, &j.acc_albedo, &j.acc_normal, &j.lcg, &j.color, &j.albedo, &j.normal, &j.rgba8};
-    for (DevBuf* b : all) b->release();
+    if (j.mem) cudaFreeAsync(j.mem, s->stream);  // after every wave issued so far
+    j.mem = nullptr;
     if (j.done_ev) cudaEventDestroy(j.done_ev);
     j.done_ev = nullptr;
     if (j.slot >= 0) s->free_slots.push_back(j.slot);
@@ -285,7 +401,7 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
     while (!s->queued.empty() && !s->free_slots.empty()) {
         Job& j = *s->jobs[s->queued.front()];
         int64_t need = job_bytes(int64_t(j.desc.width) * j.desc.height);
-        if (s->bytes_in_use + s->scene_bytes + need > s->opt.hbm_budget_bytes) break;
+        if (s->bytes_in_use + s->scene_bytes + s->guide_bytes + need > s->opt.hbm_budget_bytes) break;
         s->queued.pop_front();
         rt_status st = admit(s, j);
         if (st) {
@@ -302,11 +418,36 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
         if (did_work) *did_work = 1;
         return RT_OK;
     }
-    // Paths each job gets in this wave.
+    account_busy(s);
+    // The group this wave serves: plain jobs (0) or the guided jobs of scene
+    // k (k + 1), chosen by the policy; then the paths each of its jobs gets.
     std::vector<Job*> active;
     for (int64_t id : s->running) {
         Job& j = *s->jobs[id];
         if (j.issued < j.total) active.push_back(&j);
+    }
+    auto group = [](const Job* j) { return j->desc.guided ? j->desc.scene + 1 : 0; };
+    if (!active.empty()) {
+        int chosen = group(active.front());  // FIFO: the oldest job's group
+        if (s->opt.policy == RT_SERVE_SRPT) {
+            const Job* best = active.front();
+            for (const Job* j : active)
+                if (j->total - j->issued < best->total - best->issued) best = j;
+            chosen = group(best);
+        } else if (s->opt.policy == RT_SERVE_FAIR) {
+            // the first group at or after the rotation point that has work
+            int best = -1, first = -1;
+            for (const Job* j : active) {
+                const int gid = group(j);
+                if (first < 0 || gid < first) first = gid;
+                if (gid >= int(s->pool_rr) && (best < 0 || gid < best)) best = gid;
+            }
+            chosen = best >= 0 ? best : first;
+            s->pool_rr = size_t(chosen) + 1;
+        }
+        active.erase(std::remove_if(active.begin(), active.end(),
+                                    [&](const Job* j) { return group(j) != chosen; }),
+                     active.end());
     }
     std::vector<std::pair<Job*, int64_t>> plan;
     if (!active.empty()) {
@@ -355,6 +496,7 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
     WaveParams wp;
     std::memset(&wp, 0, sizeof(wp));
     int filled = 0, depth = 1;
+    const int gscene = plan.empty() || !plan.front().first->desc.guided ? -1 : plan.front().first->desc.scene;
     std::vector<Job*> completing;
     for (auto& pj : plan) {
         Job& j = *pj.first;
@@ -370,18 +512,51 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
     }
     if (filled > 0) {
         wp.wave_count = filled;
+        bool training = false;
+        if (gscene >= 0) {
+            rt_status gs = ensure_guide_buffers(s);
+            if (!gs) gs = ensure_scene_guide(s, gscene);
+            if (gs) return gs;
+            training = s->guides[size_t(gscene)].train_waves < s->opt.guide_train_waves;
+        }
         cudaGraphExec_t graph = nullptr;
-        rt_status gs = wave_graph(s, depth, &graph);
-        if (gs) return gs;
+        if (!training) {
+            rt_status gs = wave_graph(s, depth, gscene, &graph);
+            if (gs) return gs;
+        }
         int pos = s->ring_pos;
+        SV_CUDA(cudaEventRecord(s->ring_start[size_t(pos)], s->stream), "record event");
         s->host_ring[pos] = wp;
         SV_CUDA(cudaMemcpyAsync(s->ring.as<WaveParams>() + pos, &s->host_ring[pos], sizeof(WaveParams),
                                 cudaMemcpyHostToDevice, s->stream),
                 "upload wave");
-        SV_CUDA(cudaGraphLaunch(graph, s->stream), "launch wave");
+        if (training) {
+            // launched directly: the wave records training samples, then the
+            // scene's network takes guide_steps Adam steps on batches of them
+            SceneGuide& g = s->guides[size_t(gscene)];
+            issue_wave(s, make_ctx(s, gscene), depth, gscene, true);
+            for (int k = 0; k < s->opt.guide_steps; k++) {
+                SV_CUDA(cudaMemsetAsync(s->g_wsum.ptr, 0, sizeof(float), s->stream), "guide batch");
+                rtgh::launch_batch(s->g_buf.as<float4>(), s->g_count.as<int>(), int(s->g_buf.bytes / 32),
+                                   kGuideBatch, g.seed++ * 0x9E3779B9u, s->g_bpos.as<float>(), s->g_bdir.as<float>(),
+                                   s->g_bw.as<float>(), s->g_wsum.as<float>(), s->stream);
+                rt_status ts = guide_train_device(g.net, s->g_bpos.as<float>(), s->g_bdir.as<float>(),
+                                                  s->g_bw.as<float>(), kGuideBatch, 1.0f, s->g_wsum.as<float>(),
+                                                  s->stream);
+                if (ts) return ts;
+            }
+            g.train_waves++;
+            s->training_waves++;
+            SV_CUDA(cudaGetLastError(), "launch training wave");
+        } else {
+            SV_CUDA(cudaGraphLaunch(graph, s->stream), "launch wave");
+        }
+        if (gscene >= 0) s->guided_waves++;
         SV_CUDA(cudaEventRecord(s->ring_ev[size_t(pos)], s->stream), "record event");
+        s->ring_timed[size_t(pos)] = 1;
         s->ring_pos = (pos + 1) % s->ring_size;
         s->waves++;
+        s->depth_sum += depth;
         s->paths += filled;
         s->max_segments = std::max(s->max_segments, wp.num_seg);
         for (Job* j : completing) {
@@ -454,6 +629,9 @@ void rt_server_options_default(rt_server_options* o) {
     o->max_depth = 32;
     o->background = 1;
     o->waves_in_flight = 2;
+    o->guide_train_waves = 32;
+    o->guide_steps = 4;
+    o->guide_prob = 0.5f;
 }
 
 rt_status rt_server_create(const rt_server_options* o, rt_server** out) {
@@ -467,6 +645,13 @@ rt_status rt_server_create(const rt_server_options* o, rt_server** out) {
         if (s->opt.max_jobs <= 0) s->opt.max_jobs = 256;
         if (s->opt.max_depth <= 0) s->opt.max_depth = 32;
         if (s->opt.waves_in_flight <= 0) s->opt.waves_in_flight = 2;
+        if (s->opt.guide_train_waves <= 0) s->opt.guide_train_waves = 32;
+        if (s->opt.guide_steps <= 0) s->opt.guide_steps = 4;
+        if (s->opt.guide_prob == 0.0f) s->opt.guide_prob = 0.5f;
+    }
+    if (!(s->opt.guide_prob > 0.0f && s->opt.guide_prob <= 1.0f)) {
+        delete s;
+        return fail(RT_ERR_INVALID_ARG, "rt_server_create: guide_prob must be in (0, 1]");
     }
     if (s->opt.policy != RT_SERVE_FAIR && s->opt.policy != RT_SERVE_FIFO && s->opt.policy != RT_SERVE_SRPT) {
         delete s;
@@ -497,9 +682,16 @@ rt_status rt_server_destroy(rt_server* s) {
     if (s->worker.joinable()) s->worker.join();
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& kv : s->jobs) free_job(s, *kv.second);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    for (SceneGuide& g : s->guides)
+        if (g.net) rt_guide_destroy(g.net);
     for (cudaEvent_t e : s->ring_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : s->ring_start) cudaEventDestroy(e);
     if (s->host_ring) cudaFreeHost(s->host_ring);
+    if (s->host_jobs) cudaFreeHost(s->host_jobs);
+    if (s->dl_stream) cudaStreamDestroy(s->dl_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return RT_OK;
@@ -519,6 +711,13 @@ rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* id) 
     }
     s->scene_bytes += int64_t(ds->bytes);
     s->scenes.push_back(std::move(ds));
+    SceneGuide g;
+    for (int a = 0; a < 3; a++) {  // 1% margin around the scene bounds
+        const float ext = std::max(scene->hi[a] - scene->lo[a], 1e-6f);
+        (&g.lo.x)[a] = scene->lo[a] - 0.01f * ext;
+        (&g.inv.x)[a] = 1.0f / (1.02f * ext);
+    }
+    s->guides.push_back(g);
     if (id) *id = int32_t(s->scenes.size()) - 1;
     return RT_OK;
 }
@@ -529,7 +728,11 @@ rt_status rt_server_submit(rt_server* s, const rt_job_desc* d, int64_t* id) {
     if (d->scene < 0 || d->scene >= int(s->scenes.size())) return fail(RT_ERR_INVALID_ARG, "rt_server_submit: unknown scene");
     if (d->width <= 0 || d->height <= 0 || d->spp <= 0 || d->max_depth <= 0 || d->max_depth > s->opt.max_depth)
         return fail(RT_ERR_INVALID_ARG, "rt_server_submit: bad size, spp or max_depth (<= the server's max_depth)");
-    if (job_bytes(int64_t(d->width) * d->height) + s->scene_bytes > s->opt.hbm_budget_bytes)
+    if (d->guided) {  // the per-slot guiding buffers count against the budget from the first guided job on
+        rt_status gs = ensure_guide_buffers(s);
+        if (gs) return gs;
+    }
+    if (job_bytes(int64_t(d->width) * d->height) + s->scene_bytes + s->guide_bytes > s->opt.hbm_budget_bytes)
         return fail(RT_ERR_OUT_OF_MEMORY, "rt_server_submit: the job alone exceeds the memory budget");
     std::unique_ptr<Job> j(new Job());
     j->id = s->next_id++;
@@ -604,11 +807,13 @@ static rt_status download_job(rt_server* s, int64_t id, void* dst, bool rgba8) {
     if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_download: unknown job");
     Job& j = *it->second;
     if (j.state != RT_JOB_DONE) return fail(RT_ERR_STATE, "rt_server_download: job not done");
-    const DevBuf& b = rgba8 ? j.rgba8 : j.color;
-    if (!b.ptr) return fail(RT_ERR_STATE, "rt_server_download: job released");
-    SV_CUDA(cudaMemcpyAsync(dst, b.ptr, size_t(j.npix) * (rgba8 ? 4 : 16), cudaMemcpyDeviceToHost, s->stream),
+    if (!j.mem) return fail(RT_ERR_STATE, "rt_server_download: job released");
+    // the job's finalize has completed (its event did), so the copy need not
+    // wait behind the waves queued on the server stream
+    const void* src = rgba8 ? static_cast<const void*>(j.u32(1)) : static_cast<const void*>(j.f4(3));
+    SV_CUDA(cudaMemcpyAsync(dst, src, size_t(j.npix) * (rgba8 ? 4 : 16), cudaMemcpyDeviceToHost, s->dl_stream),
             "rt_server_download");
-    SV_CUDA(cudaStreamSynchronize(s->stream), "rt_server_download");
+    SV_CUDA(cudaStreamSynchronize(s->dl_stream), "rt_server_download");
     return RT_OK;
 }
 
@@ -653,9 +858,14 @@ rt_status rt_server_get_stats(rt_server* s, rt_server_stats* st) {
     st->jobs_running = int64_t(s->running.size());
     st->waves = s->waves;
     st->paths = s->paths;
-    st->bytes_in_use = s->bytes_in_use + s->scene_bytes;
+    st->bytes_in_use = s->bytes_in_use + s->scene_bytes + s->guide_bytes;
     st->bytes_budget = s->opt.hbm_budget_bytes;
     st->max_segments_in_a_wave = s->max_segments;
+    account_busy(s);
+    st->busy_ms = s->busy_ms;
+    st->mean_wave_depth = s->waves ? double(s->depth_sum) / double(s->waves) : 0.0;
+    st->guided_waves = s->guided_waves;
+    st->training_waves = s->training_waves;
     return RT_OK;
 }
 

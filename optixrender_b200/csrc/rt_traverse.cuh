@@ -87,6 +87,18 @@ RT_D float u8f(uint32_t w, int byte) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, sel)) - 8388608.0f;
 }
 
+// Three-input minimum / maximum (PTX ISA 8.8, sm_100).
+RT_D float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+RT_D float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // Tests the eight children of `node`; returns the hit mask of internal
 // children (bits 24..31, near-to-far) with the node's imask in bits 0..7,
 // and the triangle hit mask (bits 0..23) in `tri_bits`.
@@ -125,9 +137,11 @@ RT_D uint32_t intersect_children(const CwNode* nodes, uint32_t idx, const TravRa
             float tx0 = fmaf(u8f(xn, b), sx, ox), tx1 = fmaf(u8f(xf, b), sx, ox);
             float ty0 = fmaf(u8f(yn, b), sy, oy), ty1 = fmaf(u8f(yf, b), sy, oy);
             float tz0 = fmaf(u8f(zn, b), sz, oz), tz1 = fmaf(u8f(zf, b), sz, oz);
-            float tn = fmaxf(fmaxf(tx0, ty0), fmaxf(tz0, r.tmin));
-            float tf = fminf(fminf(tx1, ty1), fminf(tz1, tmax));
-            bool hit = meta != 0u && tn * 0.9999992f <= tf * 1.0000008f;
+            float tn = max3f(tx0, ty0, fmaxf(tz0, r.tmin));
+            float tf = min3f(tx1, ty1, fminf(tz1, tmax));
+            // conservative: the far distance is widened by 1.6e-6 relative
+            // (tn >= tmin >= 0), covering the rounding of the slab distances
+            bool hit = meta != 0u && tn <= tf * 1.0000016f;
             if (hit) {
                 const int slot = half * 4 + b;
                 if ((imask >> slot) & 1u) {
@@ -198,7 +212,24 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
 // work remains.  `src.load(i, ray, scene)` fetches queue entry i;
 // `src.finish(fin, i, tri, t, b1, b2, tri_v)` is called by the whole warp after
 // every step and stores the result of the lanes whose `fin` is set.
+// Measured on the 2.59M-triangle scene: refilling at 12 idle lanes beat 4, 8
+// and 16; postponing triangles below 20% of the lanes beat 10, 15, 30 and 40.
 constexpr int kRefillLanes = 12;
+constexpr int kPostponePercent = 20;
+// Threads per block of the persistent traversal kernels.
+constexpr int kTravBlock = 128;
+// Stack entries with this bit in x are postponed triangle groups
+// (x = first triangle, y = triangle hit bits), not node groups.
+constexpr uint32_t kTriGroup = 0x80000000u;
+
+// The per-thread traversal stack (local memory; a shared-memory stack
+// measured no faster).
+struct TravStack {
+    uint2 e[kStackSize];
+    int sp;
+    RT_D void push(uint2 v) { e[sp++] = v; }
+    RT_D uint2 pop() { return e[--sp]; }
+};
 
 struct TravState {
     TravRay r;
@@ -208,22 +239,38 @@ struct TravState {
     float tmax;
     float t, b1, b2;
     int hit;
-    int sp;
 };
 
-// One wide node and its triangles; returns true when the ray is finished.
+// One wide node (or one postponed triangle group) and its triangles; returns
+// true when the ray is finished.
 template <bool AnyHit, bool Stats>
-RT_D bool trav_step(TravState& s, uint2* stack, uint32_t& nodes_visited, uint32_t& tris_tested) {
-    uint32_t bit = __ffs(s.g.y >> 24) - 1u;
-    s.g.y &= ~(1u << (24 + bit));
-    uint32_t slot = bit ^ s.r.oct;
-    uint32_t idx = s.g.x + __popc((s.g.y & 0xFFu) & ((1u << slot) - 1u));
-    if ((s.g.y & 0xFF000000u) && s.sp < kStackSize) stack[s.sp++] = s.g;
-    uint32_t cb, tb, tbits;
-    uint32_t nb = intersect_children(s.nodes, idx, s.r, s.tmax, cb, tb, tbits);
-    if (Stats) nodes_visited++;
-    s.g = make_uint2(cb, nb);
+RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32_t& tris_tested) {
+    uint32_t tb, tbits;
+    if (s.g.x & kTriGroup) {
+        tb = s.g.x & ~kTriGroup;
+        tbits = s.g.y;
+        s.g = make_uint2(0u, 0u);
+    } else {
+        uint32_t bit = __ffs(s.g.y >> 24) - 1u;
+        s.g.y &= ~(1u << (24 + bit));
+        uint32_t slot = bit ^ s.r.oct;
+        uint32_t idx = s.g.x + __popc((s.g.y & 0xFFu) & ((1u << slot) - 1u));
+        if ((s.g.y & 0xFF000000u) && st.sp < kStackSize) st.push(s.g);
+        uint32_t cb;
+        uint32_t nb = intersect_children(s.nodes, idx, s.r, s.tmax, cb, tb, tbits);
+        if (Stats) nodes_visited++;
+        s.g = make_uint2(cb, nb);
+    }
+    // Triangle postponing (Ylitie et al. 2017): when fewer than
+    // kPostponePercent of the lanes in this step still test triangles, the
+    // rest of the group goes on the stack and the lane returns to node
+    // traversal with the others (+7% paths/s on the 2.59M-triangle scene).
+    const int n_step = __popc(__activemask());
     while (tbits) {
+        if (__popc(__activemask()) * 100 < kPostponePercent * n_step && st.sp < kStackSize) {
+            st.push(make_uint2(tb | kTriGroup, tbits));
+            break;
+        }
         uint32_t b = __ffs(tbits) - 1u;
         tbits &= ~(1u << b);
         uint32_t ti = tb + b;
@@ -240,9 +287,9 @@ RT_D bool trav_step(TravState& s, uint2* stack, uint32_t& nodes_visited, uint32_
             if (AnyHit) return true;
         }
     }
-    while (!(s.g.y & 0xFF000000u)) {
-        if (s.sp == 0) return true;
-        s.g = stack[--s.sp];
+    while (!(s.g.x & kTriGroup) && !(s.g.y & 0xFF000000u)) {
+        if (st.sp == 0) return true;
+        s.g = st.pop();
     }
     return false;
 }
@@ -251,7 +298,8 @@ template <bool AnyHit, bool Stats, class Src>
 RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& nodes_visited, uint32_t& tris_tested,
                          uint32_t& rays) {
     const int lane = threadIdx.x & 31;
-    uint2 stack[kStackSize];
+    TravStack st;
+    st.sp = 0;
     TravState s;
     int item = -1;
     bool active = false, exhausted = false;
@@ -275,7 +323,7 @@ RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& node
                     s.tri_v = sc->tri_v;
                     s.tmax = s.r.tmax;
                     s.hit = -1;
-                    s.sp = 0;
+                    st.sp = 0;
                     s.g = make_uint2(0u, 1u << (24 + s.r.oct));
                     rays++;
                     if (sc->num_nodes > 0)
@@ -285,7 +333,7 @@ RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& node
                 }
             }
         }
-        if (active && trav_step<AnyHit, Stats>(s, stack, nodes_visited, tris_tested)) {
+        if (active && trav_step<AnyHit, Stats>(s, st, nodes_visited, tris_tested)) {
             fin = true;
             active = false;
         }

@@ -6,7 +6,8 @@ Requests: resolution uniform from {256^2, 512^2, 1024^2, 1920x1080}, spp
 uniform from {4, 16, 64, 256}, scene uniform from the Cornell box (34
 triangles), the displaced icosphere with 64 spheres (2,590,720 triangles) and
 the media scene (128^3 grid), a random camera orbiting the scene's own, guided
-or plain drawn 50/50 (recorded; every job renders with the plain method).
+or plain drawn 50/50 (guided jobs sample their scene's guiding network, trained
+on the scene's first guided waves).
 
 First every request is submitted at once (saturation): aggregate Mpaths/s and
 the saturation job rate.  Then the same requests arrive as a Poisson stream at
@@ -72,7 +73,7 @@ def make_requests(n, specs, seed=1, resolutions=RESOLUTIONS, spps=SPPS):
 def _desc(req, scene_ids):
     return rt.job(scene_ids[req["scene"]], rt.camera(**req["camera"]), req["width"], req["height"], req["spp"],
                   max_depth=req["max_depth"], rr_depth=req["rr_depth"], filter=rt.FILTER_BOX,
-                  tonemap=rt.TONEMAP_ACES_SRGB, seed=req["seed"])
+                  tonemap=rt.TONEMAP_ACES_SRGB, seed=req["seed"], guided=int(req["guided"]))
 
 
 def run_stream(srv, reqs, scene_ids, arrivals_s):
@@ -149,11 +150,22 @@ def main(argv=None):
     ids = [srv.add_scene(s) for s in keep]
     warm = make_requests(4, specs, a.seed + 1, res[:1], spps[:1])
     run_stream(srv, warm, ids, [0.0] * len(warm))  # graphs captured, scenes touched
-    sat = summarize(run_stream(srv, reqs, ids, [0.0] * len(reqs)), reqs)
+    def phase(arrivals, sat_mpaths=None):
+        before = srv.stats()
+        out = summarize(run_stream(srv, reqs, ids, arrivals), reqs, sat_mpaths)
+        after = srv.stats()
+        waves = after["waves"] - before["waves"]
+        # device time of the phase's waves over its makespan: how busy the GPU was
+        out["device_busy_fraction"] = (after["busy_ms"] - before["busy_ms"]) / (out["makespan_s"] * 1e3)
+        out["waves"] = waves
+        out["mean_paths_per_wave"] = (after["paths"] - before["paths"]) / max(1, waves)
+        return out
+
+    sat = phase([0.0] * len(reqs))
     rate = a.load * len(reqs) / sat["makespan_s"]
     gaps = np.random.default_rng(a.seed + 2).exponential(1.0 / rate, len(reqs))
     arrivals = np.cumsum(gaps) - gaps[0]
-    loaded = summarize(run_stream(srv, reqs, ids, arrivals), reqs, sat["aggregate_Mpaths_s"])
+    loaded = phase(arrivals, sat["aggregate_Mpaths_s"])
     stats = srv.stats()
     srv.close()
     line = {"metric": "serving time-to-image", "unit": "ms", "higher_is_better": False,
@@ -162,7 +174,7 @@ def main(argv=None):
             "slowdown_p99_over_p50": loaded["slowdown_p99_over_p50"],
             "aggregate_Mpaths_s": loaded["aggregate_Mpaths_s"], "load": a.load, "rate_jobs_s": rate,
             "saturation": sat, "loaded": loaded, "policy": a.policy,
-            "guided_requested": int(sum(r["guided"] for r in reqs)), "guided_rendered": 0,
+            "guided_requests": int(sum(r["guided"] for r in reqs)),
             "server": stats, "data": "synthetic", "small": a.small}
     print(json.dumps(line))
     return line

@@ -27,7 +27,7 @@ def _job_for(spec, scene_id, **over):
     st.update(over)
     return rt.job(scene_id, rt.camera(**spec.camera), st["width"], st["height"], st["spp"],
                   max_depth=st["max_depth"], rr_depth=st["rr_depth"], filter=st.get("filter", rt.FILTER_BOX),
-                  tonemap=st.get("tonemap", rt.TONEMAP_REINHARD), seed=st["seed"])
+                  tonemap=st.get("tonemap", rt.TONEMAP_REINHARD), seed=st["seed"], guided=st.get("guided", 0))
 
 
 def _alone(spec, **over):
@@ -143,3 +143,58 @@ def test_submit_errors_cancel_and_timeout():
     assert e.value.code == rt.RT_ERR_TIMEOUT and time.perf_counter() - t < 1.0
     assert bg.wait(big, 120000.0)["state"] == rt.JOB_DONE
     bg.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("policy", ["fair", "srpt"])
+def test_serve_bench_small(policy):
+    """The serving benchmark end to end on small scenes: every request
+    finishes, and the device-busy fraction from the server's wave events is a
+    fraction of the phase's wall time."""
+    from optixrender_b200 import serve_bench
+    line = serve_bench.main(["--small", "--requests", "24", "--policy", policy, "--wave-paths", str(1 << 15)])
+    for ph in ("saturation", "loaded"):
+        assert line[ph]["requests"] == 24
+        assert 0.0 < line[ph]["device_busy_fraction"] <= 1.05
+    assert line["server"]["jobs_done"] == 24 * 2 + 4
+    assert line["p99_ms"] >= line["p50_ms"] > 0.0
+
+
+def _mean_diff_se(a, b):
+    d = (a[..., :3].astype(np.float64) - b[..., :3]).mean(-1)
+    return d.mean(), d.std() / np.sqrt(d.size)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("policy", [rt.SERVE_FAIR, rt.SERVE_SRPT])
+def test_guided_jobs_share_the_scene_network(policy):
+    """Guided jobs sample their scene's network: it trains on the scene's
+    first guide_train_waves guided waves only, later guided jobs reuse it, each
+    guided image agrees with a plain render within 3 standard errors, and a
+    plain job served beside them is still bit-identical to its render alone."""
+    spec = scenes.portal(48, 48, 256)
+    srv = rt.Server(rt.server_options(wave_paths=1 << 14, max_depth=8, guide_train_waves=8, policy=policy))
+    keep = scenes.build_scene(spec)
+    sid = srv.add_scene(keep)
+    plain = srv.submit(_job_for(spec, sid, seed=101))
+    first = srv.submit(_job_for(spec, sid, seed=202, guided=1))
+    for jid in (plain, first):
+        assert srv.wait(jid, 120000.0)["state"] == rt.JOB_DONE
+    st = srv.stats()
+    assert st["training_waves"] == 8 and st["guided_waves"] > 8
+    second = srv.submit(_job_for(spec, sid, seed=303, guided=1))
+    assert srv.wait(second, 120000.0)["state"] == rt.JOB_DONE
+    st2 = srv.stats()
+    assert st2["training_waves"] == 8 and st2["guided_waves"] > st["guided_waves"]
+    ref = srv.download(plain)
+    lin, _ = _alone(spec, seed=101)
+    assert np.array_equal(ref.view(np.uint32), lin.view(np.uint32))
+    for jid in (first, second):
+        img = srv.download(jid)
+        assert np.isfinite(img).all()
+        m, se = _mean_diff_se(img, ref)
+        print(f"guided job {jid}: mean diff {m:.3e} se {se:.3e}")
+        assert abs(m) <= 3 * se
+        srv.release(jid)
+    srv.release(plain)
+    srv.close()

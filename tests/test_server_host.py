@@ -13,8 +13,9 @@ PROBE = r"""
 #include <stddef.h>
 #include "rt_capi.h"
 int main(void) {
-    printf("%zu %zu %zu %zu %zu %zu\n", sizeof(rt_server_options), sizeof(rt_job_desc), sizeof(rt_job_status),
-           sizeof(rt_server_stats), offsetof(rt_job_desc, seed), offsetof(rt_job_desc, width));
+    printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(rt_server_options), sizeof(rt_job_desc), sizeof(rt_job_status),
+           sizeof(rt_server_stats), offsetof(rt_job_desc, seed), offsetof(rt_job_desc, width),
+           sizeof(rt_render_stats), sizeof(rt_guide_options));
     return 0;
 }
 """
@@ -27,13 +28,14 @@ def test_server_struct_layouts_match_the_header(tmp_path):
     subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     want = [C.sizeof(rt.ServerOptions), C.sizeof(rt.JobDesc), C.sizeof(rt.JobStatus), C.sizeof(rt.ServerStats),
-            rt.JobDesc.seed.offset, rt.JobDesc.width.offset]
+            rt.JobDesc.seed.offset, rt.JobDesc.width.offset, C.sizeof(rt.RenderStats), C.sizeof(rt.GuideOptions)]
     assert got == want
 
 
 def test_server_defaults():
     o = rt.server_options()
     assert (o.wave_paths, o.max_jobs, o.max_depth, o.background, o.waves_in_flight) == (1 << 23, 256, 32, 1, 2)
+    assert (o.guide_train_waves, o.guide_steps, o.guide_prob) == (32, 4, 0.5)
     j = rt.job(0, rt.camera((0, 0, 1), (0, 0, 0)), 8, 8, 1)
     assert (j.max_depth, j.rr_depth, j.filter, j.seed) == (25, 0, rt.FILTER_GAUSSIAN, 1)
 
