@@ -189,6 +189,7 @@ struct SceneView {
     const float4* tri_a;   // 4 per triangle: normals, texcoords, mesh id
     int num_nodes;
     int num_tris;
+    int bvh_depth;           // wide levels (<= kStackSize)
     const MeshInfo* meshes;
     const DevMaterial* materials;
     const DevLight* lights;

@@ -154,6 +154,7 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st, bool
     v.tri_v = ds.tri_v.as<float4>();
     v.tri_a = ds.tri_a.as<float4>();
     v.num_nodes = int(bvh.nodes.size());
+    v.bvh_depth = bvh.depth;
     v.num_tris = int(nt);
     v.meshes = ds.meshes.as<MeshInfo>();
     v.materials = ds.materials.as<DevMaterial>();

@@ -235,6 +235,10 @@ struct TravState {
     TravRay r;
     const CwNode* nodes;
     const float4* tri_v;
+    // Postponed triangle groups may fill the stack only up to kStackSize -
+    // BVH depth: node groups on the stack are at most one per level of the
+    // current path, so they always find room.
+    int tri_room;
     uint2 g;
     float tmax;
     float t, b1, b2;
@@ -267,7 +271,7 @@ RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32
     // traversal with the others (+7% paths/s on the 2.59M-triangle scene).
     const int n_step = __popc(__activemask());
     while (tbits) {
-        if (__popc(__activemask()) * 100 < kPostponePercent * n_step && st.sp < kStackSize) {
+        if (__popc(__activemask()) * 100 < kPostponePercent * n_step && st.sp < s.tri_room) {
             st.push(make_uint2(tb | kTriGroup, tbits));
             break;
         }
@@ -321,6 +325,7 @@ RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& node
                     prepare_ray(s.r);
                     s.nodes = sc->nodes;
                     s.tri_v = sc->tri_v;
+                    s.tri_room = kStackSize - sc->bvh_depth;
                     s.tmax = s.r.tmax;
                     s.hit = -1;
                     st.sp = 0;
