@@ -53,6 +53,8 @@ def parse():
 
 
 def dist_init(n):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); NCCL
+    on GPUs, gloo where there is none (the CPU tests of this plumbing)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -60,9 +62,28 @@ def dist_init(n):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return rank, world, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    """The maximum of x over all ranks (the slowest rank's time)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mpaths(paths_per_rank: int, world: int, ms: float) -> float:
+    """Whole-job Mpaths/s: every rank's paths over the slowest rank's time."""
+    return paths_per_rank * world / (ms / 1e3) / 1e6
 
 
 class ClockSampler:
@@ -233,12 +254,9 @@ def main():
     ms = ev0.elapsed_time(ev1)
     st0 = r.stats()
     launches_per_step, wave_paths = st0["launches"], st0["wave_paths"]
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, world)
     ms_step = ms / args.steps
-    value = paths_per_step * world / (ms_step / 1e3) / 1e6
+    value = job_mpaths(paths_per_step, world, ms_step)
 
     # timed region B: the same steps with a CUDA event pair around every kernel
     # and device counters of nodes / triangles / rays, for the roofline
@@ -281,11 +299,8 @@ def main():
         if i > 0:
             e2e_t.append(dt)
     e2e_ms = float(np.mean(e2e_t)) * 1e3
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = paths_per_step * world / (e2e_ms / 1e3) / 1e6
+    e2e_ms = reduce_max(e2e_ms, world)
+    e2e_value = job_mpaths(paths_per_step, world, e2e_ms)
     h2d = int(r.stats()["h2d_bytes"])  # launch parameters + wave table uploaded by each Render()
 
     peak, peak_kind = measured_peak()

@@ -180,6 +180,12 @@ public:
         o.spp = spp;
         SetOptions(o);
     }
+    // Renderer::denoiserOn (Renderer.h:139): DownloadPixels shows the denoised colour.
+    void SetDenoiser(bool on) {
+        Options o = GetOptions();
+        o.denoise = on ? 1 : 0;
+        SetOptions(o);
+    }
     rt_renderer* handle() { return h_; }
 
 private:

@@ -188,6 +188,10 @@ typedef struct rt_options {
     float guide_prob;         /* 0.5 */
     int32_t guide_steps;      /* 4 */
     int32_t bvh_build;        /* RT_BVH_GPU (default): built on the device; RT_BVH_HOST: on the host */
+    /* Renderer::denoiserOn (core/include/Renderer.h:139, off by default): the
+     * displayed image (RGBA8) is the denoised colour; the accumulated colour
+     * stays noisy and RT_AOV_DENOISED downloads the denoised linear colour. */
+    int32_t denoise;
 } rt_options;
 
 /* Per-render statistics. */
@@ -214,7 +218,7 @@ typedef struct rt_render_stats {
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */
-enum { RT_AOV_COLOR = 0, RT_AOV_ALBEDO = 1, RT_AOV_NORMAL = 2 };
+enum { RT_AOV_COLOR = 0, RT_AOV_ALBEDO = 1, RT_AOV_NORMAL = 2, RT_AOV_DENOISED = 3 };
 
 typedef struct rt_scene rt_scene;
 typedef struct rt_renderer rt_renderer;
@@ -260,8 +264,10 @@ RT_API rt_status rt_scene_add_medium(rt_scene* s, const rt_medium* medium);
  * coordinates, wrap, bilinear, texels read as byte/255). */
 RT_API rt_status rt_scene_add_texture(rt_scene* s, const uint8_t* rgba, int32_t width, int32_t height,
                                       int32_t* texture_id);
-/* Scene::AddTexture(fileName): uncompressed BMP (8/24/32-bit) or binary
- * PGM/PPM (P5/P6), flipped so that row 0 is the bottom. */
+/* Scene::AddTexture(fileName), core/src/Scene.cpp:66-69 (stbi_load): PNG
+ * (not interlaced; grey, RGB, palette, grey+alpha, RGBA at 1-16 bits),
+ * uncompressed BMP (8/24/32-bit) or binary PGM/PPM (P5/P6), flipped so that
+ * row 0 is the bottom. */
 RT_API rt_status rt_scene_add_texture_file(rt_scene* s, const char* path, int32_t* texture_id);
 /* Size of texture `texture_id` and, when `rgba` is not NULL, its texels as stored. */
 RT_API rt_status rt_scene_get_texture(const rt_scene* s, int32_t texture_id, int32_t* width, int32_t* height,
@@ -320,6 +326,16 @@ RT_API rt_status rt_renderer_download_linear(rt_renderer* r, float* rgba);
 /* The albedo / normal AOVs the reference feeds its denoiser
  * (core/cuda/devicePrograms.cu:518-531). */
 RT_API rt_status rt_renderer_download_aov(rt_renderer* r, int32_t kind, float* rgba);
+/* The denoiser of rt_options.denoise on caller buffers (host pointers, w*h*4
+ * floats each; row 0 = bottom): colour and its first-hit albedo and normal
+ * AOVs in, denoised linear colour out.  Replaces optixDenoiserInvoke
+ * (core/src/Renderer.cpp:756) with an edge-avoiding a-trous wavelet filter;
+ * synchronous; allocates its device buffers. */
+/* Writes an RGBA8 frame (DownloadPixels layout, row 0 = bottom) as a PNG
+ * file: the screenshot the reference's viewer saves (main.cpp:82-85). */
+RT_API rt_status rt_write_png(const char* path, const uint32_t* rgba8, int32_t width, int32_t height);
+RT_API rt_status rt_denoise_image(const float* color, const float* albedo, const float* normal, int32_t width,
+                                  int32_t height, float* out);
 /* Device pointers of the float4 colour buffer and the RGBA8 buffer. */
 RT_API rt_status rt_renderer_device_buffers(rt_renderer* r, void** color_f32x4, void** rgba8);
 RT_API rt_status rt_renderer_get_stats(const rt_renderer* r, rt_render_stats* stats);

@@ -32,7 +32,7 @@ FILTER_BOX, FILTER_TENT, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2, 3
 RNG_LCG, RNG_PCG32 = 0, 1
 BVH_GPU, BVH_HOST = 0, 1
 TONEMAP_REINHARD, TONEMAP_ACES_SRGB, TONEMAP_CLAMP = 0, 1, 2
-AOV_COLOR, AOV_ALBEDO, AOV_NORMAL = 0, 1, 2
+AOV_COLOR, AOV_ALBEDO, AOV_NORMAL, AOV_DENOISED = 0, 1, 2, 3
 VERIFY_BSDF_EVAL, VERIFY_BSDF_SAMPLE, VERIFY_LIGHT_SAMPLE, VERIFY_LIGHT_EVAL = 0, 1, 2, 3
 VERIFY_MEDIUM_SAMPLE, VERIFY_PHASE_SAMPLE, VERIFY_PHASE_EVAL = 4, 5, 6
 
@@ -78,7 +78,7 @@ class Options(C.Structure):
                 ("seed", C.c_uint64), ("tonemap", C.c_int32), ("wave_paths", C.c_int32),
                 ("collect_stats", C.c_int32), ("exposure", C.c_float), ("guided", C.c_int32),
                 ("guide_train_spp", C.c_int32), ("guide_prob", C.c_float), ("guide_steps", C.c_int32),
-                ("bvh_build", C.c_int32)]
+                ("bvh_build", C.c_int32), ("denoise", C.c_int32)]
 
 
 class RenderStats(C.Structure):
@@ -193,6 +193,8 @@ def load_library():
         "rt_renderer_get_stats": (I32, [VP, P(RenderStats)]),
         "rt_renderer_frame_index": (I32, [VP, P(I32)]),
         "rt_renderer_trace": (I32, [VP, I32, VP, I64, VP, I32]),
+        "rt_denoise_image": (I32, [P(F), P(F), P(F), I32, I32, P(F)]),
+        "rt_write_png": (I32, [C.c_char_p, P(C.c_uint32), I32, I32]),
         "rt_verify_shading": (I32, [I32, P(Material), I32, P(Light), I32, P(Medium), I32, P(F), I64, P(F)]),
         "rt_kulla_conty_lut": (I32, [P(F), P(F)]),
         "rt_guide_options_default": (None, [P(GuideOptions)]),
@@ -743,6 +745,30 @@ class Guide:
         out = np.empty(p.shape[0], np.float32)
         _check(self._lib.rt_guide_pdf(self._h, _fptr(p), None, _fptr(uu), p.shape[0], _fptr(d), _fptr(out)))
         return d, out
+
+
+def write_png(path, pixels):
+    """Writes an (H, W) uint32 RGBA8 frame (row 0 = bottom, as download_pixels) as a PNG file."""
+    lib = load_library()
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    if px.ndim != 2:
+        raise ValueError("pixels must be an (H, W) uint32 array")
+    h, w = px.shape
+    _check(lib.rt_write_png(os.fsencode(str(path)), px.ctypes.data_as(C.POINTER(C.c_uint32)), w, h))
+
+
+def denoise_image(color, albedo, normal):
+    """The denoiser of Options.denoise on (H, W, 4) float32 colour, albedo and
+    normal images (row 0 = bottom); returns the denoised colour."""
+    lib = load_library()
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (color, albedo, normal)]
+    if any(a.ndim != 3 or a.shape[2] != 4 or a.shape != arrs[0].shape for a in arrs):
+        raise ValueError("color, albedo and normal must be (H, W, 4) images of one size")
+    h, w = arrs[0].shape[:2]
+    out = np.empty((h, w, 4), np.float32)
+    fp = C.POINTER(C.c_float)
+    _check(lib.rt_denoise_image(*(a.ctypes.data_as(fp) for a in arrs), w, h, out.ctypes.data_as(fp)))
+    return out
 
 
 def verify_shading(op, inputs, materials=(), lights=(), media=()):

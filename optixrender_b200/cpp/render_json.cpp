@@ -1,7 +1,7 @@
 // render_json - headless replacement of the reference's viewer (main.cpp:165-265):
 // loads a scene JSON (models/test.json schema), renders `frames` progressive
-// launches, and writes the RGBA8 image (DownloadPixels) as a binary PPM and
-// the float colour buffer as a PFM.
+// launches, and writes the RGBA8 image (DownloadPixels) as PNG and binary PPM
+// and the float colour buffer as a PFM.
 //
 //   render_json scene.json out_prefix [frames] [spp]
 #include <cstdio>
@@ -55,7 +55,8 @@ int main(int argc, char** argv) {
         renderer.DownloadLinear(lin.data());
         std::string pre = argv[2];
         if (!write_ppm((pre + ".ppm").c_str(), px, opts.width, opts.height) ||
-            !write_pfm((pre + ".pfm").c_str(), lin, opts.width, opts.height)) {
+            !write_pfm((pre + ".pfm").c_str(), lin, opts.width, opts.height) ||
+            rt_write_png((pre + ".png").c_str(), px.data(), opts.width, opts.height) != RT_OK) {
             std::fprintf(stderr, "could not write %s.*\n", argv[2]);
             return 1;
         }

@@ -760,6 +760,102 @@ __global__ void k_finalize(const JobDesc* __restrict__ jd) {
     j.rgba8[p] = tonemap_pixel(rgba, j.tonemap, j.exposure);
 }
 
+// ------------------------------------------------------------------ denoiser
+// Replaces the OptiX AI denoiser of Renderer::Render (core/src/Renderer.cpp:
+// 660-785), a closed library: an edge-avoiding a-trous wavelet filter
+// (Dammertz, Sewtz, Hanika and Lensch, HPG 2010).  It runs on irradiance
+// (colour divided by the first-hit albedo AOV, so texture detail is not
+// blurred), stops at edges of the normal and albedo AOVs - the guide layers
+// the reference gives its denoiser - and at irradiance differences relative
+// to the centre's luminance; the result is multiplied back by the albedo and
+// tonemapped.  Before the passes, a pixel brighter than kDnFirefly times the
+// brightest of its 8 neighbours is scaled down to that bound (an isolated
+// firefly would otherwise survive the edge-stopping weights).  Five passes
+// with tap spacings 1, 2, 4, 8, 16 (5 x 5 B3-spline taps each, 65 x 65 pixels
+// reach), the irradiance tolerance halving per pass.
+constexpr float kDnAlbedoMin = 1e-3f;
+constexpr float kDnFirefly = 4.0f;
+
+RT_D float dn_lum(float4 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+RT_D float3 dn_factor(float4 al) {
+    return make_float3(al.x > kDnAlbedoMin ? al.x : 1.0f, al.y > kDnAlbedoMin ? al.y : 1.0f,
+                       al.z > kDnAlbedoMin ? al.z : 1.0f);
+}
+
+__global__ void k_dn_demod(const float4* __restrict__ color, const float4* __restrict__ albedo,
+                           float4* __restrict__ irr, int64_t n) {
+    int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const float4 c = color[p];
+    const float3 f = dn_factor(albedo[p]);
+    irr[p] = make_float4(c.x / f.x, c.y / f.y, c.z / f.z, 1.0f);
+}
+
+__global__ void k_dn_clamp(const float4* __restrict__ in, float4* __restrict__ out, int w, int h) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int64_t p = int64_t(y) * w + x;
+    const float4 c = in[p];
+    float lmax = 0.0f;
+    for (int j = -1; j <= 1; j++)
+        for (int i = -1; i <= 1; i++) {
+            const int xx = x + i, yy = y + j;
+            if ((i | j) == 0 || xx < 0 || xx >= w || yy < 0 || yy >= h) continue;
+            lmax = fmaxf(lmax, dn_lum(__ldg(in + int64_t(yy) * w + xx)));
+        }
+    const float lc = dn_lum(c), bound = kDnFirefly * lmax;
+    const float s = lc > bound && lc > 0.0f ? bound / lc : 1.0f;
+    out[p] = make_float4(c.x * s, c.y * s, c.z * s, 1.0f);
+}
+
+__global__ void k_dn_atrous(const float4* __restrict__ in, float4* __restrict__ out,
+                            const float4* __restrict__ albedo, const float4* __restrict__ normal, int w, int h,
+                            int step, float inv_sc2, float inv_sn2, float inv_sa2) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int64_t p = int64_t(y) * w + x;
+    const float4 c = in[p], n = normal[p], a = albedo[p];
+    const float lp = dn_lum(c);
+    const float cs = inv_sc2 / (lp * lp + 1e-4f);
+    const float hk[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+    float sx = 0.f, sy = 0.f, sz = 0.f, ws = 0.f;
+#pragma unroll
+    for (int j = -2; j <= 2; j++) {
+        const int yy = y + j * step;
+        if (yy < 0 || yy >= h) continue;
+#pragma unroll
+        for (int i = -2; i <= 2; i++) {
+            const int xx = x + i * step;
+            if (xx < 0 || xx >= w) continue;
+            const int64_t q = int64_t(yy) * w + xx;
+            const float4 cq = __ldg(in + q), nq = __ldg(normal + q), aq = __ldg(albedo + q);
+            const float dc = (cq.x - c.x) * (cq.x - c.x) + (cq.y - c.y) * (cq.y - c.y) + (cq.z - c.z) * (cq.z - c.z);
+            const float dn = (nq.x - n.x) * (nq.x - n.x) + (nq.y - n.y) * (nq.y - n.y) + (nq.z - n.z) * (nq.z - n.z);
+            const float da = (aq.x - a.x) * (aq.x - a.x) + (aq.y - a.y) * (aq.y - a.y) + (aq.z - a.z) * (aq.z - a.z);
+            const float wq = hk[i + 2] * hk[j + 2] * __expf(-(dc * cs + dn * inv_sn2 + da * inv_sa2));
+            sx += wq * cq.x;
+            sy += wq * cq.y;
+            sz += wq * cq.z;
+            ws += wq;
+        }
+    }
+    // the centre tap always has weight 9/64, so ws > 0 unless c is not finite
+    out[p] = ws > 0.0f ? make_float4(sx / ws, sy / ws, sz / ws, 1.0f) : c;
+}
+
+__global__ void k_dn_remod(const float4* __restrict__ irr, const float4* __restrict__ albedo,
+                           float4* __restrict__ out, uint32_t* __restrict__ rgba8, int64_t n, int tonemap,
+                           float exposure) {
+    int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const float4 e = irr[p];
+    const float3 f = dn_factor(albedo[p]);
+    const float4 c = make_float4(e.x * f.x, e.y * f.y, e.z * f.z, 1.0f);
+    out[p] = c;
+    if (rgba8) rgba8[p] = tonemap_pixel(c, tonemap, exposure);
+}
+
 // ------------------------------------------------------------------ ray queries
 template <bool AnyHit>
 __global__ void __launch_bounds__(kBlock) k_trace(SceneView sc, const float* __restrict__ rays, int64_t n,
@@ -924,6 +1020,27 @@ void launch_finalize(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
 void launch_begin_n(const JobDesc* dj, int64_t npix, cudaStream_t st) { k_begin<<<grid_for(npix, 256), 256, 0, st>>>(dj); }
 void launch_finalize_n(const JobDesc* dj, int64_t npix, cudaStream_t st) {
     k_finalize<<<grid_for(npix, 256), 256, 0, st>>>(dj);
+}
+int launch_denoise(const DenoiseArgs& d, cudaStream_t st) {
+    const int64_t n = int64_t(d.w) * d.h;
+    if (n <= 0) return 0;
+    k_dn_demod<<<grid_for(n, 256), 256, 0, st>>>(d.color, d.albedo, d.tmp0, n);
+    const dim3 blk(16, 16), grd(unsigned((d.w + 15) / 16), unsigned((d.h + 15) / 16));
+    k_dn_clamp<<<grd, blk, 0, st>>>(d.tmp0, d.tmp1, d.w, d.h);
+    float4* src = d.tmp1;
+    float4* dst = d.tmp0;
+    float inv_sc2 = 1.0f / (kDenoiseSigmaColor * kDenoiseSigmaColor);
+    for (int it = 0; it < kDenoisePasses; it++) {
+        k_dn_atrous<<<grd, blk, 0, st>>>(src, dst, d.albedo, d.normal, d.w, d.h, 1 << it, inv_sc2,
+                                         1.0f / (kDenoiseSigmaNormal * kDenoiseSigmaNormal),
+                                         1.0f / (kDenoiseSigmaAlbedo * kDenoiseSigmaAlbedo));
+        inv_sc2 *= 4.0f;  // sigma halves per pass
+        float4* t = src;
+        src = dst;
+        dst = t;
+    }
+    k_dn_remod<<<grid_for(n, 256), 256, 0, st>>>(src, d.albedo, d.out, d.rgba8, n, d.tonemap, d.exposure);
+    return kDenoisePasses + 3;
 }
 void launch_trace(const SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st) {
     if (n <= 0) return;

@@ -125,6 +125,26 @@ struct LaunchShape {
     int blocks_extend, blocks_shade, blocks_shadow;
 };
 void query_shape(LaunchShape& s);
+// The a-trous denoiser: colour, albedo and normal AOVs (W x H float4) in;
+// denoised linear colour (and, when rgba8 is not null, its tonemapped RGBA8)
+// out; tmp0 / tmp1 are W x H float4 scratch.  Returns the kernels launched.
+constexpr int kDenoisePasses = 5;
+constexpr float kDenoiseSigmaColor = 1.0f;   // irradiance difference relative to the centre's luminance
+constexpr float kDenoiseSigmaNormal = 0.3f;
+constexpr float kDenoiseSigmaAlbedo = 0.1f;
+struct DenoiseArgs {
+    const float4* color;
+    const float4* albedo;
+    const float4* normal;
+    float4* tmp0;
+    float4* tmp1;
+    float4* out;
+    uint32_t* rgba8;
+    int w, h;
+    int tonemap;
+    float exposure;
+};
+int launch_denoise(const DenoiseArgs& d, cudaStream_t st);
 void launch_begin(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);
 void launch_raygen(const rtd::Ctx& c, cudaStream_t st);
 void launch_extend(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);

@@ -13,6 +13,7 @@
 
 #include "rt_bvh.h"
 #include "rt_guide_host.h"
+#include "rt_png.h"
 #include "rt_internal.h"
 
 using namespace rtd;
@@ -212,6 +213,9 @@ struct rt_renderer {
     int capacity = 0;
     DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, ctl, segs, job;
     DevBuf sorted;            // shade queue by material type
+    DevBuf dn_tmp0, dn_tmp1, dn_out;  // denoiser scratch and output (rt_options.denoise)
+    int dn_pixels = 0;                // pixels covered by the denoiser buffers
+    bool denoised = false;            // dn_out holds the last render's denoised colour
     DevBuf mat_tex;           // per-slot textured materials (scenes with textures)
     bool sort_shade = true;   // RT_SORT_SHADE=0 keeps the shade queue in extend order
     int wave_paths = 0;       // slots per wave of the last render
@@ -261,6 +265,19 @@ rt_status ensure_pixels(rt_renderer* r, int w, int h) {
     RT_CUDA(cudaMemsetAsync(r->rgba8.ptr, 0, n * 4, r->stream), "clear frame buffers");
     r->pw = w;
     r->ph = h;
+    r->denoised = false;
+    return RT_OK;
+}
+
+rt_status ensure_denoiser(rt_renderer* r) {
+    const int n = r->pw * r->ph;
+    if (r->dn_pixels == n) return RT_OK;
+    DevBuf* bufs[] = {&r->dn_tmp0, &r->dn_tmp1, &r->dn_out};
+    for (DevBuf* b : bufs) {
+        b->release();
+        RT_CUDA(b->alloc(size_t(n) * sizeof(float4)), "allocate denoiser buffers");
+    }
+    r->dn_pixels = n;
     return RT_OK;
 }
 
@@ -650,6 +667,25 @@ rt_status rt_renderer_render(rt_renderer* r) {
     ext = int(nwaves) * o.max_depth;
     rth::launch_finalize(hj, dj, s);
     launches++;
+    r->denoised = false;
+    if (o.denoise) {  // Renderer.cpp:660-785: the displayed image is the denoised colour
+        st = ensure_denoiser(r);
+        if (st) return st;
+        rth::DenoiseArgs d;
+        d.color = r->color.as<float4>();
+        d.albedo = r->albedo.as<float4>();
+        d.normal = r->normal.as<float4>();
+        d.tmp0 = r->dn_tmp0.as<float4>();
+        d.tmp1 = r->dn_tmp1.as<float4>();
+        d.out = r->dn_out.as<float4>();
+        d.rgba8 = r->rgba8.as<uint32_t>();
+        d.w = r->pw;
+        d.h = r->ph;
+        d.tonemap = o.tonemap;
+        d.exposure = o.exposure;
+        launches += rth::launch_denoise(d, s);
+        r->denoised = true;
+    }
     RT_CUDA(cudaEventRecord(r->ev1, s), "record event");
     RT_CUDA(cudaGetLastError(), "launch");
     r->rendered = true;
@@ -717,6 +753,10 @@ rt_status rt_renderer_download_aov(rt_renderer* r, int32_t kind, float* rgba) {
     if (kind == RT_AOV_COLOR) return download(r, r->color, rgba, n);
     if (kind == RT_AOV_ALBEDO) return download(r, r->albedo, rgba, n);
     if (kind == RT_AOV_NORMAL) return download(r, r->normal, rgba, n);
+    if (kind == RT_AOV_DENOISED) {
+        if (!r->denoised) return fail(RT_ERR_STATE, "rt_renderer_download_aov: the last render was not denoised");
+        return download(r, r->dn_out, rgba, n);
+    }
     return fail(RT_ERR_INVALID_ARG, "rt_renderer_download_aov: unknown kind");
 }
 
@@ -812,6 +852,42 @@ rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, const float
     RT_CUDA(cudaMemcpyAsync(hits, sc + 2 * cap, size_t(n) * 16, cudaMemcpyDeviceToHost, r->stream),
             "rt_renderer_trace_noalloc");
     RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace_noalloc");
+    return RT_OK;
+}
+
+rt_status rt_write_png(const char* path, const uint32_t* rgba8, int32_t w, int32_t h) {
+    if (!path || !rgba8 || w <= 0 || h <= 0) return fail(RT_ERR_INVALID_ARG, "rt_write_png: bad argument");
+    std::string err;
+    if (!rti::write_png(path, rgba8, w, h, err)) return fail(RT_ERR_IO, "rt_write_png: " + err);
+    return RT_OK;
+}
+
+rt_status rt_denoise_image(const float* color, const float* albedo, const float* normal, int32_t w, int32_t h,
+                           float* out) {
+    if (!color || !albedo || !normal || !out || w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28))
+        return fail(RT_ERR_INVALID_ARG, "rt_denoise_image: bad argument");
+    const size_t bytes = size_t(w) * h * sizeof(float4);
+    DevBuf c, a, n, t0, t1, o;
+    DevBuf* all[] = {&c, &a, &n, &t0, &t1, &o};
+    for (DevBuf* b : all) RT_CUDA(b->alloc(bytes), "rt_denoise_image");
+    RT_CUDA(cudaMemcpy(c.ptr, color, bytes, cudaMemcpyHostToDevice), "rt_denoise_image");
+    RT_CUDA(cudaMemcpy(a.ptr, albedo, bytes, cudaMemcpyHostToDevice), "rt_denoise_image");
+    RT_CUDA(cudaMemcpy(n.ptr, normal, bytes, cudaMemcpyHostToDevice), "rt_denoise_image");
+    rth::DenoiseArgs d;
+    d.color = c.as<float4>();
+    d.albedo = a.as<float4>();
+    d.normal = n.as<float4>();
+    d.tmp0 = t0.as<float4>();
+    d.tmp1 = t1.as<float4>();
+    d.out = o.as<float4>();
+    d.rgba8 = nullptr;
+    d.w = w;
+    d.h = h;
+    d.tonemap = RT_TONEMAP_REINHARD;
+    d.exposure = 1.0f;
+    rth::launch_denoise(d, nullptr);
+    RT_CUDA(cudaGetLastError(), "rt_denoise_image");
+    RT_CUDA(cudaMemcpy(out, o.ptr, bytes, cudaMemcpyDeviceToHost), "rt_denoise_image");
     return RT_OK;
 }
 

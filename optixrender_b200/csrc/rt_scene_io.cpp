@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "rt_png.h"
 #include "rt_internal.h"
 
 using namespace rti;
@@ -361,8 +362,9 @@ rt_status add_obj(rt_scene* s, const std::string& path, const rt_material* mat, 
 // ------------------------------------------------------------------ LDR images
 // Texture files for Scene::AddTexture (core/src/Scene.cpp:66-69, 181-189:
 // stbi_load forced to RGBA with a vertical flip, so row 0 is the bottom of
-// the picture).  Read here without an image library: uncompressed BMP (8-bit
-// palette, 24-bit, 32-bit) and binary PGM/PPM (P5/P6, maxval <= 255).
+// the picture).  Read here without an image library: PNG (rt_png.cpp),
+// uncompressed BMP (8-bit palette, 24-bit, 32-bit) and binary PGM/PPM (P5/P6,
+// maxval <= 255).
 uint32_t rd32(const std::string& d, size_t o) {
     return uint32_t(uint8_t(d[o])) | (uint32_t(uint8_t(d[o + 1])) << 8) | (uint32_t(uint8_t(d[o + 2])) << 16) |
            (uint32_t(uint8_t(d[o + 3])) << 24);
@@ -490,8 +492,10 @@ bool read_image(const std::string& path, std::vector<uint8_t>& rgba, int& w, int
         ok = read_bmp(d, rgba, w, h, err);
     else if (d.size() >= 2 && d[0] == 'P' && (d[1] == '5' || d[1] == '6'))
         ok = read_pnm(d, rgba, w, h, err);
+    else if (d.size() >= 8 && uint8_t(d[0]) == 137 && d[1] == 'P' && d[2] == 'N' && d[3] == 'G')
+        ok = read_png(d, rgba, w, h, err);
     else {
-        err = "unsupported image format (BMP or binary PGM/PPM)";
+        err = "unsupported image format (PNG, BMP or binary PGM/PPM)";
         ok = false;
     }
     if (!ok) err = path + ": " + err;
