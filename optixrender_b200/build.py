@@ -31,9 +31,9 @@ CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fopenmp", "-Wa
 
 CU_SOURCES = ["rt_kernels.cu", "rt_trace_scratch.cu", "rt_guide.cu", "rt_guide_api.cu", "rt_bvh_gpu.cu"]
 CPP_SOURCES = ["rt_capi.cpp", "rt_renderer.cpp", "rt_bvh.cpp", "rt_tables.cpp", "rt_scene_io.cpp", "rt_server.cpp",
-               "rt_png.cpp"]
+               "rt_png.cpp", "rt_jpeg.cpp"]
 HEADERS = ["rt_device.cuh", "rt_shading.cuh", "rt_traverse.cuh", "rt_kernels.cuh", "rt_internal.h", "rt_bvh.h",
-           "rt_media.cuh", "rt_guide.cuh", "rt_guide_host.h", "rt_png.h"]
+           "rt_media.cuh", "rt_guide.cuh", "rt_guide_host.h", "rt_image.h"]
 
 
 def _newer(out: Path, inputs) -> bool:

@@ -1,4 +1,5 @@
-// rt_png.h - PNG decoding (textures) and encoding (frames), rt_png.cpp.
+// rt_image.h - image codecs without an image library: PNG decoding and
+// encoding (rt_png.cpp), baseline JPEG decoding (rt_jpeg.cpp).
 #pragma once
 
 #include <cstddef>
@@ -14,4 +15,7 @@ bool zlib_inflate(const uint8_t* src, size_t n, std::vector<uint8_t>& out, size_
 bool read_png(const std::string& file, std::vector<uint8_t>& rgba, int& w, int& h, std::string& err);
 // RGBA8 frame (row 0 = bottom, as DownloadPixels) -> PNG file.
 bool write_png(const std::string& path, const uint32_t* rgba8, int w, int h, std::string& err);
+// JPEG file bytes -> RGBA8, row 0 = bottom.  Baseline / extended sequential
+// Huffman-coded, 8-bit, grey or YCbCr, one interleaved scan.
+bool read_jpeg(const std::string& file, std::vector<uint8_t>& rgba, int& w, int& h, std::string& err);
 }  // namespace rti

@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "rt_png.h"
+#include "rt_image.h"
 
 namespace rti {
 namespace {

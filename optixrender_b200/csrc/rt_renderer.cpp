@@ -13,7 +13,7 @@
 
 #include "rt_bvh.h"
 #include "rt_guide_host.h"
-#include "rt_png.h"
+#include "rt_image.h"
 #include "rt_internal.h"
 
 using namespace rtd;

@@ -15,7 +15,7 @@
 #include <string>
 #include <vector>
 
-#include "rt_png.h"
+#include "rt_image.h"
 #include "rt_internal.h"
 
 using namespace rti;
@@ -363,6 +363,7 @@ rt_status add_obj(rt_scene* s, const std::string& path, const rt_material* mat, 
 // Texture files for Scene::AddTexture (core/src/Scene.cpp:66-69, 181-189:
 // stbi_load forced to RGBA with a vertical flip, so row 0 is the bottom of
 // the picture).  Read here without an image library: PNG (rt_png.cpp),
+// baseline JPEG (rt_jpeg.cpp),
 // uncompressed BMP (8-bit palette, 24-bit, 32-bit) and binary PGM/PPM (P5/P6,
 // maxval <= 255).
 uint32_t rd32(const std::string& d, size_t o) {
@@ -494,8 +495,10 @@ bool read_image(const std::string& path, std::vector<uint8_t>& rgba, int& w, int
         ok = read_pnm(d, rgba, w, h, err);
     else if (d.size() >= 8 && uint8_t(d[0]) == 137 && d[1] == 'P' && d[2] == 'N' && d[3] == 'G')
         ok = read_png(d, rgba, w, h, err);
+    else if (d.size() >= 3 && uint8_t(d[0]) == 0xFF && uint8_t(d[1]) == 0xD8 && uint8_t(d[2]) == 0xFF)
+        ok = read_jpeg(d, rgba, w, h, err);
     else {
-        err = "unsupported image format (PNG, BMP or binary PGM/PPM)";
+        err = "unsupported image format (PNG, JPEG, BMP or binary PGM/PPM)";
         ok = false;
     }
     if (!ok) err = path + ": " + err;
