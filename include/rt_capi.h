@@ -547,7 +547,16 @@ enum {
     /* EvaluatePhase, core/cuda/Medium.h:83-94.
      * in: 16 floats: V[3] L[3] medium_index pad[9]
      * out: 8 floats: attenuation[3] pdf pad[4] */
-    RT_VERIFY_PHASE_EVAL = 6
+    RT_VERIFY_PHASE_EVAL = 6,
+    /* What guided sampling mixes with its proposal: the real density of the
+     * directions SampleMaterial draws, at L (the reported pdfs use the
+     * reference's isotropic GGX D with cos^2 for cos^4, and plastic and the
+     * clear-coated conductor select lobes by a Fresnel term of V), the pdf
+     * EvaluateMaterial and the sampler report there, and f_dir, what plain
+     * BSDF sampling integrates at L.
+     * in: 16 floats: N[3] V[3] L[3] front_face material_index pad[5]
+     * out: 8 floats: sampling_density evaluate_pdf sampler_reported_pdf f_dir[3] pad[2] */
+    RT_VERIFY_BSDF_SAMPLE_PDF = 7
 };
 
 /* Runs one verification op over n queries on the device.  `materials`,

@@ -34,7 +34,7 @@ BVH_GPU, BVH_HOST = 0, 1
 TONEMAP_REINHARD, TONEMAP_ACES_SRGB, TONEMAP_CLAMP = 0, 1, 2
 AOV_COLOR, AOV_ALBEDO, AOV_NORMAL, AOV_DENOISED = 0, 1, 2, 3
 VERIFY_BSDF_EVAL, VERIFY_BSDF_SAMPLE, VERIFY_LIGHT_SAMPLE, VERIFY_LIGHT_EVAL = 0, 1, 2, 3
-VERIFY_MEDIUM_SAMPLE, VERIFY_PHASE_SAMPLE, VERIFY_PHASE_EVAL = 4, 5, 6
+VERIFY_MEDIUM_SAMPLE, VERIFY_PHASE_SAMPLE, VERIFY_PHASE_EVAL, VERIFY_BSDF_SAMPLE_PDF = 4, 5, 6, 7
 
 F3 = C.c_float * 3
 

@@ -537,11 +537,17 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                             float unused;
                             sample_material(sc, s, rng, V, L, unused);
                         }
-                        v3 f = eval_material(sc, s, V, L, bpdf);
-                        const float pm = gp * rtg::mixture_pdf(gmix, L) + (1.0f - gp) * bpdf;
+                        // weighted by what plain BSDF sampling integrates over the combined
+                        // real density; the emission MIS weight at the next vertex uses the
+                        // pdf plain sampling reports (guide_bsdf)
+                        v3 fd;
+                        float p_true, p_rep;
+                        guide_bsdf(sc, s, V, L, fd, p_true, p_rep);
+                        const float q = rtg::mixture_pdf(gmix, L);
+                        const float pm = gp * q + (1.0f - gp) * p_true;
                         float ct = fabsf(dot(s.sn, L));
-                        history *= (f * ct / pm);
-                        pre_pdf = pm;
+                        history *= (fd * ct / pm);
+                        pre_pdf = gp * q + (1.0f - gp) * p_rep;
                         rec_pdf = pm;
                         rec_cos = ct;
                     } else {
@@ -904,7 +910,23 @@ __global__ void k_verify(int op, SceneView sc, const DevLight* lights, const Dev
     float r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     ListRng rng;
     rng.used = 0;
-    if (op == RT_VERIFY_BSDF_EVAL || op == RT_VERIFY_BSDF_SAMPLE) {
+    if (op == RT_VERIFY_BSDF_SAMPLE_PDF) {
+        Surf s;
+        s.sn = ld3(x);
+        s.front = x[9] != 0.0f;
+        s.mat = sc.materials + int(x[10]);
+        float epdf = 0.0f;
+        eval_material(sc, s, ld3(x + 3), ld3(x + 6), epdf);
+        v3 fd;
+        float p_true, p_rep;
+        guide_bsdf(sc, s, ld3(x + 3), ld3(x + 6), fd, p_true, p_rep);
+        r[0] = p_true;
+        r[1] = epdf;
+        r[2] = p_rep;
+        r[3] = fd.x;
+        r[4] = fd.y;
+        r[5] = fd.z;
+    } else if (op == RT_VERIFY_BSDF_EVAL || op == RT_VERIFY_BSDF_SAMPLE) {
         bool sample = op == RT_VERIFY_BSDF_SAMPLE;
         Surf s;
         s.sn = ld3(x);

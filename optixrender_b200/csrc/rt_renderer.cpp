@@ -894,17 +894,19 @@ rt_status rt_denoise_image(const float* color, const float* albedo, const float*
 rt_status rt_verify_shading(int32_t op, const rt_material* materials, int32_t nmat, const rt_light* lights, int32_t nl,
                             const rt_medium* media, int32_t nm, const float* in, int64_t n, float* out) {
     if (!in || !out || n < 0) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: bad argument");
-    if (op < RT_VERIFY_BSDF_EVAL || op > RT_VERIFY_PHASE_EVAL) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: unknown op");
+    if (op < RT_VERIFY_BSDF_EVAL || op > RT_VERIFY_BSDF_SAMPLE_PDF)
+        return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: unknown op");
     for (int64_t i = 0; i < n; i++) {
         const float* x = in + i * 16;
-        int idx = op == RT_VERIFY_BSDF_EVAL ? int(x[10])
+        int idx = (op == RT_VERIFY_BSDF_EVAL || op == RT_VERIFY_BSDF_SAMPLE_PDF) ? int(x[10])
                   : op == RT_VERIFY_BSDF_SAMPLE ? int(x[13])
                   : op == RT_VERIFY_LIGHT_SAMPLE ? int(x[5])
                   : op == RT_VERIFY_LIGHT_EVAL ? int(x[7])
                   : op == RT_VERIFY_MEDIUM_SAMPLE ? int(x[3])
                   : op == RT_VERIFY_PHASE_SAMPLE ? int(x[7])
                                                   : int(x[6]);
-        int lim = (op <= RT_VERIFY_BSDF_SAMPLE) ? nmat : (op <= RT_VERIFY_LIGHT_EVAL ? nl : nm);
+        int lim = (op <= RT_VERIFY_BSDF_SAMPLE || op == RT_VERIFY_BSDF_SAMPLE_PDF) ? nmat
+                  : (op <= RT_VERIFY_LIGHT_EVAL ? nl : nm);
         if (idx < 0 || idx >= lim) return fail(RT_ERR_INVALID_ARG, "rt_verify_shading: index out of range");
     }
     if (n == 0) return RT_OK;

@@ -557,6 +557,88 @@ RT_D v3 sample_material(const SceneView& sc, const Surf& s, RNG& rng, v3 V, v3& 
     return v3(0.0f);
 }
 
+// The isotropic GGX distribution with the cos^4 of its definition (the
+// anisotropic branch of ggx_d already has it): the density with which the
+// visible-normal sampler draws half vectors is smith_g1 * (V.H) * this / (N.V).
+RT_D float ggx_d_exact(v3 H, v3 N, float au, float av) {
+    if (au != av) return ggx_d(H, N, au, av);
+    const float c = dot(H, N);
+    if (c <= 0.0f) return 0.0f;
+    const float c2 = sqr(c), t2 = (1.0f - c2) / c2, a2 = au * av;
+    return a2 / (kPi * c2 * c2 * sqr(a2 + t2));
+}
+RT_D float vndf_reflect_pdf(v3 V, v3 H, v3 N, float au, float av) {
+    return smith_g1(V, H, N, au, av) * dot(V, H) * ggx_d_exact(H, N, au, av) / dot(N, V) *
+           fabsf(1.0f / (4.0f * dot(V, H)));
+}
+
+// What plain BSDF sampling integrates, for the one-sample MIS of guided
+// sampling.  The reference's sampler draws half vectors from the exact
+// visible-normal distribution, but its isotropic DistributionGGX
+// (Microfacet.h:144-160) divides by cos^2 where the definition has cos^4, so
+// the pdf it reports, like EvaluateMaterial's, is not the density of its
+// samples; and plastic and the clear-coated conductor pick their lobe with a
+// Fresnel term of V alone (SamplePlastic, Material.h:327; Sample-
+// ClearCoatedConductor, :669) where the evaluators use F(L, N), resp. F(V, H)
+// (:273, :634).  A BSDF-sampled path is weighted by f / pdf as the sampler
+// reports them, so plain BSDF sampling integrates f_dir = p_true * E[f / pdf |
+// L].  Outputs: f_dir; p_true, the sampler's real density at L; p_rep, the
+// pdf the sampler reports at L (plain sampling's emission MIS weight uses it).
+// With these, guided sampling reduces exactly to plain sampling as the
+// mixture probability goes to zero.
+RT_D void guide_bsdf(const SceneView& sc, const Surf& s, v3 V, v3 L, v3& f_dir, float& p_true, float& p_rep) {
+    f_dir = v3(0.0f);
+    p_true = p_rep = 0.0f;
+    if (!s.mat) return;
+    const MatParams m = load_material(s.mat);
+    const v3 N = s.sn;
+    const float au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
+    switch (m.type) {
+        case RT_MAT_CONDUCTOR:
+        case RT_MAT_METAL_WORKFLOW:
+        case RT_MAT_CLEARCOATED_CONDUCTOR: {
+            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return;
+            float pb = 0.0f;
+            const v3 fb = eval_material(sc, s, V, L, pb);
+            const v3 H = normalize(V + L);
+            const float spec = vndf_reflect_pdf(V, H, N, au, av);
+            if (m.type == RT_MAT_CONDUCTOR) {
+                p_true = spec;
+            } else if (m.type == RT_MAT_METAL_WORKFLOW) {
+                const float diel = 1.0f - m.metallic, sp = m.metallic + diel, pdiff = diel / (diel + sp);
+                p_true = (1.0f - pdiff) * spec + pdiff * cosine_pdf(dot(N, L));
+            } else {
+                const float cw = m.coat_weight * fresnel_dielectric(V, N, 1.0f / 1.5f);
+                p_true = cw * vndf_reflect_pdf(V, H, N, sqr(m.cru), sqr(m.crv)) + (1.0f - cw) * spec;
+            }
+            p_rep = pb;
+            if (pb > 0.0f) f_dir = fb * (p_true / pb);
+            return;
+        }
+        case RT_MAT_PLASTIC: {
+            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return;
+            const float eta = m.int_ior / m.ext_ior;
+            const v3 H = normalize(V + L);
+            const float Fo = fresnel_dielectric(V, N, 1.0f / eta), Fi = fresnel_dielectric(L, N, 1.0f / eta);
+            const float w = plastic_weight(m);
+            float ps = Fo * w, pd = (1.0f - Fo) * (1.0f - w);
+            ps = ps / (ps + pd);
+            float unused;
+            const v3 f_spec = plastic_f(sc, m, N, V, L, H, Fo, Fo, ps, unused);  // SamplePlastic's specular branch
+            const v3 f_diff = plastic_f(sc, m, N, V, L, H, Fo, Fi, ps, p_rep);    // its diffuse branch; the reported pdf
+            const float pc = cosine_pdf(dot(N, L));
+            const float spec_true = vndf_reflect_pdf(V, H, N, au, av);
+            p_true = ps * spec_true + (1.0f - ps) * pc;
+            if (p_rep > 0.0f) f_dir = (ps * spec_true * f_spec + (1.0f - ps) * pc * f_diff) / p_rep;
+            return;
+        }
+        default: {  // cosine-sampled types: the reported pdf is the density
+            f_dir = eval_material(sc, s, V, L, p_true);
+            p_rep = p_true;
+        }
+    }
+}
+
 // ------------------------------------------------------------ lights
 struct LightParams {
     int type;

@@ -34,10 +34,25 @@ def assert_same_mean(a, b, label):
     assert abs(d.mean()) <= 3 * se
 
 
+def _coated_cornell(w, h, spp):
+    """The Cornell box with plastic walls and a rough clear-coated conductor
+    box: the two materials whose BSDF sampler density differs from the
+    evaluator's pdf."""
+    spec = scenes.cornell(w, h, spp)
+    for m in spec.meshes:
+        if m.material["type"] == rt.MAT_DIFFUSE:
+            m.material = dict(type=rt.MAT_PLASTIC, albedo=m.material["albedo"], roughness=0.4, int_ior=1.5,
+                              ext_ior=1.0)
+        else:
+            m.material = dict(type=rt.MAT_CLEARCOATED_CONDUCTOR, albedo=(1.0, 1.0, 1.0), roughness=0.5,
+                              coat_weight=1.0, coat_roughness_u=0.4, coat_roughness_v=0.4)
+    return spec
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["portal", "cornell"])
+@pytest.mark.parametrize("name", ["portal", "cornell", "coated"])
 def test_guided_agrees_with_plain_within_3se(name):
-    spec = scenes.portal(48, 48, 256) if name == "portal" else scenes.cornell(48, 48, 256)
+    spec = {"portal": scenes.portal, "cornell": scenes.cornell, "coated": _coated_cornell}[name](48, 48, 256)
     _, _, plain = render(spec, seed=101)
     _, _, guided = render(spec, seed=202, guided=1, guide_train_spp=32)
     assert np.isfinite(guided).all()
