@@ -215,6 +215,7 @@ typedef struct rt_render_stats {
     int64_t nan_throughput_paths; /* paths ended by IsNan(history), devicePrograms.cu:487-489 */
     int64_t wave_paths;        /* path slots per wave of the last Render() */
     int64_t h2d_bytes;         /* bytes copied host to device by the last Render() */
+    int64_t watchdog_walks;    /* grid-medium walks that hit the device step budget (see rt_renderer_synchronize) */
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */
@@ -318,6 +319,11 @@ RT_API rt_status rt_renderer_set_stream(rt_renderer* r, void* cuda_stream);
  * samples per pixel, running-mean accumulation when progressive, and the
  * tonemap of core/cuda/PostProcessing.cu:50-59.  Asynchronous. */
 RT_API rt_status rt_renderer_render(rt_renderer* r);
+/* Waits for the renderer's work.  RT_ERR_DEVICE_WATCHDOG: some walk through
+ * a grid medium in the last render exhausted the device's step budget (4096
+ * tentative collisions) and was ended with zero weight; the image is complete
+ * but those samples are missing (the reference's equivalent is a hung or
+ * timed-out launch). */
 RT_API rt_status rt_renderer_synchronize(rt_renderer* r);
 /* Renderer::DownloadPixels, core/src/Renderer.cpp:878-880 (RGBA8). */
 RT_API rt_status rt_renderer_download_rgba8(rt_renderer* r, uint32_t* pixels);

@@ -53,6 +53,8 @@ RT_HD v3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
 // Depth limit of the per-thread traversal stack; a BVH deeper than this is
 // rejected at upload.
 constexpr int kStackSize = 32;
+// Tentative collisions one delta- or ratio-tracking walk may take (rt_media.cuh).
+constexpr int kMaxTrackingSteps = 4096;
 
 constexpr float kEps = 1e-4f;                                  // core/cuda/Utils.h:10
 constexpr float kPi = 3.14159265358979323846f;                 // Utils.h:11

@@ -194,20 +194,21 @@ RT_D bool nee_pdf_ok(float p) { return p > 0.0f && p < FLT_MAX; }
 // SampleMediumDistance (Medium.h:233-244) for either medium type.
 template <class RNG>
 RT_D bool medium_sample(const DevMedium* mp, const MedParams& med, v3 o, v3 d, float maxd, float& dist, float& tp,
-                        v3& tr, RNG& rng) {
+                        v3& tr, RNG& rng, int& budget_hits) {
     if (med.type == RT_MEDIUM_GRID) {
         tp = 1.0f;
-        return grid_sample_distance(load_grid(mp), o, d, maxd, rng, dist, tr);
+        return grid_sample_distance(load_grid(mp), o, d, maxd, rng, dist, tr, budget_hits);
     }
     return sample_medium_distance(med, maxd, dist, tp, tr, rng);
 }
 // EvaluateMediumDistance(medium, false, ...) (Medium.h:222-231): the
 // transmittance of a next-event segment; ratio tracking for a grid.
 template <class RNG>
-RT_D v3 medium_transmittance(const DevMedium* mp, const MedParams& med, v3 o, v3 d, float dist, float& tp, RNG& rng) {
+RT_D v3 medium_transmittance(const DevMedium* mp, const MedParams& med, v3 o, v3 d, float dist, float& tp, RNG& rng,
+                             int& budget_hits) {
     if (med.type == RT_MEDIUM_GRID) {
         tp = 1.0f;
-        return v3(grid_transmittance(load_grid(mp), o, d, dist, rng));
+        return v3(grid_transmittance(load_grid(mp), o, d, dist, rng, budget_hits));
     }
     return eval_medium_distance(med, false, dist, tp);
 }
@@ -229,6 +230,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
     const WaveParams& W = wave_of(c);
     const int lane = threadIdx.x & 31;
     uint32_t nan_paths = 0;
+    int budget_hits = 0;  // media walks that ran out of steps (reported as a watchdog error)
     // Sorted queue: item i lies in the bucket whose prefix range holds it.
     __shared__ int prefix[kShadeBuckets + 1];
     const bool sorted = B.sorted != nullptr;
@@ -394,7 +396,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                     const MedParams med = load_medium(mp);
                     float distance = 0.0f, trans_pdf = 0.0f;
                     v3 tr;
-                    scattered = medium_sample(mp, med, o, d, closest, distance, trans_pdf, tr, rng);
+                    scattered = medium_sample(mp, med, o, d, closest, distance, trans_pdf, tr, rng, budget_hits);
                     history *= (tr / trans_pdf);
                     mult_trans_pdf *= trans_pdf;
                     if (scattered) {
@@ -414,7 +416,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                             int tm;
                             if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
                                 float tp2, phase_pdf;
-                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng);
+                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng, budget_hits);
                                 v3 att = evaluate_phase(med, V, sd, phase_pdf);
                                 float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, phase_pdf * tp2);
                                 nee_l = w * (tr2 / tp2) * lr * att * history / lp;
@@ -478,7 +480,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                                 const DevMedium* mp = sc.media + medium_index;
                                 const MedParams med = load_medium(mp);
                                 float tp2;
-                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng);
+                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng, budget_hits);
                                 thh = tr2 / tp2;
                                 w = power_heuristic(lp, bpdf * tp2);
                             }
@@ -513,7 +515,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                                 const DevMedium* mp = sc.media + medium_index;
                                 const MedParams med = load_medium(mp);
                                 float tp2;
-                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng);
+                                v3 tr2 = medium_transmittance(mp, med, pos, sd, cl, tp2, rng, budget_hits);
                                 thh = tr2 / tp2;
                                 if (l.type != RT_LIGHT_POINT) w = power_heuristic(lp, bpdf * tp2);
                             }
@@ -605,6 +607,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
         }
     }
     if (Stats) warp_stat(&ctl->stats[7], nan_paths);
+    if (budget_hits) atomicAdd(&ctl->error, budget_hits);
 }
 
 // ------------------------------------------------------------------ shadow

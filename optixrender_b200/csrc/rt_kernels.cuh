@@ -55,7 +55,7 @@ struct WaveCtl {
     int fetch_ext;
     int fetch_shade;
     int fetch_shadow;
-    int error;
+    int error;  // media walks that exhausted their step budget in this render
     int pad;
     unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris,
                                   // NaN samples, paths ended by a NaN throughput

@@ -10,15 +10,15 @@
 // form `history *= transmittance / trans_pdf` with trans_pdf = 1:
 //   scattered:  transmittance = albedo
 //   passed:     transmittance = 1
-// Loops are bounded (kMaxTrackingSteps); a path that runs out ends with zero
-// weight.
+// Loops are bounded (kMaxTrackingSteps): a walk that runs out ends with zero
+// weight and adds one to `budget_hits`, which the renderer reports as
+// RT_ERR_DEVICE_WATCHDOG.
 #pragma once
 
 #include "rt_device.cuh"
 
 namespace rtd {
 
-constexpr int kMaxTrackingSteps = 4096;
 
 struct GridParams {
     v3 bmin, bmax;
@@ -136,7 +136,8 @@ RT_D void majorant_walk(const GridParams& g, v3 o, v3 d, float t0, float t1, F&&
 // Delta tracking inside [0, maxd): returns true with the collision distance
 // when a real collision happens.  `steps` counts tentative collisions.
 template <class RNG>
-RT_D bool grid_sample_distance(const GridParams& g, v3 o, v3 d, float maxd, RNG& rng, float& dist, v3& weight) {
+RT_D bool grid_sample_distance(const GridParams& g, v3 o, v3 d, float maxd, RNG& rng, float& dist, v3& weight,
+                                int& budget_hits) {
     weight = v3(1.0f);
     float t0, t1;
     if (!grid_clip(g, o, d, maxd, t0, t1) || g.sigma_t <= 0.0f) return false;
@@ -149,6 +150,7 @@ RT_D bool grid_sample_distance(const GridParams& g, v3 o, v3 d, float maxd, RNG&
         while (true) {
             if (++steps > kMaxTrackingSteps) {
                 weight = v3(0.0f);
+                budget_hits++;
                 return false;
             }
             t -= logf(1.0f - rng.next()) / smax;
@@ -167,7 +169,7 @@ RT_D bool grid_sample_distance(const GridParams& g, v3 o, v3 d, float maxd, RNG&
 
 // Ratio-tracking transmittance along [0, maxd).
 template <class RNG>
-RT_D float grid_transmittance(const GridParams& g, v3 o, v3 d, float maxd, RNG& rng) {
+RT_D float grid_transmittance(const GridParams& g, v3 o, v3 d, float maxd, RNG& rng, int& budget_hits) {
     float t0, t1;
     if (!grid_clip(g, o, d, maxd, t0, t1) || g.sigma_t <= 0.0f) return 1.0f;
     float T = 1.0f;
@@ -179,6 +181,7 @@ RT_D float grid_transmittance(const GridParams& g, v3 o, v3 d, float maxd, RNG& 
         while (true) {
             if (++steps > kMaxTrackingSteps) {
                 T = 0.0f;
+                budget_hits++;
                 return false;
             }
             t -= logf(1.0f - rng.next()) / smax;

@@ -3,6 +3,8 @@
 // Renderer::Render() (core/src/Renderer.cpp:635-793).
 #include <cuda_runtime.h>
 
+#include <cstddef>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -726,6 +728,16 @@ rt_status rt_renderer_guide_samples(rt_renderer* r, float* out, int64_t max_samp
 rt_status rt_renderer_synchronize(rt_renderer* r) {
     if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_synchronize: NULL renderer");
     RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_synchronize");
+    if (r->rendered && r->ctl.ptr) {  // the device-side step budget of media walks
+        int hits = 0;
+        RT_CUDA(cudaMemcpy(&hits, static_cast<char*>(r->ctl.ptr) + offsetof(WaveCtl, error), sizeof(int),
+                           cudaMemcpyDeviceToHost),
+                "rt_renderer_synchronize");
+        if (hits > 0)
+            return fail(RT_ERR_DEVICE_WATCHDOG,
+                        std::to_string(hits) + " medium walks of the last render ran out of their " +
+                            std::to_string(kMaxTrackingSteps) + "-step budget and were ended with zero weight");
+    }
     return RT_OK;
 }
 
@@ -790,6 +802,7 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     out->tris_tested = int64_t(ctl.stats[3] + ctl.stats[5]);
     out->nan_samples = int64_t(ctl.stats[6]);
     out->nan_throughput_paths = int64_t(ctl.stats[7]);
+    out->watchdog_walks = int64_t(ctl.error);
     out->waves = r->waves;
     out->launches = r->launches;
     out->extend_launches = r->extend_launches;

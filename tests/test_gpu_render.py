@@ -158,3 +158,31 @@ def test_media_independent_streams_mean_within_3se():
     se = d.std() / np.sqrt(d.size)
     print(f"media mean gpu {gpu.mean():.5f} cpu {cpu.mean():.5f} se {se:.2e}")
     assert abs(d.mean()) <= 3 * se
+
+
+@pytest.mark.gpu
+def test_medium_step_budget_is_reported_as_a_watchdog_error():
+    """A 128^3 grid whose 8^3 majorant cells each hold one dense voxel in
+    empty space: the majorant is that voxel's density everywhere, so a walk
+    through the medium takes ~10^5 tentative collisions (ratio tracking never
+    stops early).  The device's 4096-step budget ends those walks with zero
+    weight, and the host hears of it as RT_ERR_DEVICE_WATCHDOG from
+    synchronize (no hang, no fault); the next ordinary render reports
+    nothing."""
+    spec = scenes.media(32, 24, 2, grid_res=128, env_size=(64, 32))
+    grid = [md for md in spec.media if md["type"] == rt.MEDIUM_GRID][0]
+    dens = np.zeros((128, 128, 128), np.float32)
+    dens[8::16, 8::16, 8::16] = 1.0  # one voxel in each 16^3 block
+    grid["density"] = dens
+    grid["scale"] = 1e5
+    s, r = scenes.build_renderer(spec)
+    r.render()
+    with pytest.raises(rt.RTError) as e:
+        r.synchronize()
+    assert e.value.code == rt.RT_ERR_DEVICE_WATCHDOG
+    assert r.stats()["watchdog_walks"] > 0
+    assert np.isfinite(r.download_linear()).all()
+    s2, r2 = scenes.build_renderer(scenes.media(32, 24, 2, grid_res=16, env_size=(64, 32)))
+    r2.render()
+    r2.synchronize()
+    assert r2.stats()["watchdog_walks"] == 0
