@@ -13,7 +13,8 @@ First every request is submitted at once (saturation): aggregate Mpaths/s and
 the saturation job rate.  Then the same requests arrive as a Poisson stream at
 `load` x that rate, and time-to-image (submit -> final image in device memory,
 as the server's host clock observes it) is reported as p50/p99, both raw and
-as slowdown = time-to-image / (job paths / saturation Mpaths/s).
+as slowdown = time-to-image / (job paths / saturation Mpaths/s), and per
+quartile of job size.
 
     python -m optixrender_b200.serve_bench --requests 1000 --load 0.8
 """
@@ -127,6 +128,13 @@ def summarize(sts, reqs, sat_mpaths=None):
         slow = lat / service_ms
         out.update(slowdown_p50=float(np.percentile(slow, 50)), slowdown_p99=float(np.percentile(slow, 99)))
         out["slowdown_p99_over_p50"] = out["slowdown_p99"] / out["slowdown_p50"]
+    # latency within classes of similar job size (quartiles of paths per job)
+    edges = np.quantile(paths, [0.25, 0.5, 0.75])
+    cls = np.searchsorted(edges, paths, side="right")
+    out["by_size_quartile"] = [
+        {"paths_max": int(paths[cls == k].max()), "jobs": int((cls == k).sum()),
+         "p50_ms": float(np.percentile(lat[cls == k], 50)), "p99_ms": float(np.percentile(lat[cls == k], 99))}
+        for k in range(4) if (cls == k).any()]
     return out
 
 
