@@ -33,7 +33,7 @@ CU_SOURCES = ["rt_kernels.cu", "rt_trace_scratch.cu", "rt_guide.cu", "rt_guide_a
 CPP_SOURCES = ["rt_capi.cpp", "rt_renderer.cpp", "rt_bvh.cpp", "rt_tables.cpp", "rt_scene_io.cpp", "rt_server.cpp",
                "rt_png.cpp", "rt_jpeg.cpp"]
 HEADERS = ["rt_device.cuh", "rt_shading.cuh", "rt_traverse.cuh", "rt_kernels.cuh", "rt_internal.h", "rt_bvh.h",
-           "rt_media.cuh", "rt_guide.cuh", "rt_guide_host.h", "rt_image.h"]
+           "rt_media.cuh", "rt_guide.cuh", "rt_guide_host.h", "rt_image.h", "rt_schedule.h"]
 
 
 def _newer(out: Path, inputs) -> bool:

@@ -41,6 +41,10 @@
 
 #include "rt_guide_host.h"
 #include "rt_internal.h"
+#include "rt_schedule.h"
+
+static_assert(RT_SERVE_FAIR == rti::kPlanFair && RT_SERVE_FIFO == rti::kPlanFifo && RT_SERVE_SRPT == rti::kPlanSrpt,
+              "policy numbering");
 
 using namespace rtd;
 using namespace rti;
@@ -100,7 +104,7 @@ struct rt_server {
     std::vector<int64_t> running;  // admission order
     std::vector<int> free_slots;
     int64_t next_id = 1;
-    size_t rr = 0;  // round-robin position of the fair-share policy
+    PlanState plan;  // rotation state of the fair-share policy
     int64_t bytes_in_use = 0;
     // device state
     DevBuf job_table, ring, wave_index, ctl;
@@ -120,7 +124,6 @@ struct rt_server {
     rth::LaunchShape shape{};
     // stats
     int64_t waves = 0, paths = 0, done = 0, submitted = 0, depth_sum = 0, guided_waves = 0, training_waves = 0;
-    size_t pool_rr = 0;  // rotation over job groups (plain, guided per scene) of the fair policy
     int max_segments = 0;
     double busy_ms = 0.0;
     // background thread
@@ -419,80 +422,20 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
         return RT_OK;
     }
     account_busy(s);
-    // The group this wave serves: plain jobs (0) or the guided jobs of scene
-    // k (k + 1), chosen by the policy; then the paths each of its jobs gets.
+    // The group this wave serves and the paths each of its jobs gets
+    // (rt_schedule.h).
     std::vector<Job*> active;
+    std::vector<PlanJob> pj;
     for (int64_t id : s->running) {
         Job& j = *s->jobs[id];
-        if (j.issued < j.total) active.push_back(&j);
-    }
-    auto group = [](const Job* j) { return j->desc.guided ? j->desc.scene + 1 : 0; };
-    if (!active.empty()) {
-        int chosen = group(active.front());  // FIFO: the oldest job's group
-        if (s->opt.policy == RT_SERVE_SRPT) {
-            const Job* best = active.front();
-            for (const Job* j : active)
-                if (j->total - j->issued < best->total - best->issued) best = j;
-            chosen = group(best);
-        } else if (s->opt.policy == RT_SERVE_FAIR) {
-            // the first group at or after the rotation point that has work
-            int best = -1, first = -1;
-            for (const Job* j : active) {
-                const int gid = group(j);
-                if (first < 0 || gid < first) first = gid;
-                if (gid >= int(s->pool_rr) && (best < 0 || gid < best)) best = gid;
-            }
-            chosen = best >= 0 ? best : first;
-            s->pool_rr = size_t(chosen) + 1;
+        if (j.issued < j.total) {
+            active.push_back(&j);
+            pj.push_back({j.total - j.issued, j.desc.guided ? j.desc.scene + 1 : 0});
         }
-        active.erase(std::remove_if(active.begin(), active.end(),
-                                    [&](const Job* j) { return group(j) != chosen; }),
-                     active.end());
     }
     std::vector<std::pair<Job*, int64_t>> plan;
-    if (!active.empty()) {
-        if (s->opt.policy == RT_SERVE_FIFO || s->opt.policy == RT_SERVE_SRPT) {
-            if (s->opt.policy == RT_SERVE_SRPT)  // fewest paths left first, ties by admission
-                std::stable_sort(active.begin(), active.end(), [](const Job* a, const Job* b) {
-                    return a->total - a->issued < b->total - b->issued;
-                });
-            int64_t left = s->capacity;
-            for (Job* j : active) {
-                if (left == 0 || int(plan.size()) == kMaxSegments) break;
-                int64_t take = std::min(j->total - j->issued, left);
-                plan.emplace_back(j, take);
-                left -= take;
-            }
-        } else {
-            // Fair share: up to kMaxSegments jobs, taken round-robin, split the
-            // wave evenly; a job that needs less than its share gives the rest
-            // to the others (water filling).
-            const size_t k = std::min(active.size(), size_t(kMaxSegments));
-            const size_t start = s->rr % active.size();
-            std::vector<Job*> chosen;
-            for (size_t i = 0; i < k; i++) chosen.push_back(active[(start + i) % active.size()]);
-            s->rr = start + k;
-            std::vector<size_t> order(k);
-            for (size_t i = 0; i < k; i++) order[i] = i;
-            std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-                return chosen[a]->total - chosen[a]->issued < chosen[b]->total - chosen[b]->issued;
-            });
-            std::vector<int64_t> give(k, 0);
-            int64_t left = s->capacity;
-            for (size_t n = 0; n < k; n++) {
-                size_t i = order[n];
-                give[i] = std::min(chosen[i]->total - chosen[i]->issued, left / int64_t(k - n));
-                left -= give[i];
-            }
-            for (size_t i = 0; i < k && left > 0; i++) {  // remainder of the integer split
-                int64_t extra = std::min(left, chosen[i]->total - chosen[i]->issued - give[i]);
-                give[i] += extra;
-                left -= extra;
-            }
-            for (size_t i = 0; i < k; i++)
-                if (give[i] > 0) plan.emplace_back(chosen[i], give[i]);
-        }
-    }
+    for (const auto& seg : plan_wave(pj, s->opt.policy, s->capacity, kMaxSegments, s->plan))
+        plan.emplace_back(active[seg.first], seg.second);
     WaveParams wp;
     std::memset(&wp, 0, sizeof(wp));
     int filled = 0, depth = 1;
