@@ -208,7 +208,8 @@ bool read_jpeg(const std::string& file, std::vector<uint8_t>& rgba, int& w, int&
             h = be16(s + 1);
             w = be16(s + 3);
             const int nc = s[5];
-            if (w <= 0 || h <= 0 || (nc != 1 && nc != 3) || sl < size_t(6 + 3 * nc)) {
+            if (w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28) || (nc != 1 && nc != 3) ||
+                sl < size_t(6 + 3 * nc)) {
                 err = "bad frame header";
                 return false;
             }

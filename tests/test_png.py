@@ -160,3 +160,46 @@ def test_png_errors(tmp_path, img):
     for data in (bytes(bad_crc), good[:60], _png(rows, w, h, 8, 6, 4, interlace=1)):
         with pytest.raises(rt.RTError):
             _load(tmp_path, data)
+
+
+def test_corrupted_files_fail_cleanly(tmp_path, img):
+    """Random byte flips in the compressed data of PNG and JPEG files (CRCs
+    recomputed so the PNG damage reaches the inflater) end in an error or a
+    decoded image, never in a crash."""
+    h, w = img.shape[:2]
+    rows = [r.tobytes() for r in _top_first(img)]
+    png = bytearray(_png(rows, w, h, 8, 6, 4))
+    rng = np.random.default_rng(11)
+    start = png.index(b"IDAT") + 4
+    for k in range(200):
+        bad = bytearray(png)
+        for _ in range(int(rng.integers(1, 6))):
+            bad[int(rng.integers(start, len(bad) - 12))] = int(rng.integers(0, 256))
+        # recompute the CRC of every chunk
+        pos = 8
+        while pos + 12 <= len(bad):
+            n = struct.unpack(">I", bad[pos:pos + 4])[0]
+            if pos + 12 + n > len(bad):
+                break
+            bad[pos + 8 + n:pos + 12 + n] = struct.pack(">I", zlib.crc32(bytes(bad[pos + 4:pos + 8 + n])) & 0xFFFFFFFF)
+            pos += 12 + n
+        try:
+            _load(tmp_path, bytes(bad), f"f{k}.png")
+        except rt.RTError:
+            pass
+    try:
+        from PIL import Image
+    except ImportError:
+        return
+    import io
+    b = io.BytesIO()
+    Image.fromarray(img[..., :3]).save(b, "JPEG", quality=80)
+    jpg = bytearray(b.getvalue())
+    for k in range(200):
+        bad = bytearray(jpg)
+        for _ in range(int(rng.integers(1, 6))):
+            bad[int(rng.integers(2, len(bad)))] = int(rng.integers(0, 256))
+        try:
+            _load(tmp_path, bytes(bad), f"f{k}.jpg")
+        except rt.RTError:
+            pass
