@@ -12,6 +12,7 @@
 // per block, and the hash-grid gradient is scattered with float2 atomics.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "rt_guide.cuh"
@@ -99,32 +100,19 @@ RT_D void pack_masked(const float (&d)[N / 8][4], const uint32_t (&h)[N / 16][4]
     }
 }
 
-// Weight gradient dW [M][N] += E^T X for deltas E (16 rows x M, A fragments)
-// and inputs X (16 rows x N, A fragments), added into shared memory.
-template <int M, int N>
-RT_D void weight_grad(const uint32_t (&e)[M / 16][4], const uint32_t (&x)[N / 16][4], float* gW) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-    uint32_t bt[N / 8][2];
+// Training stores, per 16-sample tile, the fragments the weight gradients
+// need, word-major ([word][lane], so every store and load is one 128-byte
+// line): output delta (2 x 4 words), then the input and delta of each hidden
+// layer, then the encoded input.  k_guide_wgrad forms dW_l = E^T X from them.
+constexpr int kFragAdo = 0, kFragH3 = 8, kFragE3 = 24, kFragH2 = 40, kFragE2 = 56, kFragH1 = 72, kFragE1 = 88,
+              kFragAx = 104, kFragWords = 112;
+
+template <int T>
+RT_D void frag_store(uint32_t* tile_frags, int off, const uint32_t (&f)[T][4], int lane) {
 #pragma unroll
-    for (int j = 0; j < N / 8; j++) {
-        const int t = j >> 1, hi = j & 1;
-        bt[j][0] = trans8x8(x[t][hi ? 2 : 0]);
-        bt[j][1] = trans8x8(x[t][hi ? 3 : 1]);
-    }
+    for (int t = 0; t < T; t++)
 #pragma unroll
-    for (int mt = 0; mt < M / 16; mt++) {
-        uint32_t at[4] = {trans8x8(e[mt][0]), trans8x8(e[mt][2]), trans8x8(e[mt][1]), trans8x8(e[mt][3])};
-#pragma unroll
-        for (int j = 0; j < N / 8; j++) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-            mma16816(d, at, bt[j][0], bt[j][1]);
-            float* p = gW + (16 * mt + g) * N + 8 * j + 2 * tig;
-            atomicAdd(p, d[0]);
-            atomicAdd(p + 1, d[1]);
-            atomicAdd(p + 8 * N, d[2]);
-            atomicAdd(p + 8 * N + 1, d[3]);
-        }
-    }
+        for (int r = 0; r < 4; r++) tile_frags[(off + 4 * t + r) * 32 + lane] = f[t][r];
 }
 
 struct Corners {
@@ -323,7 +311,7 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
                                                            const float* __restrict__ weight, int n, float scale,
                                                            const float* __restrict__ weight_sum,
                                                            float* __restrict__ grad_table,
-                                                           float* __restrict__ grad_mlp, float* __restrict__ loss) {
+                                                           uint32_t* __restrict__ frags, float* __restrict__ loss) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (weight_sum) {  // scale = 1 / (sum of the batch's weights), computed on the device
         const float ws = *weight_sum;
@@ -331,10 +319,8 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
     }
     __half* sw = reinterpret_cast<__half*>(smem);
     __half* sb = sw + kFwdHalves;
-    float* gW = reinterpret_cast<float*>(smem + (kFwdHalves + kBwdHalves) * sizeof(__half));
-    float* tiles = gW + kMlpParams;
+    float* tiles = reinterpret_cast<float*>(smem + (kFwdHalves + kBwdHalves) * sizeof(__half));
     load_weights(net.mlp, sw, sb);
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) gW[i] = 0.f;
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
     float* tile = tiles + warp * 16 * kTileStride;
@@ -379,17 +365,22 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
             ado[t][3] = pack_h2(p[8 * kTileStride + 8], p[8 * kTileStride + 9]);
         }
         __syncwarp();
+        uint32_t* tf = frags + size_t(tt) * kFragWords * 32;
+        frag_store<2>(tf, kFragAdo, ado, lane);
+        frag_store<4>(tf, kFragH3, h3, lane);
+        frag_store<4>(tf, kFragH2, h2, lane);
+        frag_store<4>(tf, kFragH1, h1, lane);
+        frag_store<2>(tf, kFragAx, ax, lane);
         uint32_t e[4][4];
-        weight_grad<kOut, kHid>(ado, h3, gW + kW0 + kW1 + kW2);
         layer<kOut, kHid, kS32>(ado, sb + kOffT3, d64);
         pack_masked<kHid>(d64, h3, e);
-        weight_grad<kHid, kHid>(e, h2, gW + kW0 + kW1);
+        frag_store<4>(tf, kFragE3, e, lane);
         layer<kHid, kHid, kS64>(e, sb + kOffT2, d64);
         pack_masked<kHid>(d64, h2, e);
-        weight_grad<kHid, kHid>(e, h1, gW + kW0);
+        frag_store<4>(tf, kFragE2, e, lane);
         layer<kHid, kHid, kS64>(e, sb + kOffT1, d64);
         pack_masked<kHid>(d64, h1, e);
-        weight_grad<kHid, kIn>(e, ax, gW);
+        frag_store<4>(tf, kFragE1, e, lane);
         float dx[4][4];
         layer<kHid, kIn, kS64>(e, sb + kOffT0, dx);
         // hash-grid gradient: this thread's levels 4j + tig for rows g (dx[j][0..1]) and g + 8 (dx[j][2..3])
@@ -408,12 +399,63 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
             }
         }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
-        if (gW[i] != 0.f) atomicAdd(grad_mlp + i, gW[i]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
     if (lane == 0 && lsum != 0.f) atomicAdd(loss, lsum);
+}
+
+// Weight gradients dW_l[M][N] += E^T X from the fragments of `tiles` tiles.
+// Warp w of a block plays role w: a 16-row block of one layer's outputs
+// (layer 3: 2 blocks, layers 2, 1, 0: 4 each), whose 16 x N gradient stays in
+// registers across the block's chunk of tiles and is added to global memory
+// once.  The 14 warps of a block read the same tiles, so those loads hit L1.
+constexpr int kWgradRoles = 14;
+template <int M, int N>
+RT_D void wgrad_role(const uint32_t* __restrict__ frags, int t0, int t1, int offE, int offX, int mt, float* gW) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    float acc[N / 8][4];
+#pragma unroll
+    for (int j = 0; j < N / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    for (int tt = t0; tt < t1; tt++) {
+        const uint32_t* tf = frags + size_t(tt) * kFragWords * 32 + lane;
+        uint32_t x[N / 16][4];
+#pragma unroll
+        for (int t = 0; t < N / 16; t++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) x[t][r] = __ldg(tf + (offX + 4 * t + r) * 32);
+        uint32_t e4[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) e4[r] = __ldg(tf + (offE + 4 * mt + r) * 32);
+        const uint32_t at[4] = {trans8x8(e4[0]), trans8x8(e4[2]), trans8x8(e4[1]), trans8x8(e4[3])};
+#pragma unroll
+        for (int j = 0; j < N / 8; j++) {
+            const int t = j >> 1, hi = j & 1;
+            mma16816(acc[j], at, trans8x8(x[t][hi ? 2 : 0]), trans8x8(x[t][hi ? 3 : 1]));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < N / 8; j++) {
+        float* p = gW + (16 * mt + g) * N + 8 * j + 2 * tig;
+        if (acc[j][0] != 0.f) atomicAdd(p, acc[j][0]);
+        if (acc[j][1] != 0.f) atomicAdd(p + 1, acc[j][1]);
+        if (acc[j][2] != 0.f) atomicAdd(p + 8 * N, acc[j][2]);
+        if (acc[j][3] != 0.f) atomicAdd(p + 8 * N + 1, acc[j][3]);
+    }
+}
+
+__global__ void __launch_bounds__(kWgradRoles * 32) k_guide_wgrad(const uint32_t* __restrict__ frags, int tiles,
+                                                                  int chunk, float* __restrict__ grad_mlp) {
+    const int role = threadIdx.x >> 5;
+    const int t0 = blockIdx.x * chunk, t1 = min(tiles, t0 + chunk);
+    if (t0 >= t1) return;
+    if (role < 2)
+        wgrad_role<kOut, kHid>(frags, t0, t1, kFragAdo, kFragH3, role, grad_mlp + kW0 + kW1 + kW2);
+    else if (role < 6)
+        wgrad_role<kHid, kHid>(frags, t0, t1, kFragE3, kFragH2, role - 2, grad_mlp + kW0 + kW1);
+    else if (role < 10)
+        wgrad_role<kHid, kHid>(frags, t0, t1, kFragE2, kFragH1, role - 6, grad_mlp + kW0);
+    else
+        wgrad_role<kHid, kIn>(frags, t0, t1, kFragE1, kFragAx, role - 10, grad_mlp);
 }
 
 // ------------------------------------------------------------------ renderer side
@@ -634,8 +676,7 @@ static size_t infer_smem() {
     return size_t(rtg::kFwdHalves) * 2 + size_t(rtg::kInferWarps) * 16 * rtg::kTileStride * 4;
 }
 size_t backward_smem() {
-    return size_t(rtg::kFwdHalves + rtg::kBwdHalves) * 2 + size_t(rtg::kMlpParams) * 4 +
-           size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4;
+    return size_t(rtg::kFwdHalves + rtg::kBwdHalves) * 2 + size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4;
 }
 
 cudaError_t prepare_kernels() {
@@ -660,17 +701,25 @@ void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, 
     rtg::k_guide_forward<<<grid_for_tiles(n, sms), rtg::kBlock, forward_smem(), st>>>(net, pos, n, mode, raw, mix);
 }
 
+size_t frag_bytes_per_tile() { return size_t(rtg::kFragWords) * 32 * 4; }
+
 void launch_backward(const rtg::NetView& net, const float* pos, const float* dir, const float* weight, int n,
-                     float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss, int sms,
-                     cudaStream_t st) {
-    if (n <= 0) return;
-    const int tiles = (n + 15) / 16;
-    int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
-    // 2 blocks per SM: the shared weights, transposes and gradient (~105 KB
-    // per block) allow no more
-    if (blocks > sms * 2) blocks = sms * 2;
-    rtg::k_guide_backward<<<blocks, rtg::kBlock, backward_smem(), st>>>(net, pos, dir, weight, n, scale, weight_sum,
-                                                                        grad_table, grad_mlp, loss);
+                     float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss,
+                     uint32_t* frags, int frag_tiles, int sms, cudaStream_t st) {
+    // chunks of at most frag_tiles tiles: the fused pass stores their
+    // fragments, then k_guide_wgrad turns them into weight gradients
+    for (int begin = 0; begin < n; begin += frag_tiles * 16) {
+        const int m = std::min(n - begin, frag_tiles * 16);
+        const int tiles = (m + 15) / 16;
+        int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
+        if (blocks > sms * 3) blocks = sms * 3;  // shared weights and transposes, ~64 KB per block
+        rtg::k_guide_backward<<<blocks, rtg::kBlock, backward_smem(), st>>>(
+            net, pos + size_t(begin) * 3, dir + size_t(begin) * 3, weight + begin, m, scale, weight_sum, grad_table,
+            frags, loss);
+        const int chunk = std::max(4, (tiles + 2 * sms - 1) / (2 * sms));
+        rtg::k_guide_wgrad<<<(tiles + chunk - 1) / chunk, rtg::kWgradRoles * 32, 0, st>>>(frags, tiles, chunk,
+                                                                                          grad_mlp);
+    }
 }
 
 void launch_infer(const rtd::Ctx& c, const rtg::NetView& net, int sms, cudaStream_t st) {

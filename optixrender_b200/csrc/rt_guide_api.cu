@@ -30,6 +30,7 @@ struct rt_guide {
     cudaStream_t stream = nullptr;
     rt_guide_options opt{};
     DevBuf table, table16, mlp, mlp16, gtable, gmlp, mt, vt, mm, vm, loss;
+    DevBuf frags;  // training fragments of up to kFragTiles tiles, allocated at the first training pass
     int step = 0;
     int res[rtg::kLevels];
 };
@@ -49,6 +50,16 @@ uint64_t splitmix(uint64_t& s) {
     return z ^ (z >> 31);
 }
 float uniform(uint64_t& s) { return float(splitmix(s) >> 40) * (1.0f / 16777216.0f); }
+
+// Training passes run in chunks of up to 2^18 samples (16,384 tiles, 235 MB
+// of fragments).
+constexpr int kFragTiles = 1 << 14;
+
+rt_status ensure_frags(rt_guide* g) {
+    if (g->frags.ptr) return RT_OK;
+    GD_CUDA(g->frags.alloc(size_t(kFragTiles) * rtgh::frag_bytes_per_tile()), "allocate training fragments");
+    return RT_OK;
+}
 
 rtg::NetView view(const rt_guide* g) {
     rtg::NetView v;
@@ -150,9 +161,11 @@ rtg::NetView guide_view(const rt_guide* g, float3 lo, float3 inv_ext) {
 // one Adam step, all on `st`.
 rt_status guide_train_device(rt_guide* g, const float* pos, const float* dir, const float* weight, int n, float scale,
                              const float* weight_sum, cudaStream_t st) {
+    rt_status fs = ensure_frags(g);
+    if (fs) return fs;
     GD_CUDA(cudaMemsetAsync(g->loss.ptr, 0, 4, st), "guide training step");
     rtgh::launch_backward(view(g), pos, dir, weight, n, scale, weight_sum, g->gtable.as<float>(), g->gmlp.as<float>(),
-                          g->loss.as<float>(), g->sms, st);
+                          g->loss.as<float>(), g->frags.as<uint32_t>(), kFragTiles, g->sms, st);
     g->step++;
     rtgh::launch_adam(g->table.as<float>(), g->table16.as<__half>(), g->gtable.as<float>(), g->mt.as<float>(),
                       g->vt.as<float>(), rtg::kTableParams, g->opt.learning_rate, g->step, st);
@@ -163,6 +176,15 @@ rt_status guide_train_device(rt_guide* g, const float* pos, const float* dir, co
 }
 
 int guide_sms(const rt_guide* g) { return g->sms; }
+
+int64_t guide_device_bytes(const rt_guide* g) {
+    const DevBuf* bufs[] = {&g->table, &g->table16, &g->mlp, &g->mlp16, &g->gtable, &g->gmlp,
+                            &g->mt, &g->vt, &g->mm, &g->vm, &g->loss, &g->frags};
+    int64_t b = 0;
+    for (const DevBuf* d : bufs) b += int64_t(d->bytes);
+    if (!g->frags.ptr) b += int64_t(kFragTiles) * int64_t(rtgh::frag_bytes_per_tile());  // allocated at the first training pass
+    return b;
+}
 
 }  // namespace rti
 
@@ -244,8 +266,11 @@ rt_status rt_guide_gradients(rt_guide* g, const float* pos, const float* dir, co
     GD_CUDA(cudaMemsetAsync(g->gtable.ptr, 0, g->gtable.bytes, g->stream), "rt_guide_gradients");
     GD_CUDA(cudaMemsetAsync(g->gmlp.ptr, 0, g->gmlp.bytes, g->stream), "rt_guide_gradients");
     GD_CUDA(cudaMemsetAsync(g->loss.ptr, 0, 4, g->stream), "rt_guide_gradients");
+    st = ensure_frags(g);
+    if (st) return st;
     rtgh::launch_backward(view(g), dp.as<float>(), dd.as<float>(), dw.as<float>(), int(n), 1.0f / float(n), nullptr,
-                          g->gtable.as<float>(), g->gmlp.as<float>(), g->loss.as<float>(), g->sms, g->stream);
+                          g->gtable.as<float>(), g->gmlp.as<float>(), g->loss.as<float>(), g->frags.as<uint32_t>(),
+                          kFragTiles, g->sms, g->stream);
     GD_CUDA(cudaGetLastError(), "rt_guide_gradients");
     if (loss) GD_CUDA(cudaMemcpyAsync(loss, g->loss.ptr, 4, cudaMemcpyDeviceToHost, g->stream), "rt_guide_gradients");
     if (grad_table)

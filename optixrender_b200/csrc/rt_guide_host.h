@@ -15,9 +15,12 @@ cudaError_t prepare_kernels();
 void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, float* raw, rtg::Mixture* mix, int sms,
                     cudaStream_t st);
 // `weight_sum` (device, may be null) replaces `scale` by 1 / *weight_sum.
+// Bytes of training fragments per 16-sample tile (the scratch `frags` of
+// launch_backward holds frag_tiles tiles).
+size_t frag_bytes_per_tile();
 void launch_backward(const rtg::NetView& net, const float* pos, const float* dir, const float* weight, int n,
-                     float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss, int sms,
-                     cudaStream_t st);
+                     float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss,
+                     uint32_t* frags, int frag_tiles, int sms, cudaStream_t st);
 // Renderer side: mixtures of a bounce's guided vertices, training samples of
 // a wave, random training batches.
 void launch_infer(const rtd::Ctx& c, const rtg::NetView& net, int sms, cudaStream_t st);
@@ -43,4 +46,6 @@ rtg::NetView guide_view(const rt_guide* g, float3 lo, float3 inv_ext);
 rt_status guide_train_device(rt_guide* g, const float* pos, const float* dir, const float* weight, int n, float scale,
                              const float* weight_sum, cudaStream_t st);
 int guide_sms(const rt_guide* g);
+// Device memory of the network, its optimiser state and its training scratch.
+int64_t guide_device_bytes(const rt_guide* g);
 }  // namespace rti

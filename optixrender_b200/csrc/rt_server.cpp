@@ -218,7 +218,9 @@ rt_status ensure_scene_guide(rt_server* s, int k) {
     rt_guide_options go;
     rt_guide_options_default(&go);
     go.seed = uint64_t(k) + 1;
-    return guide_create(&go, &g.net);
+    rt_status st = guide_create(&go, &g.net);
+    if (!st) s->guide_bytes += guide_device_bytes(g.net);  // counted against the budget from now on
+    return st;
 }
 
 // `gscene` >= 0: the wave samples the guiding network of that scene.
