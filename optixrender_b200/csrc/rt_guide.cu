@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kWarps = 4;
 constexpr int kBlock = kWarps * 32;
+constexpr int kBwdWarps = 8;  // training pass: 2 blocks of 8 warps per SM (registers, shared weights)
 // padded shared-memory rows (halves)
 constexpr int kS32 = kIn + 8;   // rows of 32 inputs
 constexpr int kS64 = kHid + 8;  // rows of 64 inputs
@@ -57,18 +58,33 @@ RT_D uint32_t trans8x8(uint32_t x) {
     return y;
 }
 
-// d[j] = A (16 x K) * W^T (K x N) for the weight W [N][K] in shared memory, row stride S.
+// Two 8x8 FP16 matrices from shared memory in mma fragment order: lane i
+// (and i + 8) gives the address of row i & 7 of matrix (i >> 3) & 1; register
+// m receives matrix m's fragment (row g, columns 2 tig and 2 tig + 1 for
+// lane 4 g + tig).
+RT_D void ldsm_x2(const __half* p, uint32_t& r0, uint32_t& r1) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+
+// d[j] = A (16 x K) * W^T (K x N) for the weight W [N][K] in shared memory,
+// row stride S halves (a multiple of 8, so every row starts on 16 bytes).
+// One ldmatrix.x2 brings the B fragments of output block j for one mma
+// k-step: matrix 0 holds rows 8j..8j+7, columns 16t..16t+7, matrix 1 the
+// next 8 columns.  (The x4 form would halve the loads again but makes the
+// compiler hoist twice the registers.)
 template <int K, int N, int S>
 RT_D void layer(const uint32_t (&a)[K / 16][4], const __half* W, float (&d)[N / 8][4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    static_assert(K % 16 == 0 && S % 8 == 0, "ldmatrix layout");
+    const int lane = threadIdx.x & 31;
+    const __half* base = W + (lane & 7) * S + 8 * ((lane >> 3) & 1);
 #pragma unroll
     for (int j = 0; j < N / 8; j++) {
         d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.0f;
-        const __half* row = W + (8 * j + g) * S + 2 * tig;
 #pragma unroll
         for (int t = 0; t < K / 16; t++) {
-            uint32_t b0 = *reinterpret_cast<const uint32_t*>(row + 16 * t);
-            uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + 16 * t + 8);
+            uint32_t b0, b1;
+            ldsm_x2(base + 8 * j * S + 16 * t, b0, b1);
             mma16816(d[j], a[t], b0, b1);
         }
     }
@@ -86,33 +102,62 @@ RT_D void pack_relu(const float (&d)[N / 8][4], uint32_t (&a)[N / 16][4]) {
     }
 }
 
-// Deltas masked by the ReLU of the forward activations `h` (A fragments), packed to A fragments.
+// ReLU mask of N / 16 A fragments: bit 8t + 2r + i is set where half i of
+// word a[t][r] is positive (32 bits for a 64-wide layer).
 template <int N>
-RT_D void pack_masked(const float (&d)[N / 8][4], const uint32_t (&h)[N / 16][4], uint32_t (&a)[N / 16][4]) {
+RT_D uint32_t relu_mask(const uint32_t (&h)[N / 16][4]) {
+    static_assert(N / 16 * 8 <= 32, "mask wider than a word");
+    uint32_t m = 0;
+#pragma unroll
+    for (int t = 0; t < N / 16; t++)
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const float2 hv = unpack_h2(h[t][r]);
+            m |= (hv.x > 0.f ? 1u : 0u) << (8 * t + 2 * r);
+            m |= (hv.y > 0.f ? 1u : 0u) << (8 * t + 2 * r + 1);
+        }
+    return m;
+}
+
+// Deltas masked by the ReLU of the forward activations (relu_mask bits), packed to A fragments.
+template <int N>
+RT_D void pack_masked(const float (&d)[N / 8][4], uint32_t mask, uint32_t (&a)[N / 16][4]) {
 #pragma unroll
     for (int t = 0; t < N / 16; t++) {
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const float* src = d[2 * t + (r >> 1)] + 2 * (r & 1);
-            float2 hv = unpack_h2(h[t][r]);
-            a[t][r] = pack_h2(hv.x > 0.f ? src[0] : 0.f, hv.y > 0.f ? src[1] : 0.f);
+            const int b = 8 * t + 2 * r;
+            a[t][r] = pack_h2((mask >> b) & 1u ? src[0] : 0.f, (mask >> (b + 1)) & 1u ? src[1] : 0.f);
         }
     }
 }
 
 // Training stores, per 16-sample tile, the fragments the weight gradients
-// need, word-major ([word][lane], so every store and load is one 128-byte
-// line): output delta (2 x 4 words), then the input and delta of each hidden
-// layer, then the encoded input.  k_guide_wgrad forms dW_l = E^T X from them.
+// need: output delta (2 x 4 words), then the input and delta of each hidden
+// layer, then the encoded input.  Word w of lane l sits at
+// [w / 4][l][w % 4], so one A fragment (4 words) is one 16-byte store or
+// load per lane and 512 contiguous bytes per warp.  k_guide_wgrad forms
+// dW_l = E^T X from them.
 constexpr int kFragAdo = 0, kFragH3 = 8, kFragE3 = 24, kFragH2 = 40, kFragE2 = 56, kFragH1 = 72, kFragE1 = 88,
               kFragAx = 104, kFragWords = 112;
+static_assert(kFragH3 % 4 == 0 && kFragE3 % 4 == 0 && kFragH2 % 4 == 0 && kFragE2 % 4 == 0 && kFragH1 % 4 == 0 &&
+                  kFragE1 % 4 == 0 && kFragAx % 4 == 0 && kFragWords % 4 == 0,
+              "fragments start on 16-byte boundaries");
 
 template <int T>
 RT_D void frag_store(uint32_t* tile_frags, int off, const uint32_t (&f)[T][4], int lane) {
+    uint4* q = reinterpret_cast<uint4*>(tile_frags) + (off / 4) * 32 + lane;
 #pragma unroll
-    for (int t = 0; t < T; t++)
-#pragma unroll
-        for (int r = 0; r < 4; r++) tile_frags[(off + 4 * t + r) * 32 + lane] = f[t][r];
+    for (int t = 0; t < T; t++) q[32 * t] = make_uint4(f[t][0], f[t][1], f[t][2], f[t][3]);
+}
+
+RT_D void frag_load(const uint32_t* tile_frags, int off, int lane, uint32_t (&f)[4]) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(tile_frags) + (off / 4) * 32 + lane);
+    f[0] = v.x;
+    f[1] = v.y;
+    f[2] = v.z;
+    f[3] = v.w;
 }
 
 struct Corners {
@@ -120,8 +165,15 @@ struct Corners {
     float w[8];
 };
 
-RT_D void level_corners(const int* res_table, int l, float3 x, Corners& c) {
-    const int res = res_table[l];
+// net.res[base + q], q = 0..3 a runtime lane index and base a constant
+// after unrolling: selecting among four constant indices keeps the
+// parameter array out of local memory (a runtime index into a kernel
+// parameter array makes the compiler copy it there).
+RT_D int level_res(const NetView& net, int base, int q) {
+    return q == 0 ? net.res[base] : q == 1 ? net.res[base + 1] : q == 2 ? net.res[base + 2] : net.res[base + 3];
+}
+
+RT_D void level_corners(int res, float3 x, Corners& c) {
     const float fr = float(res);
     float px = x.x * fr, py = x.y * fr, pz = x.z * fr;
     float cx = fminf(floorf(px), fr - 1.0f), cy = fminf(floorf(py), fr - 1.0f), cz = fminf(floorf(pz), fr - 1.0f);
@@ -137,9 +189,9 @@ RT_D void level_corners(const int* res_table, int l, float3 x, Corners& c) {
     }
 }
 
-RT_D uint32_t encode_level(const __half2* __restrict__ table, const int* res, int l, float3 x) {
+RT_D uint32_t encode_level(const __half2* __restrict__ table, int res, int l, float3 x) {
     Corners c;
-    level_corners(res, l, x, c);
+    level_corners(res, x, c);
     const __half2* t = table + size_t(l) * kT;
     float f0 = 0.f, f1 = 0.f;
 #pragma unroll
@@ -158,10 +210,11 @@ RT_D void encode_tile(const NetView& net, float3 xg, float3 xg8, bool vg, bool v
 #pragma unroll
     for (int t = 0; t < 2; t++) {
         const int l0 = 8 * t + tig, l1 = 8 * t + 4 + tig;
-        a[t][0] = vg ? encode_level(net.table, net.res, l0, xg) : 0u;
-        a[t][1] = vg8 ? encode_level(net.table, net.res, l0, xg8) : 0u;
-        a[t][2] = vg ? encode_level(net.table, net.res, l1, xg) : 0u;
-        a[t][3] = vg8 ? encode_level(net.table, net.res, l1, xg8) : 0u;
+        const int r0 = level_res(net, 8 * t, tig), r1 = level_res(net, 8 * t + 4, tig);
+        a[t][0] = vg ? encode_level(net.table, r0, l0, xg) : 0u;
+        a[t][1] = vg8 ? encode_level(net.table, r0, l0, xg8) : 0u;
+        a[t][2] = vg ? encode_level(net.table, r1, l1, xg) : 0u;
+        a[t][3] = vg8 ? encode_level(net.table, r1, l1, xg8) : 0u;
     }
 }
 
@@ -257,56 +310,85 @@ __global__ void __launch_bounds__(kBlock) k_guide_forward(NetView net, const flo
     }
 }
 
-// Loss gradient of one row with respect to its 32 raw outputs (in place),
-// for -s * log q(d); returns the row's loss term.
-RT_D float loss_grad_row(float* o, float3 d, float s, float kappa_hi) {
-    float w[kLobes], kap[kLobes], dens[kLobes];
-    float3 mu[kLobes], dth[kLobes], dph[kLobes];
-    float st[kLobes], sp[kLobes];
-    bool inr[kLobes];
+// One vMF lobe of a row's raw outputs o4 = (weight logit, log kappa, theta
+// and phi logits), evaluated at the unit direction d: everything the loss and
+// its gradient need except the mixture weight.  The angles lie in [0, 2 pi],
+// where the fast sine / cosine / exponential intrinsics are accurate to a
+// few ulp - far inside the FP16 rounding of the network around them.
+struct LobeTerms {
+    float kap, st, sp;   // concentration, sigmoid(theta logit), sigmoid(phi logit)
+    float c;             // cos(mean direction, d)
+    float dens;          // vMF density at d
+    float dth_d, dph_d;  // d . d(mean)/d(theta), d . d(mean)/d(phi)
+    bool inr;            // log kappa inside [kKappaLo, kappa_hi] (gradient passes the clamp)
+};
+
+RT_D LobeTerms lobe_terms(float kr, float tl, float pl, float3 d, float kappa_hi) {
+    LobeTerms t;
+    t.inr = kr >= kKappaLo && kr <= kappa_hi;
+    t.kap = __expf(fminf(fmaxf(kr, kKappaLo), kappa_hi));
+    t.st = 1.f / (1.f + __expf(-tl));
+    t.sp = 1.f / (1.f + __expf(-pl));
+    float s_t, c_t, s_p, c_p;
+    __sincosf(3.14159265358979f * t.st, &s_t, &c_t);
+    __sincosf(6.28318530717959f * t.sp, &s_p, &c_p);
+    t.c = s_t * c_p * d.x + s_t * s_p * d.y + c_t * d.z;
+    t.dth_d = c_t * c_p * d.x + c_t * s_p * d.y - s_t * d.z;
+    t.dph_d = -s_t * s_p * d.x + s_t * c_p * d.y;
+    t.dens = t.kap / (6.28318530717959f * -expm1f(-2.f * t.kap)) * __expf(t.kap * (t.c - 1.f));
+    return t;
+}
+
+// Loss gradient of a warp's 16-row output tile (staged in shared memory,
+// row stride kTileStride), in place: for row r the loss is -s_r log q(d_r)
+// with s_r = weight[r] * scale, and the 32 raw outputs are replaced by its
+// gradient.  Lane 2i + h takes row i's lobes 4h..4h+3; the two lanes of a
+// row combine the softmax and mixture sums with one shuffle each, so all 32
+// lanes work and every lobe is evaluated once.  Rows at or past n get zero
+// gradients.  Returns this lane's share of the tile's loss.
+RT_D float loss_grad_tile(float* tile, int row0, int n, const float* __restrict__ dir,
+                          const float* __restrict__ weight, float scale, float kappa_hi) {
+    const int lane = threadIdx.x & 31, i = lane >> 1, h = lane & 1;
+    const int row = row0 + i;
+    const bool valid = row < n;
+    float* o = tile + i * kTileStride + 16 * h;
+    const float3 d = valid ? ld_pos(dir, row) : make_float3(0.f, 0.f, 1.f);
+    const float s = valid ? weight[row] * scale : 0.f;
     float mx = o[0];
-    for (int k = 1; k < kLobes; k++) mx = fmaxf(mx, o[4 * k]);
-    float sum = 0.f;
-    for (int k = 0; k < kLobes; k++) {
-        w[k] = expf(o[4 * k] - mx);
-        sum += w[k];
+#pragma unroll
+    for (int j = 1; j < 4; j++) mx = fmaxf(mx, o[4 * j]);
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    LobeTerms t[4];
+    float e[4], sum = 0.f, qsum = 0.f;  // softmax normaliser; sum of e^(logit - mx) * density
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        t[j] = lobe_terms(o[4 * j + 1], o[4 * j + 2], o[4 * j + 3], d, kappa_hi);
+        e[j] = __expf(o[4 * j] - mx);
+        sum += e[j];
+        qsum += e[j] * t[j].dens;
     }
-    float q = 0.f;
-    for (int k = 0; k < kLobes; k++) {
-        w[k] /= sum;
-        const float kr = o[4 * k + 1];
-        inr[k] = kr >= kKappaLo && kr <= kappa_hi;
-        kap[k] = expf(fminf(fmaxf(kr, kKappaLo), kappa_hi));
-        st[k] = 1.f / (1.f + expf(-o[4 * k + 2]));
-        sp[k] = 1.f / (1.f + expf(-o[4 * k + 3]));
-        const float th = 3.14159265358979f * st[k], ph = 6.28318530717959f * sp[k];
-        const float s_t = sinf(th), c_t = cosf(th), s_p = sinf(ph), c_p = cosf(ph);
-        mu[k] = make_float3(s_t * c_p, s_t * s_p, c_t);
-        dth[k] = make_float3(c_t * c_p, c_t * s_p, -s_t);
-        dph[k] = make_float3(-s_t * s_p, s_t * c_p, 0.f);
-        const float c = mu[k].x * d.x + mu[k].y * d.y + mu[k].z * d.z;
-        dens[k] = kap[k] / (6.28318530717959f * -expm1f(-2.f * kap[k])) * expf(kap[k] * (c - 1.f));
-        q += w[k] * dens[k];
+    sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+    qsum += __shfl_xor_sync(0xffffffffu, qsum, 1);
+    const float inv_sum = 1.f / sum;
+    const float q = fmaxf(qsum * inv_sum, 1e-30f);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float w = e[j] * inv_sum;
+        const float r = w * t[j].dens / q;
+        const float dlogk = 1.f / t[j].kap - 2.f / expm1f(2.f * t[j].kap) + (t[j].c - 1.f);
+        const float sr = s * -r * t[j].kap;
+        o[4 * j] = valid ? s * (w - r) : 0.f;
+        o[4 * j + 1] = valid && t[j].inr ? sr * dlogk : 0.f;
+        o[4 * j + 2] = valid ? sr * t[j].dth_d * 3.14159265358979f * t[j].st * (1.f - t[j].st) : 0.f;
+        o[4 * j + 3] = valid ? sr * t[j].dph_d * 6.28318530717959f * t[j].sp * (1.f - t[j].sp) : 0.f;
     }
-    q = fmaxf(q, 1e-30f);
-    for (int k = 0; k < kLobes; k++) {
-        const float r = w[k] * dens[k] / q;
-        const float c = mu[k].x * d.x + mu[k].y * d.y + mu[k].z * d.z;
-        const float dlogk = 1.f / kap[k] - 2.f / expm1f(2.f * kap[k]) + (c - 1.f);
-        o[4 * k] = s * (w[k] - r);
-        o[4 * k + 1] = inr[k] ? s * -r * dlogk * kap[k] : 0.f;
-        o[4 * k + 2] = s * -r * kap[k] * (dth[k].x * d.x + dth[k].y * d.y + dth[k].z * d.z) * 3.14159265358979f *
-                       st[k] * (1.f - st[k]);
-        o[4 * k + 3] = s * -r * kap[k] * (dph[k].x * d.x + dph[k].y * d.y + dph[k].z * d.z) * 6.28318530717959f *
-                       sp[k] * (1.f - sp[k]);
-    }
-    return -s * logf(q);
+    return valid && h == 0 ? -s * logf(q) : 0.f;
 }
 
 // Forward + loss + backward of n samples (position, unit direction, weight);
 // `scale` multiplies every sample weight (1 / batch).  Adds the gradients to
 // grad_table / grad_mlp and the loss to *loss.
-__global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const float* __restrict__ pos,
+__global__ void __launch_bounds__(kBwdWarps * 32, 2) k_guide_backward(NetView net, const float* __restrict__ pos,
                                                            const float* __restrict__ dir,
                                                            const float* __restrict__ weight, int n, float scale,
                                                            const float* __restrict__ weight_sum,
@@ -320,39 +402,47 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
     __half* sw = reinterpret_cast<__half*>(smem);
     __half* sb = sw + kFwdHalves;
     float* tiles = reinterpret_cast<float*>(smem + (kFwdHalves + kBwdHalves) * sizeof(__half));
+    int* sres = reinterpret_cast<int*>(tiles + kBwdWarps * 16 * (kTileStride + 3));
     load_weights(net.mlp, sw, sb);
+    if (threadIdx.x == 0) {  // constant indices: a runtime index would copy net.res to local memory
+#pragma unroll
+        for (int q = 0; q < kLevels; q++) sres[q] = net.res[q];
+    }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
     float* tile = tiles + warp * 16 * kTileStride;
+    float* ptile = tiles + kBwdWarps * 16 * kTileStride + warp * 48;  // the tile's 16 positions
+    const int lres = sres[lane >> 1];  // resolution of this lane's level in the gradient scatter
     float lsum = 0.f;
     const int tiles_total = (n + 15) / 16;
-    for (int tt = blockIdx.x * kWarps + warp; tt < tiles_total; tt += gridDim.x * kWarps) {
+    for (int tt = blockIdx.x * kBwdWarps + warp; tt < tiles_total; tt += gridDim.x * kBwdWarps) {
         const int r0 = tt * 16 + g, r1 = r0 + 8;
         const bool v0 = r0 < n, v1 = r1 < n;
         const float3 x0 = v0 ? ld_pos(pos, r0) : make_float3(0.f, 0.f, 0.f);
         const float3 x1 = v1 ? ld_pos(pos, r1) : make_float3(0.f, 0.f, 0.f);
-        uint32_t ax[2][4], h1[4][4], h2[4][4], h3[4][4];
+        // forward: each layer's input goes to the fragments as soon as it
+        // exists; only its ReLU mask stays in registers for the backward
+        uint32_t* tf = frags + size_t(tt) * kFragWords * 32;
+        uint32_t ax[2][4], h[4][4];
         encode_tile(net, x0, x1, v0, v1, ax);
+        frag_store<2>(tf, kFragAx, ax, lane);
         float d64[8][4], out[4][4];
         layer<kIn, kHid, kS32>(ax, sw + kOffW0, d64);
-        pack_relu<kHid>(d64, h1);
-        layer<kHid, kHid, kS64>(h1, sw + kOffW1, d64);
-        pack_relu<kHid>(d64, h2);
-        layer<kHid, kHid, kS64>(h2, sw + kOffW2, d64);
-        pack_relu<kHid>(d64, h3);
-        layer<kHid, kOut, kS64>(h3, sw + kOffW3, out);
+        pack_relu<kHid>(d64, h);
+        frag_store<4>(tf, kFragH1, h, lane);
+        const uint32_t m1 = relu_mask<kHid>(h);
+        layer<kHid, kHid, kS64>(h, sw + kOffW1, d64);
+        pack_relu<kHid>(d64, h);
+        frag_store<4>(tf, kFragH2, h, lane);
+        const uint32_t m2 = relu_mask<kHid>(h);
+        layer<kHid, kHid, kS64>(h, sw + kOffW2, d64);
+        pack_relu<kHid>(d64, h);
+        frag_store<4>(tf, kFragH3, h, lane);
+        const uint32_t m3 = relu_mask<kHid>(h);
+        layer<kHid, kOut, kS64>(h, sw + kOffW3, out);
         stage_outputs(out, tile);
         __syncwarp();
-        if (lane < 16) {
-            const int row = tt * 16 + lane;
-            float* o = tile + lane * kTileStride;
-            if (row < n) {
-                const float3 dd = ld_pos(dir, row);
-                lsum += loss_grad_row(o, dd, weight[row] * scale, net.kappa_hi);
-            } else {
-                for (int k = 0; k < kOut; k++) o[k] = 0.f;
-            }
-        }
+        lsum += loss_grad_tile(tile, tt * 16, n, dir, weight, scale, net.kappa_hi);
         __syncwarp();
         // dO as A fragments (fp16)
         uint32_t ado[2][4];
@@ -365,39 +455,71 @@ __global__ void __launch_bounds__(kBlock) k_guide_backward(NetView net, const fl
             ado[t][3] = pack_h2(p[8 * kTileStride + 8], p[8 * kTileStride + 9]);
         }
         __syncwarp();
-        uint32_t* tf = frags + size_t(tt) * kFragWords * 32;
         frag_store<2>(tf, kFragAdo, ado, lane);
-        frag_store<4>(tf, kFragH3, h3, lane);
-        frag_store<4>(tf, kFragH2, h2, lane);
-        frag_store<4>(tf, kFragH1, h1, lane);
-        frag_store<2>(tf, kFragAx, ax, lane);
         uint32_t e[4][4];
         layer<kOut, kHid, kS32>(ado, sb + kOffT3, d64);
-        pack_masked<kHid>(d64, h3, e);
+        pack_masked<kHid>(d64, m3, e);
         frag_store<4>(tf, kFragE3, e, lane);
         layer<kHid, kHid, kS64>(e, sb + kOffT2, d64);
-        pack_masked<kHid>(d64, h2, e);
+        pack_masked<kHid>(d64, m2, e);
         frag_store<4>(tf, kFragE2, e, lane);
         layer<kHid, kHid, kS64>(e, sb + kOffT1, d64);
-        pack_masked<kHid>(d64, h1, e);
+        pack_masked<kHid>(d64, m1, e);
         frag_store<4>(tf, kFragE1, e, lane);
         float dx[4][4];
         layer<kHid, kIn, kS64>(e, sb + kOffT0, dx);
-        // hash-grid gradient: this thread's levels 4j + tig for rows g (dx[j][0..1]) and g + 8 (dx[j][2..3])
+        // hash-grid gradient.  The 16 x 32 input gradient goes through the
+        // staging tile so that lane 2l + hh owns level l for rows 8hh..8hh+7.
+        // Consecutive batch rows are neighbouring samples: a corner that the
+        // next row shares is summed in registers and leaves as one reduction,
+        // which spares the contended coarse levels most of their atomics.
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const int l = 4 * j + tig;
+            float* p = tile + g * kTileStride + 8 * j + 2 * tig;
+            p[0] = dx[j][0];
+            p[1] = dx[j][1];
+            p[8 * kTileStride] = dx[j][2];
+            p[8 * kTileStride + 1] = dx[j][3];
+        }
+        if (tig == 0) {
+            float* q = ptile + 3 * g;
+            q[0] = x0.x, q[1] = x0.y, q[2] = x0.z;
+            q[24] = x1.x, q[25] = x1.y, q[26] = x1.z;
+        }
+        __syncwarp();
+        {
+            const int l = lane >> 1, rbase = 8 * (lane & 1);
+            const int rows = min(8, n - tt * 16 - rbase);
+            float2* gt = reinterpret_cast<float2*>(grad_table) + size_t(l) * kT;
+            uint32_t pidx[8];
+            float2 pg[8];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                if (!(h ? v1 : v0)) continue;
+            for (int r = 0; r < 8; r++) {
+                if (r >= rows) break;
+                const int row = rbase + r;
+                const float3 x = make_float3(ptile[3 * row], ptile[3 * row + 1], ptile[3 * row + 2]);
+                const float g0 = tile[row * kTileStride + 2 * l], g1 = tile[row * kTileStride + 2 * l + 1];
                 Corners c;
-                level_corners(net.res, l, h ? x1 : x0, c);
-                float2* gt = reinterpret_cast<float2*>(grad_table) + size_t(l) * kT;
-                const float g0 = dx[j][2 * h], g1 = dx[j][2 * h + 1];
+                level_corners(lres, x, c);
 #pragma unroll
-                for (int k = 0; k < 8; k++) atomicAdd(gt + c.idx[k], make_float2(c.w[k] * g0, c.w[k] * g1));
+                for (int k = 0; k < 8; k++) {
+                    const float2 v = make_float2(c.w[k] * g0, c.w[k] * g1);
+                    if (r > 0 && c.idx[k] == pidx[k]) {
+                        pg[k].x += v.x;
+                        pg[k].y += v.y;
+                    } else {
+                        if (r > 0) atomicAdd(gt + pidx[k], pg[k]);
+                        pidx[k] = c.idx[k];
+                        pg[k] = v;
+                    }
+                }
+            }
+            if (rows > 0) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) atomicAdd(gt + pidx[k], pg[k]);
             }
         }
+        __syncwarp();
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
@@ -417,15 +539,12 @@ RT_D void wgrad_role(const uint32_t* __restrict__ frags, int t0, int t1, int off
 #pragma unroll
     for (int j = 0; j < N / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
     for (int tt = t0; tt < t1; tt++) {
-        const uint32_t* tf = frags + size_t(tt) * kFragWords * 32 + lane;
+        const uint32_t* tf = frags + size_t(tt) * kFragWords * 32;
         uint32_t x[N / 16][4];
 #pragma unroll
-        for (int t = 0; t < N / 16; t++)
-#pragma unroll
-            for (int r = 0; r < 4; r++) x[t][r] = __ldg(tf + (offX + 4 * t + r) * 32);
+        for (int t = 0; t < N / 16; t++) frag_load(tf, offX + 4 * t, lane, x[t]);
         uint32_t e4[4];
-#pragma unroll
-        for (int r = 0; r < 4; r++) e4[r] = __ldg(tf + (offE + 4 * mt + r) * 32);
+        frag_load(tf, offE + 4 * mt, lane, e4);
         const uint32_t at[4] = {trans8x8(e4[0]), trans8x8(e4[2]), trans8x8(e4[1]), trans8x8(e4[3])};
 #pragma unroll
         for (int j = 0; j < N / 8; j++) {
@@ -443,7 +562,7 @@ RT_D void wgrad_role(const uint32_t* __restrict__ frags, int t0, int t1, int off
     }
 }
 
-__global__ void __launch_bounds__(kWgradRoles * 32) k_guide_wgrad(const uint32_t* __restrict__ frags, int tiles,
+__global__ void __launch_bounds__(kWgradRoles * 32, 2) k_guide_wgrad(const uint32_t* __restrict__ frags, int tiles,
                                                                   int chunk, float* __restrict__ grad_mlp) {
     const int role = threadIdx.x >> 5;
     const int t0 = blockIdx.x * chunk, t1 = min(tiles, t0 + chunk);
@@ -466,8 +585,9 @@ struct GuidedItems {
 
 RT_D GuidedItems guided_items(const rtd::WaveCtl* ctl) {
     GuidedItems gi;
-    int m = 0;
+    int m = 0;  // a constant at every step once both loops are unrolled, so gi stays in registers
     gi.n = 0;
+#pragma unroll
     for (int b = 0; b < rtd::kShadeBuckets; b++) {
         if (b == rtd::kMissBucket || !guided_type(b)) continue;
         gi.bucket[m] = b;
@@ -475,14 +595,26 @@ RT_D GuidedItems guided_items(const rtd::WaveCtl* ctl) {
         gi.n += gi.count[m];
         m++;
     }
+#pragma unroll
     for (; m < kShadeBucketsG; m++) gi.bucket[m] = gi.count[m] = 0;
     return gi;
 }
 
+// The slot of guided item i: bucket m holds items [base_m, base_m + count_m).
+// Unrolled with constant indices (a runtime index would put gi in local memory).
 RT_D int guided_slot(const GuidedItems& gi, const rtd::WaveBufs& B, int i) {
-    int m = 0, base = 0;
-    while (m < kShadeBucketsG - 1 && i >= base + gi.count[m]) base += gi.count[m++];
-    return B.sorted[size_t(gi.bucket[m]) * size_t(B.capacity) + size_t(i - base)];
+    int bucket = gi.bucket[0], base = 0;
+    bool found = false;
+#pragma unroll
+    for (int m = 0; m < kShadeBucketsG - 1; m++) {
+        if (!found && i >= base + gi.count[m]) {
+            base += gi.count[m];
+            bucket = gi.bucket[m + 1];
+        } else {
+            found = true;
+        }
+    }
+    return B.sorted[size_t(bucket) * size_t(B.capacity) + size_t(i - base)];
 }
 
 RT_D float3 hit_position(const rtd::Ctx& c, int slot) {
@@ -597,14 +729,19 @@ __global__ void k_guide_batch(const float4* __restrict__ buf, const int* __restr
     float wi = 0.f;
     if (i < n) {
         float4 a = make_float4(0.5f, 0.5f, 0.5f, 0.f), b = make_float4(0.f, 0.f, 1.f, 0.f);
-        if (cnt > n) {  // a random subset (with replacement)
-            uint32_t h = uint32_t(i) * 0x9E3779B9u ^ seed;
+        if (cnt > n) {
+            // every (cnt / n)-th sample from a start drawn per step: each
+            // sample at most once, and neighbouring batch rows are samples
+            // written close together (in slot order, so close in space), so
+            // the hash-grid gradient of a 16-row tile merges repeated corners
+            uint32_t h = seed * 0x9E3779B9u;
             h ^= h >> 16;
             h *= 0x85EBCA6Bu;
             h ^= h >> 13;
             h *= 0xC2B2AE35u;
             h ^= h >> 16;
-            const int j = int(uint64_t(h) * uint64_t(cnt) >> 32);
+            const uint64_t start = uint64_t(h) * uint64_t(cnt) >> 32;
+            const int j = int((start + uint64_t(i) * uint64_t(cnt) / uint64_t(n)) % uint64_t(cnt));
             a = buf[2 * size_t(j)];
             b = buf[2 * size_t(j) + 1];
         } else if (i < cnt) {  // every sample once; the rest of the batch weighs nothing
@@ -676,7 +813,8 @@ static size_t infer_smem() {
     return size_t(rtg::kFwdHalves) * 2 + size_t(rtg::kInferWarps) * 16 * rtg::kTileStride * 4;
 }
 size_t backward_smem() {
-    return size_t(rtg::kFwdHalves + rtg::kBwdHalves) * 2 + size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4;
+    return size_t(rtg::kFwdHalves + rtg::kBwdHalves) * 2 + size_t(rtg::kBwdWarps) * 16 * (rtg::kTileStride + 3) * 4 +
+           size_t(rtg::kLevels) * 4;
 }
 
 cudaError_t prepare_kernels() {
@@ -711,9 +849,9 @@ void launch_backward(const rtg::NetView& net, const float* pos, const float* dir
     for (int begin = 0; begin < n; begin += frag_tiles * 16) {
         const int m = std::min(n - begin, frag_tiles * 16);
         const int tiles = (m + 15) / 16;
-        int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
-        if (blocks > sms * 3) blocks = sms * 3;  // shared weights and transposes, ~64 KB per block
-        rtg::k_guide_backward<<<blocks, rtg::kBlock, backward_smem(), st>>>(
+        int blocks = (tiles + rtg::kBwdWarps - 1) / rtg::kBwdWarps;
+        if (blocks > sms * 2) blocks = sms * 2;  // 2 resident per SM: <= 128 registers, ~73 KB shared each
+        rtg::k_guide_backward<<<blocks, rtg::kBwdWarps * 32, backward_smem(), st>>>(
             net, pos + size_t(begin) * 3, dir + size_t(begin) * 3, weight + begin, m, scale, weight_sum, grad_table,
             frags, loss);
         const int chunk = std::max(4, (tiles + 2 * sms - 1) / (2 * sms));
