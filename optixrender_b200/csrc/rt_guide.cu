@@ -780,6 +780,43 @@ __global__ void k_adam(float* __restrict__ p, __half* __restrict__ p16, float* _
     }
 }
 
+// Adam on the hash table, level l = blockIdx.y over its first n_l entries
+// (one entry = kFeats = 2 parameters, moved as float2 / half2).  Entries past
+// n_l have never had a gradient (m = v = 0), for which Adam's update is 0,
+// so leaving them out changes nothing.
+struct LevelExtents {
+    int32_t n[kLevels];  // entries of each level that any resolution so far has used
+};
+__global__ void __launch_bounds__(256) k_adam_table(float2* __restrict__ p, __half2* __restrict__ p16,
+                                                    float2* __restrict__ grad, float2* __restrict__ m,
+                                                    float2* __restrict__ v, LevelExtents ext, float lr, float b1,
+                                                    float b2, float c1, float c2, float eps) {
+    __shared__ int32_t s_n;
+    if (threadIdx.x == 0) {  // constant indices only: a runtime index would copy ext to local memory
+        int32_t n = 0;
+#pragma unroll
+        for (int q = 0; q < kLevels; q++)
+            if (int(blockIdx.y) == q) n = ext.n[q];
+        s_n = n;
+    }
+    __syncthreads();
+    const int32_t n = s_n;
+    const size_t base = size_t(blockIdx.y) * kT;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t k = base + size_t(i);
+        const float2 gr = grad[k], mo = m[k], vo = v[k], po = p[k];
+        grad[k] = make_float2(0.f, 0.f);
+        const float2 mi = make_float2(b1 * mo.x + (1.f - b1) * gr.x, b1 * mo.y + (1.f - b1) * gr.y);
+        const float2 vi = make_float2(b2 * vo.x + (1.f - b2) * gr.x * gr.x, b2 * vo.y + (1.f - b2) * gr.y * gr.y);
+        m[k] = mi;
+        v[k] = vi;
+        const float2 pi = make_float2(po.x - lr * (mi.x * c1) / (sqrtf(vi.x * c2) + eps),
+                                      po.y - lr * (mi.y * c1) / (sqrtf(vi.y * c2) + eps));
+        p[k] = pi;
+        p16[k] = __floats2half2_rn(pi.x, pi.y);
+    }
+}
+
 __global__ void k_to_half(const float* __restrict__ p, __half* __restrict__ p16, int64_t n) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
         p16[i] = __float2half_rn(p[i]);
@@ -873,13 +910,31 @@ void launch_batch(const float4* buf, const int* count, int cap, int n, uint32_t 
     rtg::k_guide_batch<<<(n + 255) / 256, 256, 0, st>>>(buf, count, cap, n, seed, pos, dir, w, weight_sum);
 }
 
+static constexpr float kAdamB1 = 0.9f, kAdamB2 = 0.99f, kAdamEps = 1e-10f;
+
 void launch_adam(float* p, __half* p16, float* grad, float* m, float* v, int64_t n, float lr, int step,
                  cudaStream_t st) {
-    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-10f;
+    const float b1 = kAdamB1, b2 = kAdamB2, eps = kAdamEps;
     const float c1 = 1.0f / (1.0f - powf(b1, float(step))), c2 = 1.0f / (1.0f - powf(b2, float(step)));
     int blocks = int((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     rtg::k_adam<<<blocks, 256, 0, st>>>(p, p16, grad, m, v, n, lr, b1, b2, c1, c2, eps);
+}
+
+void launch_adam_table(float* p, __half* p16, float* grad, float* m, float* v, const int64_t* level_entries, float lr,
+                       int step, cudaStream_t st) {
+    const float b1 = kAdamB1, b2 = kAdamB2, eps = kAdamEps;
+    const float c1 = 1.0f / (1.0f - powf(b1, float(step))), c2 = 1.0f / (1.0f - powf(b2, float(step)));
+    rtg::LevelExtents ext;
+    int64_t most = 1;
+    for (int l = 0; l < rtg::kLevels; l++) {
+        ext.n[l] = int32_t(std::min<int64_t>(level_entries[l], rtg::kT));
+        most = std::max<int64_t>(most, ext.n[l]);
+    }
+    const int gx = int(std::min<int64_t>((most + 255) / 256, 256));
+    rtg::k_adam_table<<<dim3(gx, rtg::kLevels), 256, 0, st>>>(
+        reinterpret_cast<float2*>(p), reinterpret_cast<__half2*>(p16), reinterpret_cast<float2*>(grad),
+        reinterpret_cast<float2*>(m), reinterpret_cast<float2*>(v), ext, lr, b1, b2, c1, c2, eps);
 }
 
 void launch_to_half(const float* p, __half* p16, int64_t n, cudaStream_t st) {

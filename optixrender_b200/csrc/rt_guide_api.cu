@@ -33,7 +33,21 @@ struct rt_guide {
     DevBuf frags;  // training fragments of up to kFragTiles tiles, allocated at the first training pass
     int step = 0;
     int res[rtg::kLevels];
+    int64_t used_entries[rtg::kLevels] = {};  // per level: entries any resolution so far has addressed
 };
+
+// Level resolutions for n_max, and the entries each level addresses: a dense
+// level (res + 1)^3 of them, a hashed one the whole table.  The Adam update
+// covers the largest count seen, so entries that once had a gradient keep
+// their moments decaying after a resolution change.
+static void set_resolutions(rt_guide* g, int n_max) {
+    rtgh::level_resolutions(n_max, g->res);
+    for (int l = 0; l < rtg::kLevels; l++) {
+        const int64_t r1 = int64_t(g->res[l]) + 1;
+        const int64_t n = r1 * r1 * r1 <= int64_t(rtg::kT) ? r1 * r1 * r1 : int64_t(rtg::kT);
+        g->used_entries[l] = std::max(g->used_entries[l], n);
+    }
+}
 
 namespace {
 
@@ -106,7 +120,7 @@ rt_status guide_create(const rt_guide_options* o, rt_guide** out) {
         rt_guide_destroy(g);
         return fail(RT_ERR_INVALID_ARG, "rt_guide_create: max_resolution in [2, 2^20], max_log_kappa > -2");
     }
-    rtgh::level_resolutions(g->opt.max_resolution, g->res);
+    set_resolutions(g, g->opt.max_resolution);
     rt_status st = RT_OK;
     auto check = [&](cudaError_t ce, const char* what) {
         if (st == RT_OK && ce != cudaSuccess) st = cuda_fail(ce, what);
@@ -167,8 +181,8 @@ rt_status guide_train_device(rt_guide* g, const float* pos, const float* dir, co
     rtgh::launch_backward(view(g), pos, dir, weight, n, scale, weight_sum, g->gtable.as<float>(), g->gmlp.as<float>(),
                           g->loss.as<float>(), g->frags.as<uint32_t>(), kFragTiles, g->sms, st);
     g->step++;
-    rtgh::launch_adam(g->table.as<float>(), g->table16.as<__half>(), g->gtable.as<float>(), g->mt.as<float>(),
-                      g->vt.as<float>(), rtg::kTableParams, g->opt.learning_rate, g->step, st);
+    rtgh::launch_adam_table(g->table.as<float>(), g->table16.as<__half>(), g->gtable.as<float>(), g->mt.as<float>(),
+                            g->vt.as<float>(), g->used_entries, g->opt.learning_rate, g->step, st);
     rtgh::launch_adam(g->mlp.as<float>(), g->mlp16.as<__half>(), g->gmlp.as<float>(), g->mm.as<float>(),
                       g->vm.as<float>(), rtg::kMlpParams, g->opt.learning_rate, g->step, st);
     GD_CUDA(cudaGetLastError(), "guide training step");
@@ -314,7 +328,7 @@ rt_status rt_guide_set_hyperparameters(rt_guide* g, float lr, int32_t max_resolu
     if (lr > 0.0f) g->opt.learning_rate = lr;
     if (max_resolution > 0) {
         g->opt.max_resolution = max_resolution;
-        rtgh::level_resolutions(max_resolution, g->res);
+        set_resolutions(g, max_resolution);
     }
     if (max_log_kappa != 0.0f) g->opt.max_log_kappa = max_log_kappa;
     return RT_OK;

@@ -29,6 +29,9 @@ void launch_batch(const float4* buf, const int* count, int cap, int n, uint32_t 
                   float* w, float* weight_sum, cudaStream_t st);
 void launch_adam(float* p, __half* p16, float* grad, float* m, float* v, int64_t n, float lr, int step,
                  cudaStream_t st);
+// Adam on the hash table's first level_entries[l] entries of every level l.
+void launch_adam_table(float* p, __half* p16, float* grad, float* m, float* v, const int64_t* level_entries, float lr,
+                       int step, cudaStream_t st);
 void launch_to_half(const float* p, __half* p16, int64_t n, cudaStream_t st);
 void launch_pdf_sample(const rtg::Mixture* mix, const float* dir, const float* u, int n, float* out_dir, float* pdf,
                        cudaStream_t st);

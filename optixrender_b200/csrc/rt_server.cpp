@@ -43,7 +43,8 @@
 #include "rt_internal.h"
 #include "rt_schedule.h"
 
-static_assert(RT_SERVE_FAIR == rti::kPlanFair && RT_SERVE_FIFO == rti::kPlanFifo && RT_SERVE_SRPT == rti::kPlanSrpt,
+static_assert(int(RT_SERVE_FAIR) == int(rti::kPlanFair) && int(RT_SERVE_FIFO) == int(rti::kPlanFifo) &&
+                  int(RT_SERVE_SRPT) == int(rti::kPlanSrpt),
               "policy numbering");
 
 using namespace rtd;
