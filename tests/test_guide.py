@@ -178,3 +178,51 @@ def test_online_training_learns_a_direction_field():
     good = g.pdf(pos, mu)
     bad = g.pdf(pos, -mu)
     assert np.median(good) > 1.0 and np.median(good) > 20 * np.median(bad)
+
+
+@pytest.mark.gpu
+def test_train_step_is_one_adam_step():
+    """A first train step moves every parameter with a gradient by -lr *
+    g / (|g| + eps) (Adam's first step) and leaves the rest untouched; the
+    table update covers only the entries the levels address, so this checks
+    that none with a gradient is left out."""
+    import optixrender_b200 as rt
+    lr = 1e-3
+    g = rt.Guide(learning_rate=lr, max_resolution=64)
+    table, ws = _params(41, table_scale=0.5, out_scale=0.3)
+    g.set_params(table.reshape(-1), np.concatenate([w.reshape(-1) for w in ws]))
+    pos, d, _ = _samples(8192, 42)
+    w = np.ones(len(pos), np.float32)
+    _, gt, gm = g.gradients(pos, d, w)
+    t0, m0 = g.get_params()
+    g.train_step(pos, d, w)
+    t1, m1 = g.get_params()
+    for name, p0, p1, gr in (("table", t0, t1, gt), ("mlp", m0, m1, gm)):
+        big = np.abs(gr) > 1e-3 * np.abs(gr).max()
+        step = (p1 - p0)[big].astype(np.float64)
+        print(name, "entries with gradient", int(big.sum()))
+        assert big.sum() > 100
+        assert np.allclose(step, -lr * np.sign(gr[big]), rtol=0, atol=2e-2 * lr), name
+        zero = gr == 0
+        assert np.array_equal(p1[zero], p0[zero]), name
+
+
+@pytest.mark.gpu
+def test_adam_keeps_moments_of_entries_a_lower_resolution_drops():
+    """After max_resolution goes down, table entries only the old resolution
+    addressed get no more gradient but, as in a dense Adam, keep moving on
+    their decaying first moment."""
+    import optixrender_b200 as rt
+    g = rt.Guide(learning_rate=1e-3, max_resolution=64)
+    pos, d, w = _samples(8192, 43)
+    _, gt, _ = g.gradients(pos, d, w)
+    g.train_step(pos, d, w)
+    g.set_hyperparameters(max_resolution=32)
+    t1, _ = g.get_params()
+    _, gt32, _ = g.gradients(pos, d, w)
+    g.train_step(pos, d, w)
+    t2, _ = g.get_params()
+    dropped = (gt != 0) & (gt32 == 0)
+    print("entries addressed only at 64:", int(dropped.sum()))
+    assert dropped.sum() > 1000
+    assert np.count_nonzero(t2[dropped] != t1[dropped]) > 0.9 * dropped.sum()
