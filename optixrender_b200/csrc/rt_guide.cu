@@ -718,9 +718,9 @@ __global__ void k_guide_collect(rtd::Ctx c, float4* __restrict__ buf, int* __res
     }
 }
 
-// A training batch of `n` samples: all collected ones when they fit, else a
-// uniform random subset (with replacement); accumulates the batch's weight sum
-// for the loss scale.
+// A training batch of `n` samples: all collected ones when they fit, else
+// every (count / n)-th one from a start drawn from `seed`; accumulates the
+// batch's weight sum for the loss scale.
 __global__ void k_guide_batch(const float4* __restrict__ buf, const int* __restrict__ count, int cap, int n,
                               uint32_t seed, float* __restrict__ pos, float* __restrict__ dir, float* __restrict__ w,
                               float* __restrict__ weight_sum) {
@@ -828,7 +828,7 @@ __global__ void k_guide_pdf_sample(const Mixture* __restrict__ mix, const float*
                                    float* __restrict__ pdf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const Mixture m = mix[i];
+    const Mixture* m = mix + i;
     rtd::v3 d;
     if (u) {
         d = mixture_sample(m, u[3 * i], u[3 * i + 1], u[3 * i + 2]);

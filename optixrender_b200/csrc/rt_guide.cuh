@@ -88,24 +88,28 @@ RT_D float vmf_pdf(float4 l, rtd::v3 d) {
     return l.w / (6.28318530717959f * -expm1f(-2.0f * l.w)) * __expf(l.w * (c - 1.0f));
 }
 
-RT_D float mixture_pdf(const Mixture& m, rtd::v3 d) {
-    float p = 0.0f;
+// Lobe of a mixture picked by u0: the first k with u0 < w_0 + ... + w_k (the
+// last lobe when rounding leaves u0 above the running sum).  Constant indices
+// only, so the weights stay in registers.
+RT_D int pick_lobe(const float (&w)[kLobes], float u0) {
+    int k = kLobes - 1;
+    float acc = 0.0f;
+    bool found = false;
 #pragma unroll
-    for (int k = 0; k < kLobes; k++) p += m.w[k] * vmf_pdf(m.lobe[k], d);
-    return p;
+    for (int j = 0; j < kLobes - 1; j++) {
+        acc += w[j];
+        if (!found && u0 < acc) {
+            k = j;
+            found = true;
+        }
+    }
+    return k;
 }
 
-// Picks a lobe with u0 and samples it with (u1, u2): the cosine to mu is
+// Samples the vMF lobe l = (mu, kappa) with (u1, u2): the cosine to mu is
 // 1 + log(u1 + (1 - u1) e^{-2 kappa}) / kappa (Jakob, "Numerically stable
 // sampling of the von Mises Fisher distribution on S2", 2012).
-RT_D rtd::v3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
-    int k = 0;
-    float acc = m.w[0];
-    while (k < kLobes - 1 && u0 >= acc) {
-        k++;
-        acc += m.w[k];
-    }
-    const float4 l = m.lobe[k];
+RT_D rtd::v3 vmf_sample(float4 l, float u1, float u2) {
     float w = 1.0f + __logf(u1 + (1.0f - u1) * __expf(-2.0f * l.w)) / l.w;
     w = fminf(fmaxf(w, -1.0f), 1.0f);
     const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
@@ -120,7 +124,7 @@ RT_D rtd::v3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
     return normalize(t1 * (s * cp) + t2 * (s * sp) + mu * w);
 }
 
-// The same on a mixture in global memory (read-only for the kernel).
+// Density and sampling of a mixture in global memory (read-only for the kernel).
 RT_D float mixture_pdf(const Mixture* m, rtd::v3 d) {
     const float4* w4 = reinterpret_cast<const float4*>(m->w);
     const float4 wa = __ldg(w4), wb = __ldg(w4 + 1);
@@ -130,15 +134,12 @@ RT_D float mixture_pdf(const Mixture* m, rtd::v3 d) {
     for (int k = 0; k < kLobes; k++) p += w[k] * vmf_pdf(__ldg(m->lobe + k), d);
     return p;
 }
+// Picks a lobe with u0 and samples it with (u1, u2).
 RT_D rtd::v3 mixture_sample(const Mixture* m, float u0, float u1, float u2) {
-    Mixture c;
-#pragma unroll
-    for (int k = 0; k < kLobes; k++) c.lobe[k] = __ldg(m->lobe + k);
     const float4* w4 = reinterpret_cast<const float4*>(m->w);
     const float4 wa = __ldg(w4), wb = __ldg(w4 + 1);
-    c.w[0] = wa.x, c.w[1] = wa.y, c.w[2] = wa.z, c.w[3] = wa.w;
-    c.w[4] = wb.x, c.w[5] = wb.y, c.w[6] = wb.z, c.w[7] = wb.w;
-    return mixture_sample(c, u0, u1, u2);
+    const float w[kLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    return vmf_sample(__ldg(m->lobe + pick_lobe(w, u0)), u1, u2);
 }
 
 // Network input of a surface point: the position moved by kSideOffset (in

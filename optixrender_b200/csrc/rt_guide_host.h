@@ -22,7 +22,7 @@ void launch_backward(const rtg::NetView& net, const float* pos, const float* dir
                      float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss,
                      uint32_t* frags, int frag_tiles, int sms, cudaStream_t st);
 // Renderer side: mixtures of a bounce's guided vertices, training samples of
-// a wave, random training batches.
+// a wave, training batches (strided subsets from a random start).
 void launch_infer(const rtd::Ctx& c, const rtg::NetView& net, int sms, cudaStream_t st);
 void launch_collect(const rtd::Ctx& c, float4* buf, int* count, int cap, cudaStream_t st);
 void launch_batch(const float4* buf, const int* count, int cap, int n, uint32_t seed, float* pos, float* dir,
