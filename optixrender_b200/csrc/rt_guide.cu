@@ -180,13 +180,24 @@ RT_D void level_corners(int res, float3 x, Corners& c) {
     const float fx = px - cx, fy = py - cy, fz = pz - cz;
     const uint32_t ix = uint32_t(cx), iy = uint32_t(cy), iz = uint32_t(cz);
     const uint32_t r1 = uint32_t(res) + 1u;
-    const bool dense = uint64_t(r1) * r1 * r1 <= uint64_t(kT);
+    // A level whose (res + 1)^3 grid points fit the table indexes them
+    // directly, a finer one hashes them.  Branching (rather than selecting
+    // per corner) spares the dense levels the hash arithmetic; the condition
+    // is the same for every lane on the same level.
+    if (uint64_t(r1) * r1 * r1 <= uint64_t(kT)) {
+        const uint32_t r2 = r1 * r1, base = ix + iy * r1 + iz * r2;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const uint32_t gx = ix + (k & 1), gy = iy + ((k >> 1) & 1), gz = iz + ((k >> 2) & 1);
-        c.idx[k] = dense ? gx + gy * r1 + gz * r1 * r1 : ((gx * 1u) ^ (gy * kPrime1) ^ (gz * kPrime2)) & uint32_t(kT - 1);
-        c.w[k] = ((k & 1) ? fx : 1.0f - fx) * (((k >> 1) & 1) ? fy : 1.0f - fy) * (((k >> 2) & 1) ? fz : 1.0f - fz);
+        for (int k = 0; k < 8; k++) c.idx[k] = base + (k & 1) + ((k >> 1) & 1) * r1 + ((k >> 2) & 1) * r2;
+    } else {
+        const uint32_t hx[2] = {ix, ix + 1u}, hy[2] = {iy * kPrime1, (iy + 1u) * kPrime1},
+                       hz[2] = {iz * kPrime2, (iz + 1u) * kPrime2};
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            c.idx[k] = (hx[k & 1] ^ hy[(k >> 1) & 1] ^ hz[(k >> 2) & 1]) & uint32_t(kT - 1);
     }
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        c.w[k] = ((k & 1) ? fx : 1.0f - fx) * (((k >> 1) & 1) ? fy : 1.0f - fy) * (((k >> 2) & 1) ? fz : 1.0f - fz);
 }
 
 RT_D uint32_t encode_level(const __half2* __restrict__ table, int res, int l, float3 x) {
