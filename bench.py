@@ -21,7 +21,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import re
 import os
 import subprocess
 import sys
@@ -37,6 +36,11 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 WORKLOAD = dict(width=1920, height=1080, spp=64, max_depth=16)
 NODE_BYTES, TRI_BYTES, RAY_BYTES = 80, 48, 52  # wide node, triangle record, ray in + hit out + queue entry
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_extend
+# launch of this workload, recorded from an ncu capture (the summary and its
+# command are in profiles/); this run does not measure it.  Keyed by the wave
+# size the capture used: a figure for another wave size is not reported.
+RECORDED_EXTEND_DRAM_BYTES = {}
 
 
 def parse():
@@ -210,7 +214,8 @@ class CpuRunner:
 
     def sample(self, spp, seconds, threads=0):
         """Times a band of rows (then more samples) sized to about `seconds`."""
-        from optixrender_b200 import camera, options
+        from optixrender_b200 import camera  # a plain ctypes struct: no library is loaded
+        from pyoracle import options
         spec = self.spec
         cam = camera(**spec.camera)
         H, W = spec.settings["height"], spec.settings["width"]
@@ -238,8 +243,15 @@ class CpuRunner:
                           f"{dt:.1f} s); the full step is {spp} spp"}
 
 
+def bench_config(spp, triangles, world):
+    """The workload as both arms report it."""
+    return {"workload": "spheres-1080p", **dict(WORKLOAD, spp=spp), "triangles": triangles,
+            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (scene + BVH ~0.3 GB)"}
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU path on the host cores."""
+    """--impl reference: the reference's CPU path on the host cores.  It loads
+    the reference's host build (or the oracle), never the product library."""
     from optixrender_b200 import scenes
     if rank != 0:
         return 0
@@ -256,7 +268,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "Mpaths/s", "value": v, "unit": "Mpaths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "spheres-1080p", **WORKLOAD, "spp": args.spp, "triangles": spec.num_triangles},
+            "config": bench_config(args.spp, spec.num_triangles, world),
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -349,28 +361,20 @@ def main():
                  counters["extend_rays"] * RAY_BYTES)
     ext_ms = kern["extend"]
     achieved = ext_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
-    # DRAM bytes per k_extend launch from the committed ncu summary of one wave
-    # of this workload (dram__bytes_read.sum + dram__bytes_write.sum)
-    # (used when the summary's wave size is the one this run used)
-    traffic = None
-    for prof in sorted((ROOT / "profiles").glob("k_extend*dram_traffic*.md")):
-        txt = prof.read_text()
-        m = re.search(r"k_extend bytes_per_launch: (\d+)", txt)
-        w = re.search(r"wave_paths: (\d+)", txt)
-        if m and w and int(w.group(1)) == wave_paths:
-            traffic = int(m.group(1))
+    traffic = RECORDED_EXTEND_DRAM_BYTES.get(wave_paths)
     line = {
         "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "spheres-1080p", **dict(WORKLOAD, spp=args.spp), "triangles": spec.num_triangles,
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (scene + BVH ~0.3 GB)",
-                   "wave_paths": wave_paths},
+        "config": bench_config(args.spp, spec.num_triangles, world),
+        "wave_paths": wave_paths,
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": W * H * 4},
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak if peak else None,
                      "traffic": traffic, "peak_source": peak_kind,
+                     "traffic_source": "recorded ncu capture of one k_extend launch of this workload (profiles/), "
+                                       "not measured by this run" if traffic is not None else None,
                      "algorithmic_bytes_per_launch": ext_bytes / max(1, counters["extend_launches"]),
                      "ms_extend_per_launch": ext_ms / max(1, counters["extend_launches"])},
         "kernel_ms_per_step": {k: v / args.steps for k, v in kern.items()},
@@ -381,7 +385,8 @@ def main():
                     "extend_tris": counters["extend_tris"] / max(1, counters["extend_rays"]),
                     "shadow_nodes": (counters["nodes"] - counters["extend_nodes"]) / max(1, counters["shadow_rays"]),
                     "shadow_tris": (counters["tris"] - counters["extend_tris"]) / max(1, counters["shadow_rays"])},
-        "nan_samples": counters["nan"], "paths_ended_by_nan_throughput": counters["nan_history"],
+        "nan_samples_per_step": counters["nan"] / args.steps,
+        "paths_ended_by_nan_throughput_per_step": counters["nan_history"] / args.steps,
         "launches_per_step": launches_per_step,
         "clocks": clk.summary(),
     }

@@ -124,6 +124,8 @@ public:
     void AddEnv(const std::vector<float>& rgba, int width, int height, float scale = 1.0f) {
         check(rt_scene_set_env(h_, rgba.data(), width, height, scale));
     }
+    // Scene::AddEnv(fileName) (Scene.cpp:79-81): a Radiance .hdr (or LDR) file.
+    void AddEnv(const std::string& path, float scale = 1.0f) { check(rt_scene_set_env_file(h_, path.c_str(), scale)); }
     // SceneParser::LoadFromJson (SceneParser.cpp:3-23), returning the settings.
     void LoadFromJson(const std::string& path, Options& opts, Camera& cam) {
         check(rt_scene_load_json(h_, path.c_str(), &opts, &cam));

@@ -216,6 +216,7 @@ typedef struct rt_render_stats {
     int64_t wave_paths;        /* path slots per wave of the last Render() */
     int64_t h2d_bytes;         /* bytes copied host to device by the last Render() */
     int64_t watchdog_walks;    /* grid-medium walks that hit the device step budget (see rt_renderer_synchronize) */
+    int64_t stack_overflows;   /* traversal node groups that found the stack full (0 unless the BVH depth check fails) */
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */
@@ -277,11 +278,25 @@ RT_API rt_status rt_scene_get_texture(const rt_scene* s, int32_t texture_id, int
  * an equirectangular RGBA float image (w*h*4 floats, row 0 = bottom) scaled
  * by `scale`; the sampling cache is built as in CalculateHdrCache. */
 RT_API rt_status rt_scene_set_env(rt_scene* s, const float* rgba, int32_t width, int32_t height, float scale);
+/* Scene::AddEnv(const std::string& fileName), core/src/Scene.cpp:79-81 with
+ * HdrTexture's loader (Scene.cpp:197-206: stbi_loadf, rows flipped so row 0
+ * is the bottom): a Radiance .hdr file as floats, or a PNG / baseline JPEG /
+ * BMP / PGM / PPM image converted as stbi_loadf does (colour (v/255)^2.2,
+ * alpha v/255), scaled by `scale`.  Unreadable files give RT_ERR_IO (the
+ * reference leaves the scene without an environment). */
+RT_API rt_status rt_scene_set_env_file(rt_scene* s, const char* path, float scale);
+/* The scene's environment image (width*height*4 floats, row 0 = bottom, scale
+ * applied); `rgba` may be NULL to query the size (0 x 0: no environment). */
+RT_API rt_status rt_scene_get_env(const rt_scene* s, float* rgba, int32_t* width, int32_t* height);
 /* Scene::bounds, core/include/Scene.h:213 */
 RT_API rt_status rt_scene_get_bounds(const rt_scene* s, float lo[3], float hi[3]);
 RT_API rt_status rt_scene_counts(const rt_scene* s, int64_t* triangles, int32_t* meshes, int32_t* lights,
                                  int32_t* media);
 enum { RT_BVH_GPU = 0, RT_BVH_HOST = 1 };
+/* Deepest wide BVH (levels) the traversal stack holds; deeper trees are
+ * rejected with RT_ERR_UNSUPPORTED by the builds below and by renderers and
+ * servers when they upload a scene. */
+enum { RT_MAX_BVH_DEPTH = 32 };
 
 /* The same acceleration structure built on the current device (binned SAH on
  * all SMs, then the collapse), copied back and validated on the host. */
@@ -289,7 +304,8 @@ RT_API rt_status rt_scene_build_bvh_gpu(const rt_scene* s, int64_t* num_nodes, i
 /* Builds the acceleration structure (the work of optixAccelBuild,
  * core/src/Renderer.cpp:146-285) on the host and validates it: every child and
  * triangle index in range, every quantised box containing what it bounds.
- * Needs no device. */
+ * Needs no device.  `num_nodes` and `depth` are written also when the tree is
+ * rejected for being deeper than RT_MAX_BVH_DEPTH. */
 RT_API rt_status rt_scene_build_bvh(const rt_scene* s, int64_t* num_nodes, int32_t* depth);
 /* SceneParser::LoadFromJson, core/src/SceneParser.cpp:3-23 and the schema of
  * models/test.json.  Fills `opts`/`cam` (may be NULL) from the file. */
@@ -323,7 +339,9 @@ RT_API rt_status rt_renderer_render(rt_renderer* r);
  * a grid medium in the last render exhausted the device's step budget (4096
  * tentative collisions) and was ended with zero weight; the image is complete
  * but those samples are missing (the reference's equivalent is a hung or
- * timed-out launch). */
+ * timed-out launch).  The same status reports traversals that found their
+ * 32-entry stack full (rt_render_stats.stack_overflows; renderers reject
+ * BVHs deeper than RT_MAX_BVH_DEPTH, so this stays zero). */
 RT_API rt_status rt_renderer_synchronize(rt_renderer* r);
 /* Renderer::DownloadPixels, core/src/Renderer.cpp:878-880 (RGBA8). */
 RT_API rt_status rt_renderer_download_rgba8(rt_renderer* r, uint32_t* pixels);
@@ -367,6 +385,24 @@ RT_API rt_status rt_renderer_guide_samples(rt_renderer* r, float* out, int64_t m
 RT_API rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
                                    int32_t device_ptrs);
 
+/* The queries of rt_renderer_trace (host buffers), answered by the path
+ * tracer's own persistent traversal kernels instead of a one-thread-per-ray
+ * kernel: the batch becomes the extend queue (closest hit) or the shadow
+ * queue (any hit) of a one-bounce wave, and the kernels Render() launches for
+ * devicePrograms.cu:258-269 and :303-319 run on it with the same launch
+ * shape, lane refill and triangle postponing.  Every ray must have tmin =
+ * 1e-4 (EPS, core/cuda/Utils.h:10, the offset of every ray the integrator
+ * traces) and closest-hit rays tmax = FLT_MAX or +inf (the extend kernel's
+ * extent); any-hit rays keep their own tmax.  Other extents give
+ * RT_ERR_INVALID_ARG.  hits: as rt_renderer_trace for closest hits; an
+ * occluded any-hit ray gives (0, 0, 0, 1 bits), a miss (FLT_MAX, 0, 0, -1
+ * bits).  `counters` (NULL, or 3 values) receives rays traced, wide nodes
+ * visited and triangles tested, counted by the instrumented build of the same
+ * kernel (the one rt_options.collect_stats renders with).  Batches above 2^22
+ * rays run as several waves.  Returns after the hits are in `hits`. */
+RT_API rt_status rt_renderer_trace_wavefront(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n,
+                                             float* hits, int64_t* counters);
+
 /* rt_renderer_trace with host buffers, for callers that must not allocate
  * device memory during the call (no counterpart in the reference).
  * cudaMalloc and cudaFree, which rt_renderer_trace uses for its per-call
@@ -375,12 +411,16 @@ RT_API rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float*
  * device memory for its own pool.  This call allocates nothing: the rays and
  * hits pass through one fixed device array per device (65,536 rays, 3 MiB),
  * and larger batches are rejected with RT_ERR_INVALID_ARG.  Nothing in the
- * array needs to start at zero.  The first call on each device looks up the
- * array's address (cudaGetSymbolAddress); make that first call outside any
- * stream capture.  Calls on one device share the array: calls that overlap
- * in time (several host threads, or several renderers on one device) race on
- * it and may return each other's hits, so serialise them.  Returns after the
- * hits are in `hits` (the renderer's stream is synchronised). */
+ * array needs to start at zero.  Every call works on the array of the
+ * renderer's own device (the device it was created on), whichever device is
+ * current on the calling thread, and looks up the array's address there
+ * (cudaGetSymbolAddress, which allocates nothing); the first call on a device
+ * may also load the library's kernels onto it, so make that first call
+ * outside any stream capture.  Calls on one device share the array: calls
+ * that overlap in time (several host threads, or several renderers on one
+ * device) race on it and may return each other's hits, so serialise them.
+ * Returns after the hits are in `hits` (the renderer's stream is
+ * synchronised). */
 RT_API rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n,
                                            float* hits);
 
@@ -492,11 +532,13 @@ typedef struct rt_server_stats {
     int64_t waves, paths;
     int64_t bytes_in_use, bytes_budget;
     int32_t max_segments_in_a_wave;
-    int32_t pad;
+    int32_t device;            /* the CUDA device the server was created on (and works on) */
     double busy_ms;            /* device time of the finished waves (CUDA events) */
     double mean_wave_depth;    /* bounces launched per wave, averaged */
     int64_t guided_waves;      /* waves of guided jobs, training waves included */
     int64_t training_waves;    /* guided waves followed by training steps */
+    int32_t worker_device;     /* current device of the background thread (-1: manual mode or not started) */
+    int32_t pad;
 } rt_server_stats;
 
 RT_API void rt_server_options_default(rt_server_options* o);

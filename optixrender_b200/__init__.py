@@ -88,7 +88,7 @@ class RenderStats(C.Structure):
                 ("launches", C.c_int32), ("ms_total", C.c_float), ("ms_extend", C.c_float),
                 ("ms_shade", C.c_float), ("ms_shadow", C.c_float), ("ms_other", C.c_float),
                 ("extend_launches", C.c_int64), ("nan_throughput_paths", C.c_int64), ("wave_paths", C.c_int64),
-                ("h2d_bytes", C.c_int64), ("watchdog_walks", C.c_int64)]
+                ("h2d_bytes", C.c_int64), ("watchdog_walks", C.c_int64), ("stack_overflows", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -123,8 +123,9 @@ class ServerStats(C.Structure):
     _fields_ = [("jobs_submitted", C.c_int64), ("jobs_done", C.c_int64), ("jobs_queued", C.c_int64),
                 ("jobs_running", C.c_int64), ("waves", C.c_int64), ("paths", C.c_int64),
                 ("bytes_in_use", C.c_int64), ("bytes_budget", C.c_int64), ("max_segments_in_a_wave", C.c_int32),
-                ("pad", C.c_int32), ("busy_ms", C.c_double), ("mean_wave_depth", C.c_double),
-                ("guided_waves", C.c_int64), ("training_waves", C.c_int64)]
+                ("device", C.c_int32), ("busy_ms", C.c_double), ("mean_wave_depth", C.c_double),
+                ("guided_waves", C.c_int64), ("training_waves", C.c_int64), ("worker_device", C.c_int32),
+                ("pad", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
@@ -168,6 +169,8 @@ def load_library():
         "rt_scene_add_light": (I32, [VP, P(Light)]),
         "rt_scene_add_medium": (I32, [VP, P(Medium)]),
         "rt_scene_set_env": (I32, [VP, P(F), I32, I32, F]),
+        "rt_scene_set_env_file": (I32, [VP, C.c_char_p, F]),
+        "rt_scene_get_env": (I32, [VP, P(F), P(I32), P(I32)]),
         "rt_scene_add_texture": (I32, [VP, P(C.c_uint8), I32, I32, P(I32)]),
         "rt_scene_add_texture_file": (I32, [VP, C.c_char_p, P(I32)]),
         "rt_scene_get_texture": (I32, [VP, I32, P(I32), P(I32), P(C.c_uint8)]),
@@ -193,6 +196,7 @@ def load_library():
         "rt_renderer_get_stats": (I32, [VP, P(RenderStats)]),
         "rt_renderer_frame_index": (I32, [VP, P(I32)]),
         "rt_renderer_trace": (I32, [VP, I32, VP, I64, VP, I32]),
+        "rt_renderer_trace_wavefront": (I32, [VP, I32, VP, I64, VP, P(I64)]),
         "rt_denoise_image": (I32, [P(F), P(F), P(F), I32, I32, P(F)]),
         "rt_write_png": (I32, [C.c_char_p, P(C.c_uint32), I32, I32]),
         "rt_verify_shading": (I32, [I32, P(Material), I32, P(Light), I32, P(Medium), I32, P(F), I64, P(F)]),
@@ -372,6 +376,20 @@ class Scene:
                                               a.shape[0], C.byref(tid)))
         return tid.value
 
+    def set_env_file(self, path, scale=1.0):
+        """Scene::AddEnv(fileName) (core/src/Scene.cpp:79-81): a Radiance .hdr or LDR image file."""
+        _check(self._lib.rt_scene_set_env_file(self._h, os.fsencode(str(path)), float(scale)))
+
+    def get_env(self):
+        """The environment image, (H, W, 4) float32 with row 0 at the bottom (None: no environment)."""
+        w, h = C.c_int32(), C.c_int32()
+        _check(self._lib.rt_scene_get_env(self._h, None, C.byref(w), C.byref(h)))
+        if w.value <= 0:
+            return None
+        out = np.empty((h.value, w.value, 4), np.float32)
+        _check(self._lib.rt_scene_get_env(self._h, _fptr(out), C.byref(w), C.byref(h)))
+        return out
+
     def add_texture_file(self, path):
         tid = C.c_int32()
         _check(self._lib.rt_scene_add_texture_file(self._h, str(path).encode(), C.byref(tid)))
@@ -543,6 +561,17 @@ class Renderer:
         _check(self._lib.rt_renderer_trace(self._h, 1 if any_hit else 0, r.ctypes.data, r.shape[0],
                                            out.ctypes.data, 0))
         return out
+
+    def trace_wavefront(self, rays, any_hit=False, counters=False):
+        """The same queries answered by the path tracer's persistent extend (closest hit) or shadow
+        (any hit) kernel; rays need tmin = 1e-4 (and tmax = FLT_MAX for closest hits).  With
+        `counters`, also returns (rays, wide nodes visited, triangles tested)."""
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        out = np.empty((r.shape[0], 4), dtype=np.float32)
+        cnt = (C.c_int64 * 3)()
+        _check(self._lib.rt_renderer_trace_wavefront(self._h, 1 if any_hit else 0, r.ctypes.data, r.shape[0],
+                                                     out.ctypes.data, cnt if counters else None))
+        return (out, tuple(int(v) for v in cnt)) if counters else out
 
     def guide_samples(self, max_samples=1 << 22):
         """The last training wave's samples: (n, 8) = input position, weight, direction, 1."""

@@ -58,6 +58,17 @@ struct Node2 {
 constexpr int kBins = 32;
 constexpr int kMaxLeaf = 3;
 
+// Bin of a centroid coordinate, saturating like the device build's float to
+// int conversion: a node whose centroid extent is so small that kBins / extent
+// overflows to infinity gives NaN (c == cmin) or infinity here, and both must
+// land in a valid bin.
+inline int bin_of(float c, float cmin, float scale) {
+    const float f = (c - cmin) * scale;
+    if (!(f > 0.0f)) return 0;  // also NaN
+    if (f >= float(kBins - 1)) return kBins - 1;
+    return int(f);
+}
+
 struct Builder {
     const float* tv;
     std::vector<Box> pbox;
@@ -122,7 +133,7 @@ struct Builder {
             }
             for (int i = first; i < first + count; i++) {
                 int p = prims[size_t(i)];
-                int k = std::min(kBins - 1, int((cen[size_t(p) * 3 + a] - cb.lo[a]) * scale));
+                int k = bin_of(cen[size_t(p) * 3 + a], cb.lo[a], scale);
                 bb[k].grow(pbox[size_t(p)]);
                 bc[k]++;
             }
@@ -163,8 +174,7 @@ struct Builder {
             float scale = float(kBins) / (cb.hi[a] - cb.lo[a]);
             float lo = cb.lo[a];
             auto it = std::partition(prims.begin() + first, prims.begin() + first + count, [&](int p) {
-                int k = std::min(kBins - 1, int((cen[size_t(p) * 3 + a] - lo) * scale));
-                return k < best_split;
+                return bin_of(cen[size_t(p) * 3 + a], lo, scale) < best_split;
             });
             mid = int(it - prims.begin());
             if (mid == first || mid == first + count) mid = first + count / 2;

@@ -30,6 +30,13 @@ rt_status fail(rt_status code, const std::string& msg) {
     return code;
 }
 
+rt_status check_bvh_depth(int depth) {
+    static_assert(RT_MAX_BVH_DEPTH == rtd::kStackSize, "the traversal stack bounds the BVH depth");
+    if (depth <= RT_MAX_BVH_DEPTH) return RT_OK;
+    return fail(RT_ERR_UNSUPPORTED, "BVH too deep for the traversal stack (" + std::to_string(depth) + " levels, at most " +
+                                        std::to_string(RT_MAX_BVH_DEPTH) + ")");
+}
+
 rt_status cuda_fail(cudaError_t e, const char* what) {
     g_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
     return e == cudaErrorMemoryAllocation ? RT_ERR_OUT_OF_MEMORY : RT_ERR_CUDA;
@@ -400,7 +407,7 @@ rt_status rt_scene_build_bvh(const rt_scene* s, int64_t* num_nodes, int32_t* dep
         return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
     if (num_nodes) *num_nodes = int64_t(bvh.nodes.size());
     if (depth) *depth = bvh.depth;
-    return RT_OK;
+    return check_bvh_depth(bvh.depth);
 }
 
 rt_status rt_scene_build_bvh_gpu(const rt_scene* s, int64_t* num_nodes, int32_t* depth) {
@@ -412,7 +419,7 @@ rt_status rt_scene_build_bvh_gpu(const rt_scene* s, int64_t* num_nodes, int32_t*
     if (!rth::validate_cwbvh(bvh, s->tv.data(), nt, err)) return fail(RT_ERR_UNSUPPORTED, "GPU BVH invalid: " + err);
     if (num_nodes) *num_nodes = int64_t(bvh.nodes.size());
     if (depth) *depth = bvh.depth;
-    return RT_OK;
+    return check_bvh_depth(bvh.depth);
 }
 
 // ====================================================================== tables

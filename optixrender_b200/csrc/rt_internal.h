@@ -35,6 +35,31 @@ namespace rti {
 extern thread_local std::string g_error;
 rt_status fail(rt_status code, const std::string& msg);
 rt_status cuda_fail(cudaError_t e, const char* what);
+// RT_ERR_UNSUPPORTED when a wide BVH is deeper than the traversal stack.
+rt_status check_bvh_depth(int depth);
+
+// Makes `dev` the calling thread's current device for the guard's scope and
+// restores the previous device afterwards.  Renderers and servers remember
+// the device they were created on; every entry point that touches device
+// memory or launches work takes this guard, so a call from a thread whose
+// current device is another GPU still works on the object's own device.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t status = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        int cur = -1;
+        status = cudaGetDevice(&cur);
+        if (status == cudaSuccess && cur != dev) {
+            status = cudaSetDevice(dev);
+            if (status == cudaSuccess) prev = cur;
+        }
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
 
 struct DevBuf {
     void* ptr = nullptr;

@@ -15,6 +15,7 @@
 // the next shade (or in resolve) in the reference's order: environment, then
 // light.  extend/shade/shadow are persistent kernels: each warp takes 32
 // queue entries at a time with one atomicAdd.
+#include <algorithm>
 #include <cstdio>
 
 #include "rt_kernels.cuh"
@@ -162,9 +163,10 @@ __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_extend(Ctx c) {
         ctl->fetch_shade = 0;
     }
     const int total = ctl->count[cur];
-    uint32_t nodes = 0, tris = 0, rays = 0;
+    uint32_t nodes = 0, tris = 0, rays = 0, overflows = 0;
     ExtendSrc src{&c, c.wb.queue[cur]};
-    traverse_queue<false, Stats>(src, &ctl->fetch_ext, total, nodes, tris, rays);
+    traverse_queue<false, Stats>(src, &ctl->fetch_ext, total, nodes, tris, rays, overflows);
+    if (overflows) atomicAdd(&ctl->overflow, int(overflows));
     if (Stats) {
         warp_stat(&ctl->stats[0], rays);
         warp_stat(&ctl->stats[2], nodes);
@@ -638,9 +640,10 @@ __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_shadow(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     if (blockIdx.x == 0 && threadIdx.x < kShadeBuckets) ctl->bucket[threadIdx.x] = 0;  // for the next extend
     const int total = ctl->shadow_count;
-    uint32_t nodes = 0, tris = 0, rays = 0;
+    uint32_t nodes = 0, tris = 0, rays = 0, overflows = 0;
     ShadowSrc src{&c};
-    traverse_queue<true, Stats>(src, &ctl->fetch_shadow, total, nodes, tris, rays);
+    traverse_queue<true, Stats>(src, &ctl->fetch_shadow, total, nodes, tris, rays, overflows);
+    if (overflows) atomicAdd(&ctl->overflow, int(overflows));
     if (Stats) {
         warp_stat(&ctl->stats[1], rays);
         warp_stat(&ctl->stats[4], nodes);
@@ -868,7 +871,7 @@ __global__ void k_dn_remod(const float4* __restrict__ irr, const float4* __restr
 // ------------------------------------------------------------------ ray queries
 template <bool AnyHit>
 __global__ void __launch_bounds__(kBlock) k_trace(SceneView sc, const float* __restrict__ rays, int64_t n,
-                                                  float* __restrict__ hits) {
+                                                  float* __restrict__ hits, int* overflow) {
     int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4* rr = reinterpret_cast<const float4*>(rays) + i * 2;
@@ -880,8 +883,9 @@ __global__ void __launch_bounds__(kBlock) k_trace(SceneView sc, const float* __r
     r.tmax = b.w;
     prepare_ray(r);
     float t = FLT_MAX, b1 = 0.f, b2 = 0.f;
-    uint32_t nv = 0, nt = 0;
-    int tri = traverse<AnyHit, false>(sc, r, t, b1, b2, nv, nt);
+    uint32_t nv = 0, nt = 0, ovf = 0;
+    int tri = traverse<AnyHit, false>(sc, r, t, b1, b2, nv, nt, ovf);
+    if (ovf) atomicAdd(overflow, int(ovf));
     float4 out;
     if (tri < 0) {
         out = make_float4(FLT_MAX, 0.f, 0.f, __int_as_float(-1));
@@ -892,6 +896,62 @@ __global__ void __launch_bounds__(kBlock) k_trace(SceneView sc, const float* __r
         out = make_float4(t, b1, b2, __int_as_float(orig));
     }
     reinterpret_cast<float4*>(hits)[i] = out;
+}
+
+// ------------------------------------------------------------------ wavefront ray queries
+// Stages n query rays (2 float4 each: origin + tmin, direction + tmax) as one
+// wave of the path-tracing kernels: closest-hit queries become the extend
+// queue of bounce 0 (slot i = ray i), any-hit queries become the shadow queue
+// with a unit pending contribution in nee0[i] that k_shadow clears when the
+// ray is occluded.  Resets the wave's counters as k_raygen does.
+__global__ void k_query_stage(Ctx c, const float4* __restrict__ rays, int n, int any_hit) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const WaveBufs& b = c.wb;
+    WaveCtl* ctl = b.ctl;
+    if (i == 0) {
+        ctl->count[0] = any_hit ? 0 : n;
+        ctl->count[1] = 0;
+        ctl->shadow_count = any_hit ? n : 0;
+        ctl->fetch_ext = 0;
+        ctl->fetch_shade = 0;
+        ctl->fetch_shadow = 0;
+        ctl->error = 0;
+        ctl->overflow = 0;
+        for (int k = 0; k < 8; k++) ctl->stats[k] = 0ull;
+        for (int k = 0; k < kShadeBuckets; k++) ctl->bucket[k] = 0;
+    }
+    if (i >= n) return;
+    const float4 o = rays[2 * i], d = rays[2 * i + 1];
+    if (!any_hit) {
+        b.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
+        b.ray_d[i] = make_float4(d.x, d.y, d.z, 0.0f);
+        b.queue[0][i] = i;
+    } else {
+        b.sh_o[i] = make_float4(o.x, o.y, o.z, d.w);
+        b.sh_d[i] = make_float4(d.x, d.y, d.z, __int_as_float(i * 2));
+        b.nee0[i] = make_float4(1.f, 1.f, 1.f, 0.f);
+    }
+}
+
+// Hits of a query wave in the layout of k_trace: (t, b1, b2, original
+// triangle id) for closest hits, (0, 0, 0, 1) for an occluded any-hit ray and
+// (FLT_MAX, 0, 0, -1) for a miss.
+__global__ void k_query_collect(Ctx c, SceneView sc, float4* __restrict__ out, int n, int any_hit) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const WaveBufs& b = c.wb;
+    const float4 miss = make_float4(FLT_MAX, 0.f, 0.f, __int_as_float(-1));
+    if (any_hit) {
+        out[i] = b.nee0[i].x == 0.0f ? make_float4(0.f, 0.f, 0.f, __int_as_float(1)) : miss;
+        return;
+    }
+    const float4 h = b.hit[i];
+    const int tri = __float_as_int(h.w);
+    if (tri < 0) {
+        out[i] = miss;
+        return;
+    }
+    out[i] = make_float4(h.x, h.y, h.z, __ldg(sc.tri_v + size_t(tri) * 3).w);
 }
 
 // ------------------------------------------------------------------ verification
@@ -1067,12 +1127,21 @@ int launch_denoise(const DenoiseArgs& d, cudaStream_t st) {
     k_dn_remod<<<grid_for(n, 256), 256, 0, st>>>(src, d.albedo, d.out, d.rgba8, n, d.tonemap, d.exposure);
     return kDenoisePasses + 3;
 }
-void launch_trace(const SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st) {
+void launch_trace(const SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, int* overflow,
+                  cudaStream_t st) {
     if (n <= 0) return;
     if (any_hit)
-        k_trace<true><<<grid_for(n, kBlock), kBlock, 0, st>>>(sc, rays, n, hits);
+        k_trace<true><<<grid_for(n, kBlock), kBlock, 0, st>>>(sc, rays, n, hits, overflow);
     else
-        k_trace<false><<<grid_for(n, kBlock), kBlock, 0, st>>>(sc, rays, n, hits);
+        k_trace<false><<<grid_for(n, kBlock), kBlock, 0, st>>>(sc, rays, n, hits, overflow);
+}
+void launch_query_stage(const Ctx& c, const float* rays, int n, bool any_hit, cudaStream_t st) {
+    k_query_stage<<<grid_for(std::max(n, 1), 256), 256, 0, st>>>(c, reinterpret_cast<const float4*>(rays), n,
+                                                                  any_hit ? 1 : 0);
+}
+void launch_query_collect(const Ctx& c, const SceneView& sc, float* hits, int n, bool any_hit, cudaStream_t st) {
+    if (n <= 0) return;
+    k_query_collect<<<grid_for(n, 256), 256, 0, st>>>(c, sc, reinterpret_cast<float4*>(hits), n, any_hit ? 1 : 0);
 }
 void launch_verify(int op, const SceneView& sc, const DevLight* lights, const DevMedium* media, const float* in,
                    int64_t n, float* out, cudaStream_t st) {

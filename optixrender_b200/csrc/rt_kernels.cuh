@@ -55,8 +55,8 @@ struct WaveCtl {
     int fetch_ext;
     int fetch_shade;
     int fetch_shadow;
-    int error;  // media walks that exhausted their step budget in this render
-    int pad;
+    int error;     // media walks that exhausted their step budget in this render
+    int overflow;  // traversal node groups that found the stack full (the BVH depth check keeps this 0)
     unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris,
                                   // NaN samples, paths ended by a NaN throughput
     int bucket[kShadeBuckets];    // extend results per shade bucket
@@ -155,11 +155,19 @@ void launch_next_wave(const rtd::Ctx& c, cudaStream_t st);
 void launch_finalize(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);
 void launch_begin_n(const rtd::JobDesc* dev_job, int64_t npix, cudaStream_t st);
 void launch_finalize_n(const rtd::JobDesc* dev_job, int64_t npix, cudaStream_t st);
-void launch_trace(const rtd::SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, cudaStream_t st);
+// Per-thread ray queries; `overflow` (device int) counts traversal stack overflows.
+void launch_trace(const rtd::SceneView& sc, bool any_hit, const float* rays, int64_t n, float* hits, int* overflow,
+                  cudaStream_t st);
+// Ray queries through the wavefront kernels: stage n rays (8 floats each, device)
+// as the extend queue (closest hit) or the shadow queue (any hit) of a wave,
+// run launch_extend / launch_shadow, then collect the hits (4 floats each, device).
+void launch_query_stage(const rtd::Ctx& c, const float* rays, int n, bool any_hit, cudaStream_t st);
+void launch_query_collect(const rtd::Ctx& c, const rtd::SceneView& sc, float* hits, int n, bool any_hit,
+                          cudaStream_t st);
 void launch_verify(int op, const rtd::SceneView& sc, const rtd::DevLight* lights, const rtd::DevMedium* media,
                    const float* in, int64_t n, float* out, cudaStream_t st);
 // rt_trace_scratch.cu: ray queries staged in a fixed device array.
 int64_t trace_scratch_rays();
-cudaError_t trace_scratch_address(void** ptr);
-void launch_trace_scratch(const rtd::SceneView& sc, bool any_hit, void* scratch, int n, cudaStream_t st);
+cudaError_t trace_scratch_address(int device, void** ptr);
+void launch_trace_scratch(const rtd::SceneView& sc, bool any_hit, void* scratch, int n, int* overflow, cudaStream_t st);
 }  // namespace rth

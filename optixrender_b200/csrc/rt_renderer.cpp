@@ -33,6 +33,11 @@ DeviceScene::~DeviceScene() {
         if (e_ != cudaSuccess) return cuda_fail(e_, what); \
     } while (0)
 
+// The renderer's device current for the rest of the calling scope.
+#define RT_ON_DEVICE(rr, what)                                         \
+    DeviceGuard dg_((rr)->device);                                     \
+    if (dg_.status != cudaSuccess) return cuda_fail(dg_.status, what)
+
 // Per majorant cell, the largest density any trilinear lookup inside the cell
 // can return: the maximum over the voxels within one voxel of the cell.
 void grid_majorants(const float* dens, const int res[3], int mres, std::vector<float>& out) {
@@ -63,8 +68,7 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st, bool
     } else if (!rth::build_cwbvh_gpu(s.tv.data(), nt, bvh, err, st)) {
         return fail(RT_ERR_CUDA, err);
     }
-    if (bvh.depth > kStackSize)
-        return fail(RT_ERR_UNSUPPORTED, "BVH too deep for the traversal stack (" + std::to_string(bvh.depth) + " levels)");
+    if (rt_status dst = check_bvh_depth(bvh.depth)) return dst;
     ds.bvh_depth = bvh.depth;
     std::vector<float4> tv(size_t(nt) * 3), ta(size_t(nt) * 4);
     for (int64_t t = 0; t < nt; t++) {
@@ -223,6 +227,7 @@ struct rt_renderer {
     int wave_paths = 0;       // slots per wave of the last render
     int64_t h2d_bytes = 0;    // host-to-device bytes of the last render
     DevBuf wave_index;
+    DevBuf q_job, q_wave, q_index, q_ctl;  // rt_renderer_trace_wavefront: its job, wave table and counters
     // one captured wave (raygen, (extend, shade, shadow) x depth, resolve, advance)
     cudaGraphExec_t graph = nullptr;
     int graph_capacity = -1, graph_depth = -1, graph_ring = -1;
@@ -300,6 +305,29 @@ rt_status ensure_waves(rt_renderer* r, int cap) {
     return RT_OK;
 }
 
+// The renderer's per-slot path state as the kernels see it.
+void wave_bufs(rt_renderer* r, WaveBufs& b) {
+    b.ray_o = r->ray_o.as<float4>();
+    b.ray_d = r->ray_d.as<float4>();
+    b.hit = r->hit.as<float4>();
+    b.thr = r->thr.as<float4>();
+    b.rad = r->rad.as<float4>();
+    b.nee0 = r->nee0.as<float4>();
+    b.nee1 = r->nee1.as<float4>();
+    b.stale = r->stale.as<float4>();
+    b.aov_a = r->aov_a.as<float4>();
+    b.aov_n = r->aov_n.as<float2>();
+    b.rng = r->rng.as<uint2>();
+    b.queue[0] = r->q0.as<int>();
+    b.queue[1] = r->q1.as<int>();
+    b.sh_o = r->sh_o.as<float4>();
+    b.sh_d = r->sh_d.as<float4>();
+    b.sorted = r->sort_shade ? r->sorted.as<int>() : nullptr;
+    b.mat_tex = r->ds.view.num_tex > 0 ? r->mat_tex.as<DevMaterial>() : nullptr;
+    b.ctl = r->ctl.as<WaveCtl>();
+    b.capacity = r->capacity;
+}
+
 int auto_capacity(const rt_options& o, int64_t npix, int64_t total) {
     // Large waves: the last bounces of a wave carry few paths and run at the
     // latency of a handful of rays, so fewer, larger waves spend less time
@@ -346,6 +374,18 @@ rt_status ensure_guide(rt_renderer* r, int cap, int64_t train_slots) {
         }
     }
     return RT_OK;
+}
+
+// The traversal stack-overflow counter of the renderer's control block.
+int* overflow_counter(rt_renderer* r) {
+    return reinterpret_cast<int*>(static_cast<char*>(r->ctl.ptr) + offsetof(WaveCtl, overflow));
+}
+
+rt_status overflow_status(int n, const char* what) {
+    if (n <= 0) return RT_OK;
+    return fail(RT_ERR_DEVICE_WATCHDOG, std::string(what) + ": " + std::to_string(n) +
+                                            " traversal node groups found the " + std::to_string(kStackSize) +
+                                            "-entry stack full; their subtrees were not visited");
 }
 
 rt_status check_options(const rt_options* o) {
@@ -413,6 +453,7 @@ rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_rende
 
 rt_status rt_renderer_destroy(rt_renderer* r) {
     if (!r) return RT_OK;
+    RT_ON_DEVICE(r, "rt_renderer_destroy");
     if (r->stream) cudaStreamSynchronize(r->stream);
     if (r->graph) cudaGraphExecDestroy(r->graph);
     if (r->guide) rt_guide_destroy(r->guide);
@@ -425,6 +466,7 @@ rt_status rt_renderer_destroy(rt_renderer* r) {
 
 rt_status rt_renderer_set_options(rt_renderer* r, const rt_options* o) {
     if (!r || !o) return fail(RT_ERR_INVALID_ARG, "rt_renderer_set_options: NULL argument");
+    RT_ON_DEVICE(r, "rt_renderer_set_options");
     rt_status st = check_options(o);
     if (st) return st;
     int w = r->opt.width, h = r->opt.height;
@@ -441,6 +483,7 @@ rt_status rt_renderer_get_options(const rt_renderer* r, rt_options* o) {
 
 rt_status rt_renderer_resize(rt_renderer* r, int32_t w, int32_t h) {
     if (!r || w < 0 || h < 0) return fail(RT_ERR_INVALID_ARG, "rt_renderer_resize: bad argument");
+    RT_ON_DEVICE(r, "rt_renderer_resize");
     r->opt.width = w;
     r->opt.height = h;
     if (w > 0 && h > 0) {
@@ -460,6 +503,7 @@ rt_status rt_renderer_set_camera(rt_renderer* r, const rt_camera* c) {
 
 rt_status rt_renderer_set_stream(rt_renderer* r, void* s) {
     if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_set_stream: NULL renderer");
+    RT_ON_DEVICE(r, "rt_renderer_set_stream");
     cudaStreamSynchronize(r->stream);
     if (r->own_stream) cudaStreamDestroy(r->stream);
     if (s) {
@@ -475,6 +519,7 @@ rt_status rt_renderer_set_stream(rt_renderer* r, void* s) {
 
 rt_status rt_renderer_render(rt_renderer* r) {
     if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_render: NULL renderer");
+    RT_ON_DEVICE(r, "rt_renderer_render");
     const rt_options& o = r->opt;
     if (o.width <= 0 || o.height <= 0) return RT_OK;  // Renderer.cpp:638-640
     rt_status st = ensure_pixels(r, o.width, o.height);
@@ -558,26 +603,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
     Ctx c;
     std::memset(&c, 0, sizeof(c));
     c.jobs = dj;
-    WaveBufs& b = c.wb;
-    b.ray_o = r->ray_o.as<float4>();
-    b.ray_d = r->ray_d.as<float4>();
-    b.hit = r->hit.as<float4>();
-    b.thr = r->thr.as<float4>();
-    b.rad = r->rad.as<float4>();
-    b.nee0 = r->nee0.as<float4>();
-    b.nee1 = r->nee1.as<float4>();
-    b.stale = r->stale.as<float4>();
-    b.aov_a = r->aov_a.as<float4>();
-    b.aov_n = r->aov_n.as<float2>();
-    b.rng = r->rng.as<uint2>();
-    b.queue[0] = r->q0.as<int>();
-    b.queue[1] = r->q1.as<int>();
-    b.sh_o = r->sh_o.as<float4>();
-    b.sh_d = r->sh_d.as<float4>();
-    b.sorted = r->sort_shade ? r->sorted.as<int>() : nullptr;
-    b.mat_tex = r->ds.view.num_tex > 0 ? r->mat_tex.as<DevMaterial>() : nullptr;
-    b.ctl = r->ctl.as<WaveCtl>();
-    b.capacity = r->capacity;
+    wave_bufs(r, c.wb);
     c.waves = r->segs.as<WaveParams>();
     c.wave_index = r->wave_index.as<int>();
     c.wave_ring = int(nwaves);
@@ -700,6 +726,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
 
 rt_status rt_renderer_guide(rt_renderer* r, rt_guide** guide) {
     if (!r || !guide) return fail(RT_ERR_INVALID_ARG, "rt_renderer_guide: NULL argument");
+    RT_ON_DEVICE(r, "rt_renderer_guide");
     if (!r->guide) {
         rt_status st = ensure_guide(r, 0, 0);
         if (st) return st;
@@ -710,6 +737,7 @@ rt_status rt_renderer_guide(rt_renderer* r, rt_guide** guide) {
 
 rt_status rt_renderer_guide_samples(rt_renderer* r, float* out, int64_t max_samples, int64_t* count) {
     if (!r || !count) return fail(RT_ERR_INVALID_ARG, "rt_renderer_guide_samples: NULL argument");
+    RT_ON_DEVICE(r, "rt_renderer_guide_samples");
     *count = 0;
     if (!r->g_count.ptr) return RT_OK;
     int n = 0;
@@ -727,22 +755,26 @@ rt_status rt_renderer_guide_samples(rt_renderer* r, float* out, int64_t max_samp
 
 rt_status rt_renderer_synchronize(rt_renderer* r) {
     if (!r) return fail(RT_ERR_INVALID_ARG, "rt_renderer_synchronize: NULL renderer");
+    RT_ON_DEVICE(r, "rt_renderer_synchronize");
     RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_synchronize");
-    if (r->rendered && r->ctl.ptr) {  // the device-side step budget of media walks
-        int hits = 0;
-        RT_CUDA(cudaMemcpy(&hits, static_cast<char*>(r->ctl.ptr) + offsetof(WaveCtl, error), sizeof(int),
+    if (r->rendered && r->ctl.ptr) {  // the device-side step budget of media walks, traversal stack overflows
+        int hits[2] = {0, 0};
+        static_assert(offsetof(WaveCtl, overflow) == offsetof(WaveCtl, error) + sizeof(int), "counter layout");
+        RT_CUDA(cudaMemcpy(hits, static_cast<char*>(r->ctl.ptr) + offsetof(WaveCtl, error), 2 * sizeof(int),
                            cudaMemcpyDeviceToHost),
                 "rt_renderer_synchronize");
-        if (hits > 0)
+        if (hits[0] > 0)
             return fail(RT_ERR_DEVICE_WATCHDOG,
-                        std::to_string(hits) + " medium walks of the last render ran out of their " +
+                        std::to_string(hits[0]) + " medium walks of the last render ran out of their " +
                             std::to_string(kMaxTrackingSteps) + "-step budget and were ended with zero weight");
+        if (hits[1] > 0) return overflow_status(hits[1], "the last render");
     }
     return RT_OK;
 }
 
 static rt_status download(rt_renderer* r, const DevBuf& b, void* dst, size_t bytes) {
     if (!r || !dst) return fail(RT_ERR_INVALID_ARG, "download: NULL argument");
+    RT_ON_DEVICE(r, "download");
     if (!b.ptr) return fail(RT_ERR_STATE, "download: nothing rendered at this size");
     RT_CUDA(cudaMemcpyAsync(dst, b.ptr, bytes, cudaMemcpyDeviceToHost, r->stream), "download");
     RT_CUDA(cudaStreamSynchronize(r->stream), "download");
@@ -788,6 +820,7 @@ rt_status rt_renderer_frame_index(const rt_renderer* r, int32_t* f) {
 rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     rt_renderer* r = const_cast<rt_renderer*>(rc);
     if (!r || !out) return fail(RT_ERR_INVALID_ARG, "rt_renderer_get_stats: NULL argument");
+    RT_ON_DEVICE(r, "rt_renderer_get_stats");
     std::memset(out, 0, sizeof(*out));
     if (!r->rendered) return RT_OK;
     RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_get_stats");
@@ -803,6 +836,7 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     out->nan_samples = int64_t(ctl.stats[6]);
     out->nan_throughput_paths = int64_t(ctl.stats[7]);
     out->watchdog_walks = int64_t(ctl.error);
+    out->stack_overflows = int64_t(ctl.overflow);
     out->waves = r->waves;
     out->launches = r->launches;
     out->extend_launches = r->extend_launches;
@@ -827,22 +861,111 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
 rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
                             int32_t device_ptrs) {
     if (!r || (n > 0 && (!rays || !hits)) || n < 0) return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace: bad argument");
+    RT_ON_DEVICE(r, "rt_renderer_trace");
     if (n == 0) return RT_OK;
+    int* ovf = overflow_counter(r);
+    int h_ovf = 0;
+    RT_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int), r->stream), "rt_renderer_trace");
     if (device_ptrs) {
-        rth::launch_trace(r->ds.view, any_hit != 0, rays, n, hits, r->stream);
+        rth::launch_trace(r->ds.view, any_hit != 0, rays, n, hits, ovf, r->stream);
         RT_CUDA(cudaGetLastError(), "rt_renderer_trace");
+        RT_CUDA(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, r->stream), "rt_renderer_trace");
         RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace");
-        return RT_OK;
+        return overflow_status(h_ovf, "rt_renderer_trace");
     }
     DevBuf dr, dh;
     RT_CUDA(dr.alloc(size_t(n) * 32), "rt_renderer_trace: allocate");
     RT_CUDA(dh.alloc(size_t(n) * 16), "rt_renderer_trace: allocate");
     RT_CUDA(cudaMemcpyAsync(dr.ptr, rays, size_t(n) * 32, cudaMemcpyHostToDevice, r->stream), "rt_renderer_trace");
-    rth::launch_trace(r->ds.view, any_hit != 0, dr.as<float>(), n, dh.as<float>(), r->stream);
+    rth::launch_trace(r->ds.view, any_hit != 0, dr.as<float>(), n, dh.as<float>(), ovf, r->stream);
     RT_CUDA(cudaGetLastError(), "rt_renderer_trace");
     RT_CUDA(cudaMemcpyAsync(hits, dh.ptr, size_t(n) * 16, cudaMemcpyDeviceToHost, r->stream), "rt_renderer_trace");
+    RT_CUDA(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, r->stream), "rt_renderer_trace");
     RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace");
-    return RT_OK;
+    return overflow_status(h_ovf, "rt_renderer_trace");
+}
+
+// Ray queries through the path tracer's own persistent traversal kernels:
+// the batch is staged as the extend queue (closest hit) or the shadow queue
+// (any hit) of a one-bounce wave and k_extend / k_shadow run on it with the
+// launch shape of Render(), so these hits come from exactly the loop that
+// renders images (lane refill, triangle postponing, near-to-far order).
+rt_status rt_renderer_trace_wavefront(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits,
+                                      int64_t* counters) {
+    if (!r || n < 0 || (n > 0 && (!rays || !hits)))
+        return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace_wavefront: bad argument");
+    RT_ON_DEVICE(r, "rt_renderer_trace_wavefront");
+    if (counters) counters[0] = counters[1] = counters[2] = 0;
+    for (int64_t i = 0; i < n; i++) {  // the kernels' own ray extents
+        const float tmin = rays[i * 8 + 3], tmax = rays[i * 8 + 7];
+        if (tmin != kEps || std::isnan(tmax) || (!any_hit && tmax < FLT_MAX))
+            return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace_wavefront: ray " + std::to_string(i) +
+                                                " must have tmin = 1e-4 (the integrator's ray offset) and, for "
+                                                "closest-hit queries, tmax = FLT_MAX or infinity");
+    }
+    if (n == 0) return RT_OK;
+    constexpr int kChunk = 1 << 22;
+    const int chunk = int(std::min<int64_t>(n, kChunk));
+    rt_status st = ensure_waves(r, chunk);
+    if (st) return st;
+    if (!r->q_job.ptr) {
+        RT_CUDA(r->q_job.alloc(sizeof(JobDesc)), "rt_renderer_trace_wavefront: allocate");
+        RT_CUDA(r->q_wave.alloc(sizeof(WaveParams)), "rt_renderer_trace_wavefront: allocate");
+        RT_CUDA(r->q_index.alloc(sizeof(int)), "rt_renderer_trace_wavefront: allocate");
+        RT_CUDA(r->q_ctl.alloc(sizeof(WaveCtl)), "rt_renderer_trace_wavefront: allocate");
+    }
+    cudaStream_t s = r->stream;
+    JobDesc hj;
+    std::memset(&hj, 0, sizeof(hj));
+    hj.sc = r->ds.view;
+    RT_CUDA(cudaMemcpyAsync(r->q_job.ptr, &hj, sizeof(hj), cudaMemcpyHostToDevice, s), "rt_renderer_trace_wavefront");
+    RT_CUDA(cudaMemsetAsync(r->q_index.ptr, 0, sizeof(int), s), "rt_renderer_trace_wavefront");
+    DevBuf dr, dh;
+    RT_CUDA(dr.alloc(size_t(chunk) * 32), "rt_renderer_trace_wavefront: allocate");
+    RT_CUDA(dh.alloc(size_t(chunk) * 16), "rt_renderer_trace_wavefront: allocate");
+    Ctx c;
+    std::memset(&c, 0, sizeof(c));
+    c.jobs = r->q_job.as<JobDesc>();
+    wave_bufs(r, c.wb);
+    c.wb.ctl = r->q_ctl.as<WaveCtl>();
+    c.waves = r->q_wave.as<WaveParams>();
+    c.wave_index = r->q_index.as<int>();
+    c.wave_ring = 1;
+    c.bounce = 0;
+    c.max_depth = 1;
+    const bool stats = counters != nullptr;
+    int overflows = 0;
+    for (int64_t b0 = 0; b0 < n; b0 += chunk) {
+        const int m = int(std::min<int64_t>(chunk, n - b0));
+        WaveParams wp;
+        std::memset(&wp, 0, sizeof(wp));
+        wp.num_seg = 1;
+        wp.wave_count = m;
+        wp.seg[0].count = m;
+        RT_CUDA(cudaMemcpyAsync(r->q_wave.ptr, &wp, sizeof(wp), cudaMemcpyHostToDevice, s), "rt_renderer_trace_wavefront");
+        RT_CUDA(cudaMemcpyAsync(dr.ptr, rays + b0 * 8, size_t(m) * 32, cudaMemcpyHostToDevice, s),
+                "rt_renderer_trace_wavefront");
+        rth::launch_query_stage(c, dr.as<float>(), m, any_hit != 0, s);
+        if (any_hit)
+            rth::launch_shadow(c, r->shape, stats, s);
+        else
+            rth::launch_extend(c, r->shape, stats, s);
+        rth::launch_query_collect(c, r->ds.view, dh.as<float>(), m, any_hit != 0, s);
+        RT_CUDA(cudaGetLastError(), "rt_renderer_trace_wavefront");
+        RT_CUDA(cudaMemcpyAsync(hits + b0 * 4, dh.ptr, size_t(m) * 16, cudaMemcpyDeviceToHost, s),
+                "rt_renderer_trace_wavefront");
+        WaveCtl ctl;
+        RT_CUDA(cudaMemcpyAsync(&ctl, r->q_ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost, s), "rt_renderer_trace_wavefront");
+        RT_CUDA(cudaStreamSynchronize(s), "rt_renderer_trace_wavefront");
+        overflows += ctl.overflow;
+        if (counters) {
+            const int o = any_hit ? 1 : 0;  // stats: extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris
+            counters[0] += int64_t(ctl.stats[o]);
+            counters[1] += int64_t(ctl.stats[2 + 2 * o]);
+            counters[2] += int64_t(ctl.stats[3 + 2 * o]);
+        }
+    }
+    return overflow_status(overflows, "rt_renderer_trace_wavefront");
 }
 
 // Same queries as rt_renderer_trace with host buffers, staged in the fixed
@@ -850,6 +973,7 @@ rt_status rt_renderer_trace(rt_renderer* r, int32_t any_hit, const float* rays, 
 rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, const float* rays, int64_t n, float* hits) {
     if (!r || n < 0 || (n > 0 && (!rays || !hits)))
         return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace_noalloc: bad argument");
+    RT_ON_DEVICE(r, "rt_renderer_trace_noalloc");
     const int64_t cap = rth::trace_scratch_rays();
     if (n > cap)
         return fail(RT_ERR_INVALID_ARG, "rt_renderer_trace_noalloc: " + std::to_string(n) + " rays exceed the " +
@@ -857,15 +981,19 @@ rt_status rt_renderer_trace_noalloc(rt_renderer* r, int32_t any_hit, const float
                                             " of the static scratch; split the batch or use rt_renderer_trace");
     if (n == 0) return RT_OK;
     void* scratch = nullptr;
-    RT_CUDA(rth::trace_scratch_address(&scratch), "rt_renderer_trace_noalloc: scratch address");
+    RT_CUDA(rth::trace_scratch_address(r->device, &scratch), "rt_renderer_trace_noalloc: scratch address");
     float4* sc = static_cast<float4*>(scratch);
+    int* ovf = overflow_counter(r);  // the renderer's own control block: nothing allocated
+    int h_ovf = 0;
+    RT_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int), r->stream), "rt_renderer_trace_noalloc");
     RT_CUDA(cudaMemcpyAsync(sc, rays, size_t(n) * 32, cudaMemcpyHostToDevice, r->stream), "rt_renderer_trace_noalloc");
-    rth::launch_trace_scratch(r->ds.view, any_hit != 0, scratch, int(n), r->stream);
+    rth::launch_trace_scratch(r->ds.view, any_hit != 0, scratch, int(n), ovf, r->stream);
     RT_CUDA(cudaGetLastError(), "rt_renderer_trace_noalloc");
     RT_CUDA(cudaMemcpyAsync(hits, sc + 2 * cap, size_t(n) * 16, cudaMemcpyDeviceToHost, r->stream),
             "rt_renderer_trace_noalloc");
+    RT_CUDA(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, r->stream), "rt_renderer_trace_noalloc");
     RT_CUDA(cudaStreamSynchronize(r->stream), "rt_renderer_trace_noalloc");
-    return RT_OK;
+    return overflow_status(h_ovf, "rt_renderer_trace_noalloc");
 }
 
 rt_status rt_write_png(const char* path, const uint32_t* rgba8, int32_t w, int32_t h) {

@@ -899,6 +899,45 @@ RT_API rt_status rt_scene_add_texture_file(rt_scene* s, const char* path, int32_
     return rt_scene_add_texture(s, px.data(), w, h, id);
 }
 
+// Scene::AddEnv(fileName) + HdrTexture (core/src/Scene.cpp:79-81, 197-206):
+// stbi_loadf with vertical flip.  Radiance .hdr files keep their floats; PNG,
+// JPEG, BMP and PGM/PPM bytes become floats as stbi_loadf makes them
+// ((v / 255)^2.2 for colour, v / 255 for alpha).
+rt_status rt_scene_set_env_file(rt_scene* s, const char* path, float scale) {
+    if (!s || !path) return fail(RT_ERR_INVALID_ARG, "rt_scene_set_env_file: NULL argument");
+    std::string head;
+    {
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) return fail(RT_ERR_IO, std::string("rt_scene_set_env_file: could not read ") + path);
+        char b[2] = {0, 0};
+        const size_t got = std::fread(b, 1, 2, f);
+        std::fclose(f);
+        head.assign(b, got);
+    }
+    std::vector<float> img;
+    int w = 0, h = 0;
+    std::string err;
+    if (head == "#?") {
+        if (!read_hdr(path, img, w, h, err)) return fail(RT_ERR_IO, "rt_scene_set_env_file: " + err);
+    } else {
+        std::vector<uint8_t> px;
+        if (!read_image(path, px, w, h, err)) return fail(RT_ERR_IO, "rt_scene_set_env_file: " + err);
+        float lut[256];
+        for (int v = 0; v < 256; v++) lut[v] = float(std::pow(double(v) / 255.0, 2.2));
+        img.resize(px.size());
+        for (size_t i = 0; i < px.size(); i++) img[i] = (i & 3) == 3 ? float(px[i]) / 255.0f : lut[px[i]];
+    }
+    return rt_scene_set_env(s, img.data(), w, h, scale);
+}
+
+rt_status rt_scene_get_env(const rt_scene* s, float* rgba, int32_t* width, int32_t* height) {
+    if (!s) return fail(RT_ERR_INVALID_ARG, "rt_scene_get_env: NULL scene");
+    if (width) *width = s->env_w;
+    if (height) *height = s->env_h;
+    if (rgba && !s->env.empty()) std::memcpy(rgba, s->env.data(), s->env.size() * sizeof(float));
+    return RT_OK;
+}
+
 rt_status rt_scene_load_json(rt_scene* s, const char* path, rt_options* opts, rt_camera* cam) {
     if (!s || !path) return fail(RT_ERR_INVALID_ARG, "rt_scene_load_json: NULL argument");
     std::string text;

@@ -58,6 +58,11 @@ namespace {
         if (e_ != cudaSuccess) return cuda_fail(e_, what); \
     } while (0)
 
+// The server's device current for the rest of the calling scope.
+#define SV_ON_DEVICE(srv, what)                                        \
+    DeviceGuard dg_((srv)->device);                                    \
+    if (dg_.status != cudaSuccess) return cuda_fail(dg_.status, what)
+
 struct Job {
     int64_t id;
     rt_job_desc desc;
@@ -131,6 +136,7 @@ struct rt_server {
     std::mutex mu;
     std::condition_variable cv;
     std::thread worker;
+    int worker_device = -1;  // current device of the background thread, once it runs
     bool stop = false;
     std::string bg_error;
 
@@ -520,7 +526,23 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
 }
 
 void worker_loop(rt_server* s) {
+    // A new thread starts on device 0: the events, graphs and launches below
+    // belong to the device the server was created on.
+    cudaError_t de = cudaSetDevice(s->device);
+    int dev = -1;
+    if (de == cudaSuccess) de = cudaGetDevice(&dev);
     std::unique_lock<std::mutex> lk(s->mu);
+    s->worker_device = dev;
+    if (de != cudaSuccess) {  // every job fails with the reason
+        s->bg_error = std::string("background thread: cudaSetDevice failed: ") + cudaGetErrorString(de);
+        while (!s->stop) {
+            for (int64_t id : s->queued) s->jobs[id]->state = RT_JOB_FAILED;
+            s->queued.clear();
+            s->cv.notify_all();
+            s->cv.wait(lk);
+        }
+        return;
+    }
     while (!s->stop) {
         if (s->queued.empty() && s->running.empty()) {
             s->cv.wait(lk);
@@ -620,6 +642,7 @@ rt_status rt_server_create(const rt_server_options* o, rt_server** out) {
 
 rt_status rt_server_destroy(rt_server* s) {
     if (!s) return RT_OK;
+    SV_ON_DEVICE(s, "rt_server_destroy");
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
@@ -645,6 +668,7 @@ rt_status rt_server_destroy(rt_server* s) {
 
 rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* id) {
     if (!s || !scene) return fail(RT_ERR_INVALID_ARG, "rt_server_add_scene: NULL argument");
+    SV_ON_DEVICE(s, "rt_server_add_scene");
     std::lock_guard<std::mutex> lk(s->mu);
     std::unique_ptr<DeviceScene> ds(new DeviceScene());
     rt_status st = upload_scene(*scene, *ds, s->stream);
@@ -670,6 +694,7 @@ rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* id) 
 
 rt_status rt_server_submit(rt_server* s, const rt_job_desc* d, int64_t* id) {
     if (!s || !d) return fail(RT_ERR_INVALID_ARG, "rt_server_submit: NULL argument");
+    SV_ON_DEVICE(s, "rt_server_submit");
     std::lock_guard<std::mutex> lk(s->mu);
     if (d->scene < 0 || d->scene >= int(s->scenes.size())) return fail(RT_ERR_INVALID_ARG, "rt_server_submit: unknown scene");
     if (d->width <= 0 || d->height <= 0 || d->spp <= 0 || d->max_depth <= 0 || d->max_depth > s->opt.max_depth)
@@ -716,6 +741,7 @@ rt_status rt_server_poll(rt_server* s, int64_t id, rt_job_status* st) {
 
 rt_status rt_server_wait(rt_server* s, int64_t id, double timeout_ms, rt_job_status* st) {
     if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_wait: NULL server");
+    SV_ON_DEVICE(s, "rt_server_wait");
     const auto t_end = std::chrono::steady_clock::now() + std::chrono::microseconds(int64_t(timeout_ms * 1000.0));
     std::unique_lock<std::mutex> lk(s->mu);
     while (true) {
@@ -748,6 +774,7 @@ rt_status rt_server_wait(rt_server* s, int64_t id, double timeout_ms, rt_job_sta
 
 static rt_status download_job(rt_server* s, int64_t id, void* dst, bool rgba8) {
     if (!s || !dst) return fail(RT_ERR_INVALID_ARG, "rt_server_download: NULL argument");
+    SV_ON_DEVICE(s, "rt_server_download");
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->jobs.find(id);
     if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_download: unknown job");
@@ -771,6 +798,7 @@ rt_status rt_server_download_rgba8(rt_server* s, int64_t id, uint32_t* pixels) {
 
 rt_status rt_server_release(rt_server* s, int64_t id) {
     if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_release: NULL server");
+    SV_ON_DEVICE(s, "rt_server_release");
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->jobs.find(id);
     if (it == s->jobs.end()) return fail(RT_ERR_INVALID_ARG, "rt_server_release: unknown job");
@@ -786,6 +814,7 @@ rt_status rt_server_release(rt_server* s, int64_t id) {
 rt_status rt_server_step(rt_server* s, int32_t* did_work) {
     if (!s) return fail(RT_ERR_INVALID_ARG, "rt_server_step: NULL server");
     if (s->opt.background) return fail(RT_ERR_STATE, "rt_server_step: server runs in the background");
+    SV_ON_DEVICE(s, "rt_server_step");
     std::lock_guard<std::mutex> lk(s->mu);
     cudaEvent_t blocked = nullptr;
     rt_status st = step_locked(s, did_work, &blocked);
@@ -796,6 +825,7 @@ rt_status rt_server_step(rt_server* s, int32_t* did_work) {
 
 rt_status rt_server_get_stats(rt_server* s, rt_server_stats* st) {
     if (!s || !st) return fail(RT_ERR_INVALID_ARG, "rt_server_get_stats: NULL argument");
+    SV_ON_DEVICE(s, "rt_server_get_stats");
     std::lock_guard<std::mutex> lk(s->mu);
     std::memset(st, 0, sizeof(*st));
     st->jobs_submitted = s->submitted;
@@ -812,6 +842,8 @@ rt_status rt_server_get_stats(rt_server* s, rt_server_stats* st) {
     st->mean_wave_depth = s->waves ? double(s->depth_sum) / double(s->waves) : 0.0;
     st->guided_waves = s->guided_waves;
     st->training_waves = s->training_waves;
+    st->device = s->device;
+    st->worker_device = s->opt.background ? s->worker_device : -1;
     return RT_OK;
 }
 

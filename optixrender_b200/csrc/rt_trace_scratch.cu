@@ -7,7 +7,6 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
-#include <mutex>
 
 #include "rt_kernels.cuh"
 #include "rt_traverse.cuh"
@@ -25,7 +24,7 @@ static __device__ __align__(256) float4 g_trace_scratch[3 * kTraceScratchRays];
 // k_trace (rt_kernels.cu) reading its rays from, and writing its hits to,
 // the scratch array passed in by the host.
 template <bool AnyHit>
-__global__ void __launch_bounds__(128) k_trace_scratch(SceneView sc, float4* scratch, int n) {
+__global__ void __launch_bounds__(128) k_trace_scratch(SceneView sc, float4* scratch, int n, int* overflow) {
     const int i = int(blockIdx.x) * int(blockDim.x) + int(threadIdx.x);
     if (i >= n) return;
     const float4* rays = scratch;
@@ -38,8 +37,9 @@ __global__ void __launch_bounds__(128) k_trace_scratch(SceneView sc, float4* scr
     r.tmax = b.w;
     prepare_ray(r);
     float t = FLT_MAX, b1 = 0.f, b2 = 0.f;
-    uint32_t nv = 0, nt = 0;
-    int tri = traverse<AnyHit, false>(sc, r, t, b1, b2, nv, nt);
+    uint32_t nv = 0, nt = 0, ovf = 0;
+    int tri = traverse<AnyHit, false>(sc, r, t, b1, b2, nv, nt, ovf);
+    if (ovf) atomicAdd(overflow, int(ovf));
     float4 out;
     if (tri < 0) {
         out = make_float4(FLT_MAX, 0.f, 0.f, __int_as_float(-1));
@@ -58,35 +58,26 @@ namespace rth {
 
 int64_t trace_scratch_rays() { return rtd::kTraceScratchRays; }
 
-// Device address of the scratch array on the current device, looked up once
-// per device with cudaGetSymbolAddress.
-cudaError_t trace_scratch_address(void** ptr) {
-    constexpr int kMaxDevices = 64;
-    static std::mutex mu;
-    static void* addr[kMaxDevices] = {};
-    int dev = 0;
+// Device address of the scratch array on `device`, which must be the calling
+// thread's current device (the entry point makes the renderer's device
+// current).  Looked up on every call: cudaGetSymbolAddress allocates nothing
+// and is cheap, and a cached address would go stale after a device reset.
+cudaError_t trace_scratch_address(int device, void** ptr) {
+    int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, rtd::g_trace_scratch);
-        if (e != cudaSuccess) return e;
-        addr[dev] = p;
-    }
-    *ptr = addr[dev];
-    return cudaSuccess;
+    if (dev != device) return cudaErrorInvalidDevice;
+    return cudaGetSymbolAddress(ptr, rtd::g_trace_scratch);
 }
 
-void launch_trace_scratch(const rtd::SceneView& sc, bool any_hit, void* scratch, int n, cudaStream_t st) {
+void launch_trace_scratch(const rtd::SceneView& sc, bool any_hit, void* scratch, int n, int* overflow, cudaStream_t st) {
     if (n <= 0) return;
     const int block = 128, grid = (n + block - 1) / block;
     float4* s = static_cast<float4*>(scratch);
     if (any_hit)
-        rtd::k_trace_scratch<true><<<grid, block, 0, st>>>(sc, s, n);
+        rtd::k_trace_scratch<true><<<grid, block, 0, st>>>(sc, s, n, overflow);
     else
-        rtd::k_trace_scratch<false><<<grid, block, 0, st>>>(sc, s, n);
+        rtd::k_trace_scratch<false><<<grid, block, 0, st>>>(sc, s, n, overflow);
 }
 
 }  // namespace rth

@@ -166,9 +166,12 @@ RT_D uint32_t intersect_children(const CwNode* nodes, uint32_t idx, const TravRa
 
 // Returns the index of the closest hit triangle (or -1) in [tmin, tmax).
 // `nodes_visited` / `tris_tested` are only updated when Stats is true.
+// `overflows` counts node groups that found the stack full (their subtrees
+// are not visited); the renderer rejects BVHs deeper than the stack, so it
+// stays zero unless that check is broken, and callers report it as an error.
 template <bool AnyHit, bool Stats>
 RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, float& b2, uint32_t& nodes_visited,
-                  uint32_t& tris_tested) {
+                  uint32_t& tris_tested, uint32_t& overflows) {
     int hit_tri = -1;
     float tmax = r.tmax;
     if (sc.num_nodes <= 0) return -1;
@@ -182,7 +185,12 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
         g.y &= ~(1u << (24 + bit));
         uint32_t slot = bit ^ r.oct;
         uint32_t idx = g.x + __popc((g.y & 0xFFu) & ((1u << slot) - 1u));
-        if ((g.y & 0xFF000000u) && sp < kStackSize) stack[sp++] = g;
+        if (g.y & 0xFF000000u) {
+            if (sp < kStackSize)
+                stack[sp++] = g;
+            else
+                overflows++;
+        }
         uint32_t cb, tb, tbits;
         uint32_t nb = intersect_children(sc.nodes, idx, r, tmax, cb, tb, tbits);
         if (Stats) nodes_visited++;
@@ -254,9 +262,9 @@ struct TravState {
 };
 
 // One wide node (or one postponed triangle group) and its triangles; returns
-// true when the ray is finished.
+// true when the ray is finished.  `overflows` as in traverse().
 template <bool AnyHit, bool Stats>
-RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32_t& tris_tested) {
+RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32_t& tris_tested, uint32_t& overflows) {
     uint32_t tb, tbits;
     if (s.g.x & kTriGroup) {
         tb = s.g.x & ~kTriGroup;
@@ -267,7 +275,12 @@ RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32
         s.g.y &= ~(1u << (24 + bit));
         uint32_t slot = bit ^ s.r.oct;
         uint32_t idx = s.g.x + __popc((s.g.y & 0xFFu) & ((1u << slot) - 1u));
-        if ((s.g.y & 0xFF000000u) && st.sp < kStackSize) st.push(s.g);
+        if (s.g.y & 0xFF000000u) {
+            if (st.sp < kStackSize)
+                st.push(s.g);
+            else
+                overflows++;
+        }
         uint32_t cb;
         uint32_t nb = intersect_children(s.nodes, idx, s.r, s.tmax, cb, tb, tbits);
         if (Stats) nodes_visited++;
@@ -308,7 +321,7 @@ RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32
 
 template <bool AnyHit, bool Stats, class Src>
 RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& nodes_visited, uint32_t& tris_tested,
-                         uint32_t& rays) {
+                         uint32_t& rays, uint32_t& overflows) {
     const int lane = threadIdx.x & 31;
     TravStack st;
     st.sp = 0;
@@ -346,7 +359,7 @@ RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& node
                 }
             }
         }
-        if (active && trav_step<AnyHit, Stats>(s, st, nodes_visited, tris_tested)) {
+        if (active && trav_step<AnyHit, Stats>(s, st, nodes_visited, tris_tested, overflows)) {
             fin = true;
             active = false;
         }

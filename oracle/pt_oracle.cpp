@@ -7,6 +7,7 @@
 // camera of Renderer::SetCamera (core/src/Renderer.cpp:796-813) and the
 // tonemap of core/cuda/PostProcessing.cu:18-48, with an OpenMP loop over
 // pixels standing in for optixLaunch.
+#include <cstring>
 #include <omp.h>
 
 #include <memory>
@@ -746,6 +747,56 @@ int orc_shading(int32_t precision, int32_t op, const rt_material* mats, int32_t 
 }
 
 void orc_kulla_conty(float* bsdf, float* avg) { kulla_conty(bsdf, avg); }
+
+// The reference's field defaults (core/include/Scene.h:48-55 Medium,
+// :70-116 Material, :143-155 Light) restated for the C ABI structs, so the
+// oracle builds scenes without the product library.  Phase::g has no
+// initialiser there; it is zero here.
+void orc_material_default(rt_material* m) {
+    std::memset(m, 0, sizeof(*m));
+    m->type = RT_MAT_METAL_WORKFLOW;
+    const float eta[3] = {0.14282f, 0.37414f, 1.43944f}, k[3] = {3.97472f, 2.38066f, 1.59981f};
+    for (int a = 0; a < 3; a++) {
+        m->albedo[a] = 1.0f;
+        m->eta[a] = eta[a];
+        m->k[a] = k[a];
+        m->specular[a] = 1.0f;
+    }
+    m->roughness = 0.1f;
+    m->anisotropy = 0.0f;
+    m->int_ior = 1.5f;
+    m->ext_ior = 1.0f;
+    m->nonlinear = 1;
+    m->metallic = 0.8f;
+    m->coat_weight = 2.0f;
+    m->coat_roughness_u = 0.1f;
+    m->coat_roughness_v = 0.1f;
+    for (int t = 0; t < 8; t++) m->texture_ids[t] = -1;
+}
+
+void orc_light_default(rt_light* l) {
+    std::memset(l, 0, sizeof(*l));
+    l->type = RT_LIGHT_SPHERE;
+    for (int a = 0; a < 3; a++) l->radiance[a] = 3.0f;
+    l->position[0] = 6.0f;
+    l->position[1] = 2.0f;
+    l->u[2] = 6.0f;
+    l->v[0] = 6.0f;
+    l->radius = 3.0f;
+    l->medium = -1;
+}
+
+void orc_medium_default(rt_medium* m) {
+    std::memset(m, 0, sizeof(*m));
+    m->type = RT_MEDIUM_HOMOGENEOUS;
+    m->phase = RT_PHASE_ISOTROPIC;
+    const float ss[3] = {0.74f, 0.88f, 1.01f}, sa[3] = {0.032f, 0.17f, 0.48f};
+    for (int a = 0; a < 3; a++) {
+        m->sigma_s[a] = ss[a];
+        m->sigma_a[a] = sa[a];
+    }
+    m->scale = 500.0f;
+}
 
 void orc_env_cache(const float* rgba, int32_t w, int32_t h, float* cache) { env_cache(rgba, w, h, cache); }
 

@@ -48,6 +48,82 @@ def _f(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+# ------------------------------------------------------------ scene structs
+# The C ABI's struct layouts come from the optixrender_b200 package (plain
+# ctypes classes; importing them loads no library).  Their default values come
+# from a CPU library: the oracle's restatement of the reference's defaults
+# (prefix "orc") or the reference's own default-constructed structs in its
+# host build (prefix "refpt", oracle/refpt.py), so the oracle and the
+# benchmark's reference arm never load the product library.
+_VEC3 = {"albedo", "eta", "k", "specular", "radiance", "position", "u", "v", "g", "sigma_s", "sigma_a",
+         "bounds_min", "bounds_max"}
+
+
+def _fill(obj, kw):
+    for k, v in kw.items():
+        if k in _VEC3:
+            setattr(obj, k, (C.c_float * 3)(*[float(x) for x in v]))
+        elif k == "texture_ids":
+            ids = list(v) + [-1] * (8 - len(v))
+            obj.texture_ids = (C.c_int32 * 8)(*ids)
+        elif k == "grid_res":
+            obj.grid_res = (C.c_int32 * 3)(*v)
+        else:
+            setattr(obj, k, v)
+    return obj
+
+
+class StructDefaults:
+    """Material / Light / Medium constructors with defaults from `lib`'s
+    <prefix>_material_default, <prefix>_light_default, <prefix>_medium_default."""
+
+    def __init__(self, lib, prefix):
+        import optixrender_b200 as rt
+        self.rt = rt
+        self.fns = {}
+        for name, cls in (("material", rt.Material), ("light", rt.Light), ("medium", rt.Medium)):
+            fn = getattr(lib, f"{prefix}_{name}_default")
+            fn.restype = None
+            fn.argtypes = [C.POINTER(cls)]
+            self.fns[name] = (fn, cls)
+
+    def _make(self, name, type_, kw):
+        fn, cls = self.fns[name]
+        o = cls()
+        fn(C.byref(o))
+        o.type = type_
+        return _fill(o, kw)
+
+    def material(self, type=0, **kw):
+        return self._make("material", type, kw)
+
+    def light(self, type=0, **kw):
+        return self._make("light", type, kw)
+
+    def medium(self, type=0, density=None, **kw):
+        m = self._make("medium", type, kw)
+        if density is not None:
+            d = np.ascontiguousarray(density, dtype=np.float32)
+            m._density_keepalive = d
+            m.density = d.ctypes.data_as(C.POINTER(C.c_float))
+        return m
+
+
+def oracle_structs():
+    return StructDefaults(load(), "orc")
+
+
+def options(**kw):
+    """rt_options with the reference's launch defaults (LaunchParams.h:29-30 and
+    :66: one sample, 25 bounces, Gaussian filter; the reference's LCG stream),
+    built without the product library."""
+    import optixrender_b200 as rt
+    o = rt.Options()
+    o.spp, o.max_depth, o.filter, o.rng, o.seed, o.exposure = 1, 25, rt.FILTER_GAUSSIAN, rt.RNG_LCG, 1, 1.0
+    o.guide_train_spp, o.guide_prob, o.guide_steps = 32, 0.5, 4
+    return _fill(o, kw)
+
+
 def _normalize(v):
     """float32 normalize with the library's operation order: v / sqrt((x*x + y*y) + z*z)."""
     v = v.astype(np.float32)
@@ -72,6 +148,7 @@ class OracleScene:
     def __init__(self, spec):
         import optixrender_b200 as rt
         lib = load()
+        st = oracle_structs()
         tris, tmesh = [], []
         tnorm, tuv = [], []
         mats = []
@@ -83,7 +160,7 @@ class OracleScene:
             tnorm.append(None if tn is None else _normalize(tn.reshape(-1, 3)).reshape(-1, 9))
             tuv.append(m.tri_texcoords())
             tmesh.append(np.full(t.shape[0], i, np.int32))
-            mats.append(rt.material(**m.material))
+            mats.append(st.material(**m.material))
             media_pairs += [m.out_medium, m.in_medium]
         self.tv = np.ascontiguousarray(np.concatenate(tris), np.float32)
         self.tn = self.tuv = None
@@ -97,8 +174,8 @@ class OracleScene:
         self.tmesh = np.ascontiguousarray(np.concatenate(tmesh), np.int32)
         self.mats = (rt.Material * len(mats))(*mats)
         self.mm = np.asarray(media_pairs, np.int32)
-        self.lights = (rt.Light * max(1, len(spec.lights)))(*[rt.light(**l) for l in spec.lights])
-        self.media = (rt.Medium * max(1, len(spec.media)))(*[rt.medium(**m) for m in spec.media])
+        self.lights = (rt.Light * max(1, len(spec.lights)))(*[st.light(**l) for l in spec.lights])
+        self.media = (rt.Medium * max(1, len(spec.media)))(*[st.medium(**m) for m in spec.media])
         env = spec.env
         self.env = None if env is None else np.ascontiguousarray(env, np.float32)
         eh, ew = (0, 0) if env is None else env.shape[:2]

@@ -9,6 +9,7 @@
 // TEST INFRASTRUCTURE ONLY: the timed CPU baseline of bench.py (kind
 // "reference") and a statistical cross-check of the oracle.  Built by
 // oracle/Makefile into oracle/_ref/ when the reference tree is present.
+#include <cstring>
 #include <omp.h>
 
 #include "pt_oracle.hpp"  // before the reference headers: they define EPS as a macro
@@ -374,6 +375,62 @@ void* refpt_scene_new(const float* tri_v, const int32_t* tri_mesh, int64_t ntri,
 }
 
 void refpt_scene_free(void* p) { delete static_cast<RefScene*>(p); }
+
+// The reference's own default-constructed Material, Light and Medium
+// (core/include/Scene.h:48-155) as the C ABI structs, so the benchmark's
+// reference arm builds its scene without the product library.
+void refpt_material_default(rt_material* out) {
+    Material r{};  // value-initialised: fields without an initialiser are zero
+    std::memset(out, 0, sizeof(*out));
+    out->type = int32_t(r.type);
+    for (int a = 0; a < 3; a++) {
+        out->albedo[a] = r.albedo[a];
+        out->eta[a] = r.eta[a];
+        out->k[a] = r.k[a];
+        out->specular[a] = r.specular[a];
+    }
+    out->roughness = r.roughness;
+    out->anisotropy = r.anisotropy;
+    out->int_ior = r.int_ior;
+    out->ext_ior = r.ext_ior;
+    out->nonlinear = r.nonlinear ? 1 : 0;
+    out->metallic = r.metallic;
+    out->coat_weight = r.coat_weight;
+    out->coat_roughness_u = r.coat_roughness_u;
+    out->coat_roughness_v = r.coat_roughness_v;
+    const int ids[8] = {r.albedoTextureID, r.roughnessTextureID, r.anisotropyTextureID, r.specularTextureID,
+                        r.metallicTextureID, r.coat_roughness_uTextureID, r.coat_roughness_vTextureID,
+                        r.normalTextureID};
+    for (int t = 0; t < 8; t++) out->texture_ids[t] = ids[t];
+}
+
+void refpt_light_default(rt_light* out) {
+    Light r{};
+    std::memset(out, 0, sizeof(*out));
+    out->type = int32_t(r.type);
+    out->double_side = r.doubleSide ? 1 : 0;
+    for (int a = 0; a < 3; a++) {
+        out->radiance[a] = r.radiance[a];
+        out->position[a] = r.position[a];
+        out->u[a] = r.u[a];
+        out->v[a] = r.v[a];
+    }
+    out->radius = r.radius;
+    out->medium = r.medium;
+}
+
+void refpt_medium_default(rt_medium* out) {
+    Medium r{};
+    std::memset(out, 0, sizeof(*out));
+    out->type = int32_t(r.type);
+    out->phase = int32_t(r.phase.type);
+    for (int a = 0; a < 3; a++) {
+        out->g[a] = 0.0f;  // Phase::g is left indeterminate by the reference (vec3f's empty constructor)
+        out->sigma_s[a] = r.sigma_s[a];
+        out->sigma_a[a] = r.sigma_a[a];
+    }
+    out->scale = r.scale;
+}
 
 // One launch (numPixelSamples = opts->spp) of rows [row0, row1) into color
 // (w*h*4 floats); cam = position, direction, horizontal, vertical.

@@ -38,24 +38,32 @@ def _f(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+def ref_structs():
+    """Material / Light / Medium constructors whose defaults are the reference's
+    own default-constructed structs (core/include/Scene.h:48-155)."""
+    import pyoracle
+    return pyoracle.StructDefaults(load(), "refpt")
+
+
 class RefScene:
     def __init__(self, spec):
         import optixrender_b200 as rt
         import pyoracle
         lib = load()
+        st = ref_structs()
         tris, tmesh, mats, mm = [], [], [], []
         for i, m in enumerate(spec.meshes):
             t = m.triangles()
             tris.append(t)
             tmesh.append(np.full(t.shape[0], i, np.int32))
-            mats.append(rt.material(**m.material))
+            mats.append(st.material(**m.material))
             mm += [m.out_medium, m.in_medium]
         self.tv = np.ascontiguousarray(np.concatenate(tris), np.float32)
         self.tmesh = np.ascontiguousarray(np.concatenate(tmesh), np.int32)
         self.mats = (rt.Material * len(mats))(*mats)
         self.mm = np.asarray(mm, np.int32)
-        self.lights = (rt.Light * max(1, len(spec.lights)))(*[rt.light(**l) for l in spec.lights])
-        self.media = (rt.Medium * max(1, len(spec.media)))(*[rt.medium(**m) for m in spec.media])
+        self.lights = (rt.Light * max(1, len(spec.lights)))(*[st.light(**l) for l in spec.lights])
+        self.media = (rt.Medium * max(1, len(spec.media)))(*[st.medium(**m) for m in spec.media])
         self.env = None if spec.env is None else np.ascontiguousarray(spec.env, np.float32)
         eh, ew = (0, 0) if spec.env is None else spec.env.shape[:2]
         self.h = lib.refpt_scene_new(_f(self.tv), self.tmesh.ctypes.data_as(C.POINTER(C.c_int32)), self.tv.shape[0],

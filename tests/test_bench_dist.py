@@ -49,3 +49,29 @@ def test_two_gloo_ranks():
         assert ms == pytest.approx(15.0)  # max over ranks
         assert value == pytest.approx(2 * 1_000_000 / 0.015 / 1e6)
         assert ref_rc == 0
+
+
+def test_reference_arm_loads_no_product_library():
+    """bench.py --impl reference runs the reference's CPU path (its host build,
+    or the oracle) without mapping the product library, and reports the same
+    config as the product arm."""
+    import json
+    import subprocess
+    code = (
+        "import sys, json, argparse\n"
+        f"sys.path.insert(0, {str(ROOT)!r})\n"
+        "import bench\n"
+        "args = argparse.Namespace(spp=1, warmup=0, steps=1, cpu_seconds=0.3)\n"
+        "bench.run_reference(args, 0, 1)\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('MAPS', 'liboptixrender_b200' in maps)\n"
+    )
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert lines[-1] == "MAPS False"
+    line = json.loads(next(l for l in lines if l.startswith("{")))
+    assert line["impl"] == "reference" and line["value"] > 0
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert line["config"] == bench.bench_config(1, 1310720 + 64 * 20000, 1)

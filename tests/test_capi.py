@@ -113,6 +113,39 @@ def test_wide_bvh_builds_and_validates(name):
         assert s.counts()["triangles"] == 2590720
 
 
+def _chain_scene(lo, hi, step):
+    """Triangles at positions 2^e for e in [lo, hi): each binned SAH split
+    peels off the largest few, so the tree is a chain, and the small end has
+    centroid extents for which 32 / extent overflows."""
+    x = 2.0 ** np.arange(lo, hi, step)
+    z = np.zeros_like(x)
+    tris = np.stack([np.stack([x, z, z], 1), np.stack([1.25 * x, 0.25 * x, z], 1), np.stack([x, z, 0.25 * x], 1)], 1)
+    s = rt.Scene()
+    s.add_mesh(tris.astype(np.float32).reshape(-1, 3), rt.material(rt.MAT_DIFFUSE))
+    return s
+
+
+def test_bvh_deeper_than_the_traversal_stack_is_rejected():
+    """The traversal keeps node groups on a 32-entry stack, so a tree deeper
+    than RT_MAX_BVH_DEPTH levels could skip subtrees: the build reports the
+    depth and refuses the tree (renderers and servers share the check)."""
+    lib = rt.load_library()
+    s = _chain_scene(-149, 127, 0.2)
+    nodes, depth = C.c_int64(), C.c_int32()
+    st = lib.rt_scene_build_bvh(s.handle, C.byref(nodes), C.byref(depth))
+    assert depth.value > 32 and nodes.value > 0
+    assert st == rt.RT_ERR_UNSUPPORTED
+    assert "too deep" in lib.rt_last_error_message().decode()
+
+
+def test_bvh_build_of_vanishing_centroid_extents():
+    """Nodes whose centroid extent is so small that the bin scale overflows
+    to infinity: every centroid must still land in one of the 32 bins."""
+    s = _chain_scene(-120, 120, 0.5)
+    nodes, depth = s.build_bvh()
+    assert nodes >= 1 and 1 <= depth <= 32
+
+
 def test_obj_loader(tmp_path):
     obj = tmp_path / "q.obj"
     obj.write_text("v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvt 0 0\nvt 1 0\nvt 1 1\nvt 0 1\nvn 0 0 1\n"
@@ -176,6 +209,38 @@ def test_json_scene_loads_reference_schema(tmp_path):
     assert np.allclose(lo, [1, 0, -2], atol=1e-5) and np.allclose(hi, [1, 2, 0], atol=1e-5)
     # look_at defaults to the scene bounds centre (main.cpp:221)
     assert np.allclose(list(cam.at), (lo + hi) / 2, atol=1e-5)
+
+
+def test_env_from_file_as_scene_add_env(tmp_path):
+    """Scene::AddEnv(fileName) (core/src/Scene.cpp:79-81, 197-206): a Radiance
+    file keeps its floats with row 0 at the bottom; an LDR image is converted
+    as stbi_loadf converts it, (v/255)^2.2 for colour and v/255 for alpha."""
+    rng = np.random.default_rng(3)
+    env = rng.uniform(0.01, 20.0, (6, 10, 4)).astype(np.float32)
+    env[..., 3] = 1.0
+    _write_hdr(tmp_path / "sky.hdr", env)
+    s = rt.Scene()
+    assert s.get_env() is None
+    s.set_env_file(tmp_path / "sky.hdr", scale=2.0)
+    got = s.get_env()
+    assert got.shape == (6, 10, 4)
+    # RGBE: 8-bit mantissas under one shared exponent per pixel
+    tol = 2.0 * env[..., :3].max(-1, keepdims=True) / 128
+    assert np.all(np.abs(got[..., :3] - 2.0 * env[..., :3]) <= tol)
+    # the same file through the JSON "infinite" light gives the same image
+    s2 = rt.Scene()
+    s2.load_json_string('{"light": [{"type": "infinite", "hdr_path": "sky.hdr", "scale": 2}]}', str(tmp_path))
+    assert np.array_equal(s2.get_env(), got)
+    px = rng.integers(0, 2 ** 32, (5, 7), dtype=np.uint64).astype(np.uint32)
+    rt.write_png(tmp_path / "sky.png", px)
+    s.set_env_file(tmp_path / "sky.png")
+    ldr = s.get_env()
+    b = px.view(np.uint8).reshape(5, 7, 4).astype(np.float64)
+    np.testing.assert_allclose(ldr[..., :3], (b[..., :3] / 255.0) ** 2.2, rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(ldr[..., 3], b[..., 3] / 255.0, rtol=1e-6)
+    with pytest.raises(rt.RTError) as e:
+        s.set_env_file(tmp_path / "missing.hdr")
+    assert e.value.code == rt.RT_ERR_IO
 
 
 def test_json_rejects_unknown_material_and_medium():

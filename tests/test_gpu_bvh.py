@@ -74,3 +74,27 @@ def test_closest_hits_through_gpu_bvh_match_host_bvh():
     assert agree >= 0.9999
     hit = ids[1] >= 0
     assert np.allclose(hits[0][hit, 0], hits[1][hit, 0], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_build_of_degenerate_chains():
+    """Triangles at positions 2^e: binned SAH peels off a few per split, so
+    the tree is a chain, and at the small end 32 / extent overflows (the
+    device's saturating bin index keeps every centroid in a bin).  The chain
+    that fits the traversal stack builds and validates on the device like on
+    the host; the one deeper than RT_MAX_BVH_DEPTH is refused by both."""
+    from test_capi import _chain_scene
+    import ctypes as C
+    lib = rt.load_library()
+    s = _chain_scene(-120, 120, 0.5)
+    gn, gd = s.build_bvh_gpu()
+    hn, hd = s.build_bvh()
+    assert gd <= 32 and abs(gd - hd) <= 3
+    deep = _chain_scene(-149, 127, 0.2)
+    nodes, depth = C.c_int64(), C.c_int32()
+    st = lib.rt_scene_build_bvh_gpu(deep.handle, C.byref(nodes), C.byref(depth))
+    assert st in (rt.RT_ERR_UNSUPPORTED, rt.RT_ERR_CUDA)
+    if st == rt.RT_ERR_UNSUPPORTED:
+        assert depth.value > 32
+    with pytest.raises(rt.RTError):  # a renderer refuses the scene too
+        rt.Renderer(deep, rt.options(width=4, height=4))

@@ -198,3 +198,37 @@ def test_guided_jobs_share_the_scene_network(policy):
         srv.release(jid)
     srv.release(plain)
     srv.close()
+
+
+@pytest.mark.gpu
+def test_background_worker_works_on_the_servers_device():
+    """The background thread makes the server's device current before it
+    records events, captures graphs or launches waves (a new thread starts on
+    device 0); the stats report both.  Jobs submitted, awaited and downloaded
+    from another host thread come out the same as from the creating thread."""
+    import threading
+    torch = pytest.importorskip("torch")
+    spec = scenes.cornell(32, 32, 2, seed=9)
+    srv = rt.Server(rt.server_options(wave_paths=4096, max_jobs=4, max_depth=8))
+    keep = scenes.build_scene(spec)
+    sid = srv.add_scene(keep)
+    jid = srv.submit(_job_for(spec, sid))
+    assert srv.wait(jid, 60000.0)["state"] == rt.JOB_DONE
+    st = srv.stats()
+    assert st["device"] == torch.cuda.current_device()
+    assert st["worker_device"] == st["device"]
+    out = {}
+
+    def other_thread():
+        j2 = srv.submit(_job_for(spec, sid))
+        out["state"] = srv.wait(j2, 60000.0)["state"]
+        out["img"] = srv.download(j2)
+        srv.release(j2)
+
+    t = threading.Thread(target=other_thread)
+    t.start()
+    t.join(120.0)
+    assert out["state"] == rt.JOB_DONE
+    assert np.array_equal(out["img"].view(np.uint32), srv.download(jid).view(np.uint32))
+    srv.release(jid)
+    srv.close()

@@ -130,3 +130,23 @@ def test_live_reference_build_when_present():
     shading.ref_kulla_conty(lut.ctypes.data_as(F), avg.ctypes.data_as(F))
     assert np.array_equal(lut, GOLD["kc_lut"].ravel())
     assert bool(shading.ref_pair_order_reversed()) == bool(GOLD["pair_order_reversed"])
+
+
+def test_struct_defaults_agree_with_the_reference():
+    """Scene struct defaults (core/include/Scene.h:48-155): the oracle's
+    restatement, the reference's own default-constructed structs (when its
+    host build is present) and the product's rt_*_default give the same
+    fields."""
+    import refpt
+
+    def fields(o):
+        return {k: (list(getattr(o, k)) if hasattr(getattr(o, k), "__len__") else getattr(o, k))
+                for k, _ in o._fields_ if k not in ("density", "majorant_res", "grid_res", "bounds_min", "bounds_max")}
+
+    srcs = [pyoracle.oracle_structs()]
+    if refpt.available():
+        srcs.append(refpt.ref_structs())
+    for kind in ("material", "light", "medium"):
+        prod = fields(getattr(rt, kind)(type=0))
+        for src in srcs:
+            assert fields(getattr(src, kind)(type=0)) == prod, kind
