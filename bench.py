@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library's choice)")
+    p.add_argument("--ref-spp", type=int, default=16384,
+                   help="samples per pixel of the FP64-accumulated plain reference the frame's relMSE is measured "
+                        "against (0: no relMSE)")
     return p.parse_args()
 
 
@@ -356,6 +359,19 @@ def main():
     e2e_value = job_mpaths(paths_per_step, world, e2e_ms)
     h2d = int(r.stats()["h2d_bytes"])  # launch parameters + wave table uploaded by each Render()
 
+    # image error of the benchmarked frame (after every timed region): relMSE
+    # against a plain render of ref_spp samples per pixel with independent
+    # seeds, accumulated in FP64; the reference's own noise adds about
+    # spp / ref_spp of the value (0.4% at 64 / 16384)
+    quality = None
+    if args.ref_spp > 0 and rank == 0:
+        from optixrender_b200.guide_bench import reference, relmse
+        frame = r.download_linear()
+        ref_img, ref_spp, ref_ms = reference(spec, args.ref_spp)
+        quality = {"relmse": relmse(frame, ref_img), "reference_spp": ref_spp,
+                   "reference": "plain render, frames of 256 spp with independent seeds accumulated in FP64",
+                   "reference_device_ms": ref_ms}
+        del ref_img
     peak, peak_kind = measured_peak()
     ext_bytes = (counters["extend_nodes"] * NODE_BYTES + counters["extend_tris"] * TRI_BYTES +
                  counters["extend_rays"] * RAY_BYTES)
@@ -389,6 +405,7 @@ def main():
         "paths_ended_by_nan_throughput_per_step": counters["nan_history"] / args.steps,
         "launches_per_step": launches_per_step,
         "clocks": clk.summary(),
+        "image": quality,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = CpuRunner(spec).sample(args.spp, args.cpu_seconds)

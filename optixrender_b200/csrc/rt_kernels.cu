@@ -216,8 +216,12 @@ RT_D v3 medium_transmittance(const DevMedium* mp, const MedParams& med, v3 o, v3
 }
 
 // ------------------------------------------------------------------ shade
-// (5 blocks per SM at 96 registers spill 320 B and measured within noise.)
-template <bool Stats>
+// Full = false compiles the kernel without the participating-media,
+// path-guiding and material-texture branches, for waves whose scenes have
+// none of them (the host picks it from Ctx::features): those branches set
+// the register budget of the whole kernel, so the common path runs at a
+// lower occupancy when they are compiled in.
+template <bool Stats, bool Full>
 __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     const int cur = c.bounce & 1, nxt = cur ^ 1;
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
             radiance += xyz(n1);
             const rtg::GuideCtx& G = c.G;
             const size_t cap = size_t(B.capacity);
-            if (G.rec != nullptr && bounce >= 1 && bounce - 1 < rtg::kGuideRec)  // radiance before the next vertex
+            if (Full && G.rec != nullptr && bounce >= 1 && bounce - 1 < rtg::kGuideRec)  // radiance before the next vertex
                 G.rec[(size_t(bounce - 1) * 4 + 3) * cap + slot] = f4(radiance, 0.0f);
             v3 V = -d, L = d;
             float gp = 0.0f;  // probability of sampling the guiding mixture at this vertex
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 s.mat = sc.materials + mi.material;
                 int stale_mesh = mesh;
                 const int4* mt = reinterpret_cast<const int4*>(s.mat);
-                if (__ldg(mt + 5).z != 0 && B.mat_tex != nullptr) {
+                if (Full && __ldg(mt + 5).z != 0 && B.mat_tex != nullptr) {
                     // texture overrides of the closest-hit program (devicePrograms.cu:84-115)
                     float tcx = w0 * a0.w + u * a2.w + v * a3.y;
                     float tcy = w0 * a1.w + u * a3.x + v * a3.z;
@@ -338,7 +342,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                     stale_mesh = mesh | kStaleTextured;
                 }
                 v3 P = w0 * xyz(p0) + u * xyz(p1) + v * xyz(p2);
-                if (G.rec != nullptr) gin = rtg::guide_input(o + h4.x * d, xyz(p0), xyz(p1), xyz(p2), d, G);
+                if (Full && G.rec != nullptr) gin = rtg::guide_input(o + h4.x * d, xyz(p0), xyz(p1), xyz(p2), d, G);
                 s.front = dot(d, Ns) < 0.0f;
                 s.sn = s.front ? Ns : -Ns;
                 closest = length(P - o);
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 s.front = true;
                 if (mesh < 0)
                     s.mat = nullptr;
-                else if (mesh & kStaleTextured)  // the last hit's textured material stays, as isect.material does
+                else if (Full && (mesh & kStaleTextured))  // the last hit's textured material stays, as isect.material does
                     s.mat = B.mat_tex + slot;
                 else
                     s.mat = sc.materials + sc.meshes[mesh].material;
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 }
             }
             const rtg::Mixture* gmix = nullptr;
-            if (G.mix != nullptr && tri >= 0 && s.mat != nullptr) {
+            if (Full && G.mix != nullptr && tri >= 0 && s.mat != nullptr) {
                 const float* mw = reinterpret_cast<const float*>(s.mat);  // type, roughness (plain loads)
                 const int mtype = __float_as_int(mw[0]);
                 const bool glossy = mtype == RT_MAT_CONDUCTOR || mtype == RT_MAT_CLEARCOATED_CONDUCTOR;
@@ -391,7 +395,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
             float mult_trans_pdf = 1.0f;
             v3 nee_e(0.0f), nee_l(0.0f);
             // ---- media (devicePrograms.cu:274-338)
-            if (sc.num_media != 0) {
+            if (Full && sc.num_media != 0) {
                 medium_index = (hit_light || s.front) ? out_m : in_m;
                 if (medium_index != -1) {
                     const DevMedium* mp = sc.media + medium_index;
@@ -474,11 +478,11 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                         if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
                             float bpdf;
                             v3 f = eval_material(sc, s, V, sd, bpdf);
-                            if (gp > 0.0f) bpdf = gp * rtg::mixture_pdf(gmix, sd) + (1.0f - gp) * bpdf;
+                            if (Full && gp > 0.0f) bpdf = gp * rtg::mixture_pdf(gmix, sd) + (1.0f - gp) * bpdf;
                             float ct = fabsf(dot(s.sn, sd));
                             float w = power_heuristic(lp, bpdf);
                             v3 thh(1.0f);
-                            if (medium_index != -1) {
+                            if (Full && medium_index != -1) {
                                 const DevMedium* mp = sc.media + medium_index;
                                 const MedParams med = load_medium(mp);
                                 float tp2;
@@ -509,11 +513,11 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                         if (!light_trace(sc, pos, sd, cl, tvv, tpdf, tm) && nee_pdf_ok(lp)) {
                             float bpdf;
                             v3 f = eval_material(sc, s, V, sd, bpdf);
-                            if (gp > 0.0f) bpdf = gp * rtg::mixture_pdf(gmix, sd) + (1.0f - gp) * bpdf;
+                            if (Full && gp > 0.0f) bpdf = gp * rtg::mixture_pdf(gmix, sd) + (1.0f - gp) * bpdf;
                             float ct = fabsf(dot(s.sn, sd));
                             float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, bpdf);
                             v3 thh(1.0f);
-                            if (medium_index != -1) {
+                            if (Full && medium_index != -1) {
                                 const DevMedium* mp = sc.media + medium_index;
                                 const MedParams med = load_medium(mp);
                                 float tp2;
@@ -530,7 +534,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                     }
                     // BSDF sampling, devicePrograms.cu:474-477
                     float bpdf = 0.0f;
-                    if (gp > 0.0f) {
+                    if (Full && gp > 0.0f) {
                         // one-sample MIS of the mixture and the BSDF: the direction comes
                         // from the mixture with probability gp, and is weighted by the
                         // combined density gp * q + (1 - gp) * p_bsdf
@@ -578,7 +582,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 }
             }
             cont = alive && (bounce + 1 < jp.max_depth);
-            if (G.rec != nullptr && cont && rec_pdf > 0.0f && rec_cos > 0.0f && bounce < rtg::kGuideRec) {
+            if (Full && G.rec != nullptr && cont && rec_pdf > 0.0f && rec_cos > 0.0f && bounce < rtg::kGuideRec) {
                 // training record: network input, pdf, direction, |cos|, throughput after this vertex
                 float4* R = G.rec + size_t(bounce) * 4 * cap + slot;
                 R[0] = make_float4(gin.x, gin.y, gin.z, rec_pdf);
@@ -1067,8 +1071,10 @@ void query_shape(LaunchShape& s) {
     int b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend<false>, kBlock, 0);
     s.blocks_extend = s.sms * (b > 0 ? b : 1);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false, true>, kBlock, 0);
     s.blocks_shade = s.sms * (b > 0 ? b : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false, false>, kBlock, 0);
+    s.blocks_shade_plain = s.sms * (b > 0 ? b : 1);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shadow<false>, kBlock, 0);
     s.blocks_shadow = s.sms * (b > 0 ? b : 1);
 }
@@ -1086,10 +1092,19 @@ void launch_extend(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t 
         k_extend<false><<<s.blocks_extend, kBlock, 0, st>>>(c);
 }
 void launch_shade(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
-    if (stats)
-        k_shade<true><<<s.blocks_shade, kBlock, 0, st>>>(c);
-    else
-        k_shade<false><<<s.blocks_shade, kBlock, 0, st>>>(c);
+    const bool full = c.features != 0;
+    const int blocks = full ? s.blocks_shade : s.blocks_shade_plain;
+    if (stats) {
+        if (full)
+            k_shade<true, true><<<blocks, kBlock, 0, st>>>(c);
+        else
+            k_shade<true, false><<<blocks, kBlock, 0, st>>>(c);
+    } else {
+        if (full)
+            k_shade<false, true><<<blocks, kBlock, 0, st>>>(c);
+        else
+            k_shade<false, false><<<blocks, kBlock, 0, st>>>(c);
+    }
 }
 void launch_shadow(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
     if (stats)

@@ -103,7 +103,11 @@ struct Ctx {
     int bounce;
     int max_depth;  // largest max_depth of the jobs in the wave
     rtg::GuideCtx G;  // path guiding (G.mix null: not guided)
+    int features;     // kFeature* bits of the wave's scenes and jobs (host side: picks the shade kernel)
 };
+
+// Scene and job features that need the full shade kernel.
+constexpr int kFeatureMedia = 1, kFeatureGuide = 2, kFeatureTextures = 4;
 
 #ifdef __CUDACC__
 RT_D const WaveParams& wave_of(const Ctx& c) { return c.waves[*c.wave_index]; }
@@ -123,6 +127,7 @@ namespace rth {
 struct LaunchShape {
     int sms;
     int blocks_extend, blocks_shade, blocks_shadow;
+    int blocks_shade_plain;  // the shade kernel without media, guiding and textures
 };
 void query_shape(LaunchShape& s);
 // The a-trous denoiser: colour, albedo and normal AOVs (W x H float4) in;

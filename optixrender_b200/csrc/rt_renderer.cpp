@@ -608,6 +608,8 @@ rt_status rt_renderer_render(rt_renderer* r) {
     c.wave_index = r->wave_index.as<int>();
     c.wave_ring = int(nwaves);
     c.max_depth = o.max_depth;
+    c.features = (r->ds.view.num_media > 0 ? kFeatureMedia : 0) | (guided ? kFeatureGuide : 0) |
+                 (r->ds.view.num_tex > 0 ? kFeatureTextures : 0);
     rtg::NetView net{};
     if (guided) {
         float3 lo, inv;

@@ -105,6 +105,7 @@ struct rt_server {
     std::vector<std::unique_ptr<DeviceScene>> scenes;
     std::vector<SceneGuide> guides;  // one per scene; networks created at the first guided wave
     int64_t scene_bytes = 0;
+    int scene_features = 0;  // kFeatureMedia / kFeatureTextures of any resident scene
     std::map<int64_t, std::unique_ptr<Job>> jobs;
     std::deque<int64_t> queued;
     std::vector<int64_t> running;  // admission order
@@ -259,6 +260,7 @@ Ctx make_ctx(rt_server* s, int gscene = -1) {
     c.wave_index = s->wave_index.as<int>();
     c.wave_ring = s->ring_size;
     c.max_depth = s->opt.max_depth;
+    c.features = s->scene_features | (gscene >= 0 ? kFeatureGuide : 0);
     if (gscene >= 0) {
         const SceneGuide& g = s->guides[size_t(gscene)];
         c.G.mix = s->g_mix.as<rtg::Mixture>();
@@ -673,11 +675,17 @@ rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* id) 
     std::unique_ptr<DeviceScene> ds(new DeviceScene());
     rt_status st = upload_scene(*scene, *ds, s->stream);
     if (st) return st;
-    if (ds->view.num_tex > 0 && !s->mat_tex.ptr) {
+    const int feat = (ds->view.num_media > 0 ? kFeatureMedia : 0) | (ds->view.num_tex > 0 ? kFeatureTextures : 0);
+    const bool need_tex = ds->view.num_tex > 0 && !s->mat_tex.ptr;
+    if (need_tex || (s->scene_features | feat) != s->scene_features) {
+        // graphs captured without the textured-material buffer, or with the
+        // shade kernel that leaves out media and textures, are recaptured
         SV_CUDA(cudaStreamSynchronize(s->stream), "rt_server_add_scene");
-        SV_CUDA(s->mat_tex.alloc(size_t(s->capacity) * sizeof(DevMaterial)), "allocate textured materials");
-        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);  // captured without the buffer
+        if (need_tex)
+            SV_CUDA(s->mat_tex.alloc(size_t(s->capacity) * sizeof(DevMaterial)), "allocate textured materials");
+        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
         s->graphs.clear();
+        s->scene_features |= feat;
     }
     s->scene_bytes += int64_t(ds->bytes);
     s->scenes.push_back(std::move(ds));

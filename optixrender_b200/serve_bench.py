@@ -17,6 +17,12 @@ as slowdown = time-to-image / (job paths / saturation Mpaths/s), and per
 quartile of job size.
 
     python -m optixrender_b200.serve_bench --requests 1000 --load 0.8
+    python -m optixrender_b200.serve_bench --requests 1000 --loads 0.25,0.5,0.8,1.0   # latency against load
+    python -m optixrender_b200.serve_bench --mix plain-spheres --loads ""            # saturation only
+
+`--mix plain-spheres` draws every request from the 1080p spheres scene without
+guiding, the mix whose saturation throughput compares with a single
+Renderer's on the benchmark frame.
 """
 import argparse
 import json
@@ -57,17 +63,19 @@ def orbit_camera(cam, rng):
     return out
 
 
-def make_requests(n, specs, seed=1, resolutions=RESOLUTIONS, spps=SPPS):
+def make_requests(n, specs, seed=1, resolutions=RESOLUTIONS, spps=SPPS, scene_choices=None, guided=None):
     rng = np.random.default_rng(seed)
     reqs = []
+    choices = list(range(len(specs))) if scene_choices is None else list(scene_choices)
     for i in range(n):
-        si = int(rng.integers(len(specs)))
+        si = choices[int(rng.integers(len(choices)))]
         w, h = resolutions[int(rng.integers(len(resolutions)))]
         spp = spps[int(rng.integers(len(spps)))]
         spec = specs[si]
         reqs.append(dict(scene=si, width=w, height=h, spp=spp, max_depth=spec.settings["max_depth"],
                          rr_depth=spec.settings["rr_depth"], camera=orbit_camera(spec.camera, rng),
-                         guided=bool(rng.integers(2)), seed=int(rng.integers(1 << 62))))
+                         guided=bool(rng.integers(2)) if guided is None else bool(guided),
+                         seed=int(rng.integers(1 << 62))))
     return reqs
 
 
@@ -146,12 +154,19 @@ def main(argv=None):
     p.add_argument("--policy", default="fair", choices=["fair", "fifo", "srpt"])
     p.add_argument("--wave-paths", type=int, default=1 << 23)
     p.add_argument("--max-jobs", type=int, default=256)
+    p.add_argument("--loads", default=None,
+                   help="comma-separated loads (fractions of the saturation job rate) to sweep; overrides --load")
+    p.add_argument("--mix", default="c4", choices=["c4", "plain-spheres"])
     p.add_argument("--small", action="store_true", help="small scenes and resolutions (tests)")
     a = p.parse_args(argv)
     specs, keep = build_scenes(a.small)
     res = [(32, 32), (64, 48), (96, 64), (128, 72)] if a.small else RESOLUTIONS
     spps = [1, 2, 4, 8] if a.small else SPPS
-    reqs = make_requests(a.requests, specs, a.seed, res, spps)
+    if a.mix == "plain-spheres":
+        reqs = make_requests(a.requests, specs, a.seed, res, spps, scene_choices=[1], guided=False)
+    else:
+        reqs = make_requests(a.requests, specs, a.seed, res, spps)
+    loads = [a.load] if a.loads is None else [float(x) for x in a.loads.split(",") if x.strip()]
     srv = rt.Server(rt.server_options(wave_paths=a.wave_paths, max_jobs=a.max_jobs, max_depth=32,
                                       policy={"fair": rt.SERVE_FAIR, "fifo": rt.SERVE_FIFO,
                                               "srpt": rt.SERVE_SRPT}[a.policy]))
@@ -170,20 +185,28 @@ def main(argv=None):
         return out
 
     sat = phase([0.0] * len(reqs))
-    rate = a.load * len(reqs) / sat["makespan_s"]
-    gaps = np.random.default_rng(a.seed + 2).exponential(1.0 / rate, len(reqs))
-    arrivals = np.cumsum(gaps) - gaps[0]
-    loaded = phase(arrivals, sat["aggregate_Mpaths_s"])
+    curve = []
+    for load in loads:
+        rate = load * len(reqs) / sat["makespan_s"]
+        gaps = np.random.default_rng(a.seed + 2).exponential(1.0 / rate, len(reqs))
+        arrivals = np.cumsum(gaps) - gaps[0]
+        pt = phase(arrivals, sat["aggregate_Mpaths_s"])
+        pt["load"], pt["rate_jobs_s"] = load, rate
+        curve.append(pt)
     stats = srv.stats()
     srv.close()
-    line = {"metric": "serving time-to-image", "unit": "ms", "higher_is_better": False,
-            "p50_ms": loaded["p50_ms"], "p99_ms": loaded["p99_ms"], "p99_over_p50": loaded["p99_over_p50"],
-            "slowdown_p50": loaded["slowdown_p50"], "slowdown_p99": loaded["slowdown_p99"],
-            "slowdown_p99_over_p50": loaded["slowdown_p99_over_p50"],
-            "aggregate_Mpaths_s": loaded["aggregate_Mpaths_s"], "load": a.load, "rate_jobs_s": rate,
-            "saturation": sat, "loaded": loaded, "policy": a.policy,
+    line = {"metric": "serving time-to-image", "unit": "ms", "higher_is_better": False, "mix": a.mix,
+            "policy": a.policy, "wave_paths": a.wave_paths, "saturation": sat, "curve": curve,
             "guided_requests": int(sum(r["guided"] for r in reqs)),
             "server": stats, "data": "synthetic", "small": a.small}
+    for pt in curve:  # the headline point: the load closest to 0.8
+        if abs(pt["load"] - 0.8) <= min(abs(q["load"] - 0.8) for q in curve):
+            line.update(p50_ms=pt["p50_ms"], p99_ms=pt["p99_ms"], p99_over_p50=pt["p99_over_p50"],
+                        slowdown_p50=pt["slowdown_p50"], slowdown_p99=pt["slowdown_p99"],
+                        slowdown_p99_over_p50=pt["slowdown_p99_over_p50"],
+                        aggregate_Mpaths_s=pt["aggregate_Mpaths_s"], load=pt["load"], rate_jobs_s=pt["rate_jobs_s"],
+                        loaded=pt)
+            break
     print(json.dumps(line))
     return line
 

@@ -186,3 +186,71 @@ def test_medium_step_budget_is_reported_as_a_watchdog_error():
     r2.render()
     r2.synchronize()
     assert r2.stats()["watchdog_walks"] == 0
+
+
+@pytest.mark.gpu
+def test_c0_cornell_exact_configuration():
+    """C0 exactly: Cornell box, 34 triangles, 256x256, 16 spp, max depth 8,
+    Russian roulette from depth 3, PCG32 seed 1, linear FP32 output; same
+    streams as the FP32 oracle, then an independent stream within 3 SE."""
+    spec = scenes.cornell(256, 256, 16, seed=1)
+    st = spec.settings
+    assert (st["width"], st["height"], st["spp"], st["max_depth"], st["rr_depth"], st["rng"], st["seed"]) == \
+        (256, 256, 16, 8, 3, rt.RNG_PCG32, 1)
+    assert sum(len(m.triangles()) for m in spec.meshes) == 34
+    r, gpu, cpu, alb, nrm = render_both(spec)
+    agree = pixel_agreement(gpu, cpu)
+    mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
+    print(f"C0: pixels agreeing {agree:.5f}, means {mg:.6f} / {mc:.6f}")
+    assert agree >= 0.99
+    assert abs(mg - mc) <= 1e-3 * abs(mc)
+    o = rt.options(**dict(st, seed=2))
+    ind = pyoracle.OracleScene(spec).render(o, rt.camera(**spec.camera))[0][..., :3].astype(np.float64).mean(-1)
+    d = gpu[..., :3].astype(np.float64).mean(-1) - ind
+    se = d.std() / np.sqrt(d.size)
+    assert abs(d.mean()) <= 3 * se
+
+
+@pytest.mark.gpu
+def test_c2_media_full_grid_same_streams():
+    """C2's medium at full size: the 128^3 fBm density grid (sigma_t 0-5,
+    albedo 0.9, HG g = 0.6) with its 8^3 majorant grid inside the IOR-1.33
+    sphere, the fog, the area light and the sky, depth 32, at 160x90 and
+    16 spp (the oracle's time bounds the resolution)."""
+    spec = scenes.media(160, 90, 16, grid_res=128, env_size=(512, 256))
+    grid = [m for m in spec.media if m["type"] == rt.MEDIUM_GRID][0]
+    assert grid["density"].shape == (128, 128, 128) and grid["majorant_res"] == 8
+    assert 0.0 <= grid["density"].min() and grid["density"].max() <= 5.0
+    r, gpu, cpu, alb, nrm = render_both(spec)
+    agree = pixel_agreement(gpu, cpu)
+    mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
+    print(f"C2 full grid: agreeing {agree:.4f} means {mg:.5f} / {mc:.5f}")
+    assert agree >= 0.90
+    assert abs(mg - mc) <= 2e-2 * abs(mc)
+    r.synchronize()  # no walk ran out of its step budget
+
+
+def _point_light_cornell(w, h, spp, seed=1):
+    """The Cornell box lit by a point light (radiant intensity 1.2 W/sr) in
+    place of the ceiling quad."""
+    spec = scenes.cornell(w, h, spp, seed=seed)
+    spec.lights[:] = [dict(type=rt.LIGHT_POINT, position=(0.5, 0.8, 0.4), radiance=(1.2, 1.0, 0.8))]
+    return spec
+
+
+@pytest.mark.gpu
+def test_point_light_scene_same_and_independent_streams():
+    """Point lights (no reference counterpart; NEE only, MIS weight 1):
+    same-stream parity with the oracle and an independent stream within 3 SE."""
+    spec = _point_light_cornell(96, 96, 16)
+    r, gpu, cpu, alb, nrm = render_both(spec)
+    agree = pixel_agreement(gpu, cpu)
+    mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
+    print(f"point light: agreeing {agree:.4f} means {mg:.6f} / {mc:.6f}")
+    assert mg > 0.01
+    assert agree >= 0.97
+    assert abs(mg - mc) <= 1e-3 * abs(mc)
+    o = rt.options(**dict(spec.settings, seed=9))
+    ind = pyoracle.OracleScene(spec).render(o, rt.camera(**spec.camera))[0][..., :3].astype(np.float64).mean(-1)
+    d = gpu[..., :3].astype(np.float64).mean(-1) - ind
+    assert abs(d.mean()) <= 3 * d.std() / np.sqrt(d.size)

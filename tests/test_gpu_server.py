@@ -152,11 +152,13 @@ def test_serve_bench_small(policy):
     finishes, and the device-busy fraction from the server's wave events is a
     fraction of the phase's wall time."""
     from optixrender_b200 import serve_bench
-    line = serve_bench.main(["--small", "--requests", "24", "--policy", policy, "--wave-paths", str(1 << 15)])
-    for ph in ("saturation", "loaded"):
-        assert line[ph]["requests"] == 24
-        assert 0.0 < line[ph]["device_busy_fraction"] <= 1.05
-    assert line["server"]["jobs_done"] == 24 * 2 + 4
+    line = serve_bench.main(["--small", "--requests", "24", "--policy", policy, "--wave-paths", str(1 << 15),
+                             "--loads", "0.5,0.8"])
+    for ph in [line["saturation"]] + line["curve"]:
+        assert ph["requests"] == 24
+        assert 0.0 < ph["device_busy_fraction"] <= 1.05
+    assert [pt["load"] for pt in line["curve"]] == [0.5, 0.8] and line["load"] == 0.8
+    assert line["server"]["jobs_done"] == 24 * 3 + 4
     assert line["p99_ms"] >= line["p50_ms"] > 0.0
 
 

@@ -199,3 +199,34 @@ def test_guided_bsdf_terms(mtype):
     else:
         assert z_eval > 10.0
     assert abs(quad - plain) <= 3 * se + 2e-3 * abs(plain)
+
+
+@pytest.mark.gpu
+def test_point_light_sample_and_eval_match_fp64():
+    """Point lights on the device (sample_light / evaluate_light) against the
+    FP64 oracle, which itself is pinned to the reference's sphere light in the
+    small-radius limit (tests/test_oracle_pins.py): radiance I / d^2, the unit
+    direction and distance to the light, pdf 1 (a delta light); a ray can never
+    hit one (evaluation gives zero radiance and pdf)."""
+    rng = np.random.default_rng(23)
+    lights = [rt.light(rt.LIGHT_POINT, position=(0.3, 1.2, -0.4), radiance=(2.0, 3.0, 4.0)),
+              rt.light(rt.LIGHT_POINT, position=(-1.0, 0.2, 0.9), radiance=(0.5, 0.25, 0.125))]
+    n = 4000
+    ls = np.zeros((n, 16), np.float32)
+    ls[:, 0:3] = rng.uniform(-1.5, 1.5, (n, 3))
+    ls[:, 3:5] = rng.random((n, 2))
+    ls[:, 5] = rng.integers(0, len(lights), n)
+    gpu = rt.verify_shading(rt.VERIFY_LIGHT_SAMPLE, ls, MATS, lights, MEDIA)
+    f64 = pyoracle.shading(rt.VERIFY_LIGHT_SAMPLE, ls, MATS, lights, MEDIA, precision=64)
+    e = rel_err(gpu, f64, list(range(8)))
+    print(f"point light sample: within 1e-5 {np.mean(e <= 1e-5):.4f}, max {e.max():.2e}")
+    assert np.mean(e <= 1e-5) >= 0.995 and e.max() < 1e-4
+    assert np.all(gpu[:, 3] == 1.0)
+    le = np.zeros((n, 16), np.float32)
+    le[:, 0:3] = rng.uniform(-1.0, 1.0, (n, 3))
+    d = rng.normal(size=(n, 3))
+    le[:, 3:6] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    le[:, 6] = 3.0e38
+    le[:, 7] = rng.integers(0, len(lights), n)
+    ev = rt.verify_shading(rt.VERIFY_LIGHT_EVAL, le, MATS, lights, MEDIA)
+    assert np.all(ev[:, 0:4] == 0.0)

@@ -150,3 +150,56 @@ def test_struct_defaults_agree_with_the_reference():
         prod = fields(getattr(rt, kind)(type=0))
         for src in srcs:
             assert fields(getattr(src, kind)(type=0)) == prod, kind
+
+
+def test_point_light_is_the_small_sphere_limit_of_the_reference():
+    """Point lights have no reference counterpart; their nearest analogue is
+    the reference's sphere light (SampleSphere, core/cuda/Light.h:118-141) as
+    its radius goes to zero.  A uniformly emitting sphere of radius r and
+    radiance I / (pi r^2) that lies wholly above a surface's horizon gives that
+    surface exactly the irradiance of a point of intensity I, I cos / d^2, for
+    any r; so the reference's own sphere sampling (a 16 x 16 stratified grid of
+    its two random numbers, r / d <= 0.05) must reproduce the oracle's point
+    light within the FP32 rounding of its cone (1 - cos theta_max)."""
+    libs = pyoracle.ref_libs()
+    if libs is None:
+        pytest.skip("reference host build not present (oracle/_ref)")
+    shading = libs[0]
+    F = C.POINTER(C.c_float)
+    rng = np.random.default_rng(17)
+    c, I, radius = np.array([0.2, 1.1, -0.3]), np.array([2.0, 3.0, 4.0]), 0.04
+    point = rt.light(rt.LIGHT_POINT, position=tuple(c), radiance=tuple(I))
+    sphere = rt.light(rt.LIGHT_SPHERE, position=tuple(c), radius=radius,
+                      radiance=tuple(I / (np.pi * radius * radius)))
+    p = c + rng.normal(size=(400, 3)) * 0.8
+    p = p[np.linalg.norm(p - c, axis=1) > 0.8]
+    to_c = (c - p) / np.linalg.norm(c - p, axis=1, keepdims=True)
+    nrm = to_c + rng.normal(size=p.shape) * 0.5
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    keep = (nrm * to_c).sum(1) > 0.3  # the whole sphere above the horizon
+    p, nrm = p[keep], nrm[keep]
+    n_pts, k = len(p), 256
+    g = (np.arange(16) + 0.5) / 16
+    u = np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+    x = np.zeros((n_pts * k, 16), np.float32)
+    x[:, 0:3] = np.repeat(p, k, 0)
+    x[:, 3:5] = np.tile(u, (n_pts, 1))
+    Ls = (rt.Light * 1)(sphere)
+    M = (rt.Material * 1)(rt.material(rt.MAT_DIFFUSE))
+    D = (rt.Medium * 1)(rt.medium())
+    y = np.zeros((n_pts * k, 8), np.float32)
+    shading.ref_shading(rt.VERIFY_LIGHT_SAMPLE, C.cast(M, C.c_void_p), 1, C.cast(Ls, C.c_void_p), 1,
+                        C.cast(D, C.c_void_p), 0, x.ctypes.data_as(F), x.shape[0], y.ctypes.data_as(F))
+    cos = np.maximum(0.0, (y[:, 4:7].astype(np.float64) * np.repeat(nrm, k, 0)).sum(1))
+    e_sphere = (y[:, 0:3] * (cos / y[:, 3])[:, None]).reshape(n_pts, k, 3).mean(1)
+    xp = np.zeros((n_pts, 16), np.float32)
+    xp[:, 0:3] = p
+    yp = pyoracle.shading(rt.VERIFY_LIGHT_SAMPLE, xp, [rt.material(rt.MAT_DIFFUSE)], [point], [], precision=64)
+    assert np.all(yp[:, 3] == 1.0)  # a delta light: its sample carries weight 1
+    np.testing.assert_allclose(yp[:, 7], np.linalg.norm(p - c, axis=1), rtol=1e-6)
+    np.testing.assert_allclose(yp[:, 4:7], to_c[keep], rtol=0, atol=1e-6)
+    e_point = yp[:, 0:3] * np.maximum(0.0, (yp[:, 4:7] * nrm).sum(1))[:, None]
+    assert n_pts > 100
+    rel = np.abs(e_sphere - e_point) / e_point
+    print(f"point vs sphere: max rel {rel.max():.2e}, mean {rel.mean():.2e} over {n_pts} points")
+    assert rel.max() < 2e-3
