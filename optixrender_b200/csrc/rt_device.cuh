@@ -16,36 +16,71 @@
 namespace rtd {
 
 // ------------------------------------------------------------------ vec3
-struct v3 {
-    float x, y, z;
-    RT_HD v3() : x(0.f), y(0.f), z(0.f) {}
-    RT_HD explicit v3(float s) : x(s), y(s), z(s) {}
-    RT_HD v3(float a, float b, float c) : x(a), y(b), z(c) {}
-    RT_HD float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+// A 3-vector of float (v3, the renderer's arithmetic) or double (v3d, the
+// BSDF sampler's).  The scalar of a mixed vector-scalar expression converts
+// to the vector's type, so float literals keep their float value.
+template <class R>
+struct vec3t {
+    R x, y, z;
+    RT_HD vec3t() : x(R(0)), y(R(0)), z(R(0)) {}
+    RT_HD explicit vec3t(R s) : x(s), y(s), z(s) {}
+    RT_HD vec3t(R a, R b, R c) : x(a), y(b), z(c) {}
+    RT_HD R operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
 };
-RT_HD v3 operator+(v3 a, v3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-RT_HD v3 operator-(v3 a, v3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-RT_HD v3 operator*(v3 a, v3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
-RT_HD v3 operator/(v3 a, v3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
-RT_HD v3 operator*(v3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-RT_HD v3 operator*(float s, v3 a) { return v3(s * a.x, s * a.y, s * a.z); }
-RT_HD v3 operator/(v3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
-RT_HD v3 operator+(v3 a, float s) { return v3(a.x + s, a.y + s, a.z + s); }
-RT_HD v3 operator-(float s, v3 a) { return v3(s - a.x, s - a.y, s - a.z); }
-RT_HD v3 operator-(v3 a, float s) { return v3(a.x - s, a.y - s, a.z - s); }
-RT_HD v3 operator-(v3 a) { return v3(-a.x, -a.y, -a.z); }
-RT_HD v3& operator+=(v3& a, v3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
-RT_HD v3& operator*=(v3& a, v3 b) { a.x *= b.x; a.y *= b.y; a.z *= b.z; return a; }
-RT_HD v3& operator*=(v3& a, float s) { a.x *= s; a.y *= s; a.z *= s; return a; }
-RT_HD v3& operator/=(v3& a, float s) { a.x /= s; a.y /= s; a.z /= s; return a; }
-RT_HD float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-RT_HD v3 cross(v3 a, v3 b) { return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
-RT_HD float length(v3 v) { return sqrtf(dot(v, v)); }
+using v3 = vec3t<float>;
+using v3d = vec3t<double>;
+template <class T>
+struct same_t {
+    using type = T;
+};
+template <class R> using sc_t = typename same_t<R>::type;  // not deduced: takes the vector's scalar type
+
+template <class R> RT_HD vec3t<R> operator+(vec3t<R> a, vec3t<R> b) { return vec3t<R>(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class R> RT_HD vec3t<R> operator-(vec3t<R> a, vec3t<R> b) { return vec3t<R>(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class R> RT_HD vec3t<R> operator*(vec3t<R> a, vec3t<R> b) { return vec3t<R>(a.x * b.x, a.y * b.y, a.z * b.z); }
+template <class R> RT_HD vec3t<R> operator/(vec3t<R> a, vec3t<R> b) { return vec3t<R>(a.x / b.x, a.y / b.y, a.z / b.z); }
+template <class R> RT_HD vec3t<R> operator*(vec3t<R> a, sc_t<R> s) { return vec3t<R>(a.x * s, a.y * s, a.z * s); }
+template <class R> RT_HD vec3t<R> operator*(sc_t<R> s, vec3t<R> a) { return vec3t<R>(s * a.x, s * a.y, s * a.z); }
+template <class R> RT_HD vec3t<R> operator/(vec3t<R> a, sc_t<R> s) { return vec3t<R>(a.x / s, a.y / s, a.z / s); }
+template <class R> RT_HD vec3t<R> operator+(vec3t<R> a, sc_t<R> s) { return vec3t<R>(a.x + s, a.y + s, a.z + s); }
+template <class R> RT_HD vec3t<R> operator-(sc_t<R> s, vec3t<R> a) { return vec3t<R>(s - a.x, s - a.y, s - a.z); }
+template <class R> RT_HD vec3t<R> operator-(vec3t<R> a, sc_t<R> s) { return vec3t<R>(a.x - s, a.y - s, a.z - s); }
+template <class R> RT_HD vec3t<R> operator-(vec3t<R> a) { return vec3t<R>(-a.x, -a.y, -a.z); }
+template <class R> RT_HD vec3t<R>& operator+=(vec3t<R>& a, vec3t<R> b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+template <class R> RT_HD vec3t<R>& operator*=(vec3t<R>& a, vec3t<R> b) { a.x *= b.x; a.y *= b.y; a.z *= b.z; return a; }
+template <class R> RT_HD vec3t<R>& operator*=(vec3t<R>& a, sc_t<R> s) { a.x *= s; a.y *= s; a.z *= s; return a; }
+template <class R> RT_HD vec3t<R>& operator/=(vec3t<R>& a, sc_t<R> s) { a.x /= s; a.y /= s; a.z /= s; return a; }
+template <class R> RT_HD R dot(vec3t<R> a, vec3t<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> RT_HD vec3t<R> cross(vec3t<R> a, vec3t<R> b) {
+    return vec3t<R>(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+// Math of either precision: the float forms are the ones the renderer has
+// always used (sqrtf, fabsf, ...); the double forms are CUDA's double ones.
+RT_HD float sqrt_r(float x) { return sqrtf(x); }
+RT_HD double sqrt_r(double x) { return sqrt(x); }
+RT_HD float fabs_r(float x) { return fabsf(x); }
+RT_HD double fabs_r(double x) { return fabs(x); }
+RT_HD float fmin_r(float a, float b) { return fminf(a, b); }
+RT_HD double fmin_r(double a, double b) { return fmin(a, b); }
+RT_HD float fmax_r(float a, float b) { return fmaxf(a, b); }
+RT_HD double fmax_r(double a, double b) { return fmax(a, b); }
+// a float literal beside a double promotes to double
+RT_HD double fmin_r(float a, double b) { return fmin(double(a), b); }
+RT_HD double fmin_r(double a, float b) { return fmin(a, double(b)); }
+RT_HD double fmax_r(float a, double b) { return fmax(double(a), b); }
+RT_HD double fmax_r(double a, float b) { return fmax(a, double(b)); }
+RT_HD void sincos_r(float a, float* s, float* c) { sincosf(a, s, c); }
+RT_HD void sincos_r(double a, double* s, double* c) { sincos(a, s, c); }
+template <class R> RT_HD R length(vec3t<R> v) { return sqrt_r(dot(v, v)); }
 // Component-wise division by the length, as gdt's normalize (vec.h:306-310).
-RT_HD v3 normalize(v3 v) { return v / sqrtf(dot(v, v)); }
-RT_HD bool any_nan(v3 v) { return v.x != v.x || v.y != v.y || v.z != v.z; }
+template <class R> RT_HD vec3t<R> normalize(vec3t<R> v) { return v / sqrt_r(dot(v, v)); }
+template <class R> RT_HD bool any_nan(vec3t<R> v) { return v.x != v.x || v.y != v.y || v.z != v.z; }
 RT_HD float sqr(float x) { return x * x; }
+RT_HD double sqr(double x) { return x * x; }
 RT_HD float mixf(float x, float y, float t) { return x * (1.0f - t) + y * t; }
+template <class R> RT_HD R mix_r(R x, R y, R t) { return x * (R(1) - t) + y * t; }
+RT_HD v3d to_d(v3 a) { return v3d(double(a.x), double(a.y), double(a.z)); }
+RT_HD v3 to_f(v3d a) { return v3(float(a.x), float(a.y), float(a.z)); }
 RT_HD v3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 RT_HD float4 f4(v3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 RT_HD v3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
@@ -60,6 +95,13 @@ constexpr float kEps = 1e-4f;                                  // core/cuda/Util
 constexpr float kPi = 3.14159265358979323846f;                 // Utils.h:11
 constexpr float kTwoPi = 6.28318530717958647692f;              // Utils.h:14
 constexpr float kInvPi = 0.318309886183790671538f;             // Utils.h:13
+// The same constants rounded to either precision (float: identical to the above).
+template <class R>
+struct Kc {
+    static constexpr R pi = R(3.14159265358979323846);
+    static constexpr R two_pi = R(6.28318530717958647692);
+    static constexpr R inv_pi = R(0.318309886183790671538);
+};
 
 // ------------------------------------------------------------------ random
 // gdt::LCG<16> of the reference (common/gdt/gdt/random/random.h:54-87).

@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                                 v3 att = evaluate_phase(med, V, sd, phase_pdf);
                                 float w = l.type == RT_LIGHT_POINT ? 1.0f : power_heuristic(lp, phase_pdf * tp2);
                                 nee_l = w * (tr2 / tp2) * lr * att * history / lp;
-                                sh1 = true;
+                                sh1 = !(nee_l.x == 0.0f && nee_l.y == 0.0f && nee_l.z == 0.0f);
                                 s1o = pos;
                                 s1d = sd;
                                 s1t = ld - kEps;
@@ -491,7 +491,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                                 w = power_heuristic(lp, bpdf * tp2);
                             }
                             nee_e = w * thh * lr * f * ct * history / lp;
-                            sh0 = true;
+                            // a shadow ray only decides whether its contribution counts:
+                            // one with none (the light below the horizon, f = 0) is not
+                            // traced (it halves the shadow rays of the benchmark frame)
+                            sh0 = !(nee_e.x == 0.0f && nee_e.y == 0.0f && nee_e.z == 0.0f);
                             s0o = pos;
                             s0d = sd;
                             s0t = FLT_MAX;
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                                 if (l.type != RT_LIGHT_POINT) w = power_heuristic(lp, bpdf * tp2);
                             }
                             nee_l = w * thh * lr * f * ct * history / lp;
-                            sh1 = true;
+                            sh1 = !(nee_l.x == 0.0f && nee_l.y == 0.0f && nee_l.z == 0.0f);
                             s1o = pos;
                             s1d = sd;
                             s1t = ld - kEps;

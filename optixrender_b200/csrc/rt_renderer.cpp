@@ -67,6 +67,12 @@ rt_status upload_scene(const rt_scene& s, DeviceScene& ds, cudaStream_t st, bool
         if (!rth::build_cwbvh(s.tv.data(), nt, bvh, err)) return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
     } else if (!rth::build_cwbvh_gpu(s.tv.data(), nt, bvh, err, st)) {
         return fail(RT_ERR_CUDA, err);
+    } else if (!rth::validate_cwbvh(bvh, s.tv.data(), nt, err)) {
+        // The device build is checked like the host build checks its own
+        // tree (every index in range, every quantised box containing what it
+        // bounds).  Inputs it gets wrong - coordinates spanning the whole
+        // float range - are built again on the host.
+        if (!rth::build_cwbvh(s.tv.data(), nt, bvh, err)) return fail(RT_ERR_UNSUPPORTED, "BVH build failed: " + err);
     }
     if (rt_status dst = check_bvh_depth(bvh.depth)) return dst;
     ds.bvh_depth = bvh.depth;

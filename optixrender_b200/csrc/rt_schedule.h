@@ -1,11 +1,13 @@
 // rt_schedule.h - the render server's wave planner, without CUDA.
 //
 // Given the admitted jobs that still have paths to issue (in admission
-// order), the policy picks the group the next wave serves - plain jobs of
-// any scene (group 0) or the guided jobs of scene k (group k + 1), since one
-// wave samples at most one guiding network - and then how many paths each of
-// that group's jobs contributes, in at most `max_segments` segments of a
-// wave of `capacity` path slots:
+// order), the policy picks the group the next wave serves and then how many
+// paths each of that group's jobs contributes, in at most `max_segments`
+// segments of a wave of `capacity` path slots.  The server's groups are the
+// plain jobs of scenes without media or textures (group 0), the plain jobs of
+// scenes with them (group 1) and the guided jobs of scene k (group k + 2):
+// one wave runs one build of the shade kernel and samples at most one guiding
+// network, so a plain job's wave runs the same kernel as a Render() of it.
 //   FIFO: the oldest job's group; jobs in admission order take all they can.
 //   SRPT: the group of the job with the fewest paths left; jobs with the
 //         fewest paths left first (ties by admission).
@@ -26,7 +28,7 @@ enum : int { kPlanFair = 0, kPlanFifo = 1, kPlanSrpt = 2 };
 
 struct PlanJob {
     int64_t remaining;  // paths not yet issued (> 0)
-    int group;          // 0 plain, k + 1 guided on scene k
+    int group;          // jobs of one group may share a wave
 };
 
 struct PlanState {

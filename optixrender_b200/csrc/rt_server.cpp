@@ -105,7 +105,7 @@ struct rt_server {
     std::vector<std::unique_ptr<DeviceScene>> scenes;
     std::vector<SceneGuide> guides;  // one per scene; networks created at the first guided wave
     int64_t scene_bytes = 0;
-    int scene_features = 0;  // kFeatureMedia / kFeatureTextures of any resident scene
+    std::vector<int> scene_features;  // per scene: kFeatureMedia / kFeatureTextures
     std::map<int64_t, std::unique_ptr<Job>> jobs;
     std::deque<int64_t> queued;
     std::vector<int64_t> running;  // admission order
@@ -231,8 +231,19 @@ rt_status ensure_scene_guide(rt_server* s, int k) {
     return st;
 }
 
-// `gscene` >= 0: the wave samples the guiding network of that scene.
-Ctx make_ctx(rt_server* s, int gscene = -1) {
+// Wave groups (rt_schedule.h): plain jobs of scenes without media or
+// textures (the plain shade kernel), plain jobs of scenes with them and the
+// guided jobs of each scene (the full shade kernel).
+constexpr int kGroupPlain = 0, kGroupFull = 1, kGroupGuided0 = 2;
+int job_group(const rt_server* s, const rt_job_desc& d) {
+    if (d.guided) return kGroupGuided0 + d.scene;
+    return s->scene_features[size_t(d.scene)] != 0 ? kGroupFull : kGroupPlain;
+}
+
+// `group`: the wave's group; a guided group's wave samples the guiding
+// network of its scene.
+Ctx make_ctx(rt_server* s, int group) {
+    const int gscene = group >= kGroupGuided0 ? group - kGroupGuided0 : -1;
     Ctx c;
     std::memset(&c, 0, sizeof(c));
     c.jobs = s->job_table.as<JobDesc>();
@@ -260,7 +271,7 @@ Ctx make_ctx(rt_server* s, int gscene = -1) {
     c.wave_index = s->wave_index.as<int>();
     c.wave_ring = s->ring_size;
     c.max_depth = s->opt.max_depth;
-    c.features = s->scene_features | (gscene >= 0 ? kFeatureGuide : 0);
+    c.features = group == kGroupPlain ? 0 : group == kGroupFull ? kFeatureMedia | kFeatureTextures : kFeatureGuide;
     if (gscene >= 0) {
         const SceneGuide& g = s->guides[size_t(gscene)];
         c.G.mix = s->g_mix.as<rtg::Mixture>();
@@ -304,8 +315,9 @@ void issue_wave(rt_server* s, const Ctx& c0, int depth, int gscene, bool trainin
 // One captured wave per bounce count: raygen, (extend, shade, shadow) x depth,
 // resolve, advance of the wave ring.  A wave uses the graph of the deepest
 // job in it; each path still stops at its own job's max_depth.
-rt_status wave_graph(rt_server* s, int depth, int gscene, cudaGraphExec_t* out) {
-    const std::pair<int, int> key(depth, gscene + 1);
+rt_status wave_graph(rt_server* s, int depth, int group, cudaGraphExec_t* out) {
+    const int gscene = group >= kGroupGuided0 ? group - kGroupGuided0 : -1;
+    const std::pair<int, int> key(depth, group);
     auto it = s->graphs.find(key);
     if (it != s->graphs.end()) {
         *out = it->second;
@@ -313,7 +325,7 @@ rt_status wave_graph(rt_server* s, int depth, int gscene, cudaGraphExec_t* out) 
     }
     cudaGraph_t g = nullptr;
     SV_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin graph capture");
-    issue_wave(s, make_ctx(s, gscene), depth, gscene, false);
+    issue_wave(s, make_ctx(s, group), depth, gscene, false);
     SV_CUDA(cudaStreamEndCapture(s->stream, &g), "end graph capture");
     cudaGraphExec_t ge = nullptr;
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
@@ -441,7 +453,7 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
         Job& j = *s->jobs[id];
         if (j.issued < j.total) {
             active.push_back(&j);
-            pj.push_back({j.total - j.issued, j.desc.guided ? j.desc.scene + 1 : 0});
+            pj.push_back({j.total - j.issued, job_group(s, j.desc)});
         }
     }
     std::vector<std::pair<Job*, int64_t>> plan;
@@ -450,7 +462,8 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
     WaveParams wp;
     std::memset(&wp, 0, sizeof(wp));
     int filled = 0, depth = 1;
-    const int gscene = plan.empty() || !plan.front().first->desc.guided ? -1 : plan.front().first->desc.scene;
+    const int group = plan.empty() ? kGroupPlain : job_group(s, plan.front().first->desc);
+    const int gscene = group >= kGroupGuided0 ? group - kGroupGuided0 : -1;
     std::vector<Job*> completing;
     for (auto& pj : plan) {
         Job& j = *pj.first;
@@ -475,7 +488,7 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
         }
         cudaGraphExec_t graph = nullptr;
         if (!training) {
-            rt_status gs = wave_graph(s, depth, gscene, &graph);
+            rt_status gs = wave_graph(s, depth, group, &graph);
             if (gs) return gs;
         }
         int pos = s->ring_pos;
@@ -488,7 +501,7 @@ rt_status step_locked(rt_server* s, int32_t* did_work, cudaEvent_t* blocked) {
             // launched directly: the wave records training samples, then the
             // scene's network takes guide_steps Adam steps on batches of them
             SceneGuide& g = s->guides[size_t(gscene)];
-            issue_wave(s, make_ctx(s, gscene), depth, gscene, true);
+            issue_wave(s, make_ctx(s, group), depth, gscene, true);
             for (int k = 0; k < s->opt.guide_steps; k++) {
                 SV_CUDA(cudaMemsetAsync(s->g_wsum.ptr, 0, sizeof(float), s->stream), "guide batch");
                 rtgh::launch_batch(s->g_buf.as<float4>(), s->g_count.as<int>(), int(s->g_buf.bytes / 32),
@@ -675,18 +688,14 @@ rt_status rt_server_add_scene(rt_server* s, const rt_scene* scene, int32_t* id) 
     std::unique_ptr<DeviceScene> ds(new DeviceScene());
     rt_status st = upload_scene(*scene, *ds, s->stream);
     if (st) return st;
-    const int feat = (ds->view.num_media > 0 ? kFeatureMedia : 0) | (ds->view.num_tex > 0 ? kFeatureTextures : 0);
-    const bool need_tex = ds->view.num_tex > 0 && !s->mat_tex.ptr;
-    if (need_tex || (s->scene_features | feat) != s->scene_features) {
-        // graphs captured without the textured-material buffer, or with the
-        // shade kernel that leaves out media and textures, are recaptured
+    if (ds->view.num_tex > 0 && !s->mat_tex.ptr) {
         SV_CUDA(cudaStreamSynchronize(s->stream), "rt_server_add_scene");
-        if (need_tex)
-            SV_CUDA(s->mat_tex.alloc(size_t(s->capacity) * sizeof(DevMaterial)), "allocate textured materials");
-        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+        SV_CUDA(s->mat_tex.alloc(size_t(s->capacity) * sizeof(DevMaterial)), "allocate textured materials");
+        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);  // captured without the buffer
         s->graphs.clear();
-        s->scene_features |= feat;
     }
+    s->scene_features.push_back((ds->view.num_media > 0 ? kFeatureMedia : 0) |
+                                (ds->view.num_tex > 0 ? kFeatureTextures : 0));
     s->scene_bytes += int64_t(ds->bytes);
     s->scenes.push_back(std::move(ds));
     SceneGuide g;

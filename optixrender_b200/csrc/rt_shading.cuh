@@ -36,16 +36,6 @@ RT_D v3 uniform_sample_cone(float s0, float s1, float cos_angle) {  // Sampling.
     return normalize(v3(st * cp, st * sp, ct));
 }
 RT_D float uniform_pdf_cone(float cos_angle) { return 1.0f / (kTwoPi * (1.0f - cos_angle)); }
-RT_D v3 cosine_sample_hemisphere(float s0, float s1) {  // Sampling.h:56-69
-    float r = sqrtf(s0);
-    float phi = kTwoPi * s1;
-    float sp, cp;
-    sincosf(phi, &sp, &cp);
-    v3 p(r * cp, r * sp, 0.0f);
-    p.z = sqrtf(fmaxf(0.0f, 1.0f - p.x * p.x - p.y * p.y));
-    return normalize(p);
-}
-RT_D float cosine_pdf(float ndotl) { return ndotl * kInvPi; }
 RT_D v3 uniform_sample_sphere(float s0, float s1) {  // Sampling.h:76-88
     float phi = kTwoPi * s0;
     float ct = 1.0f - 2.0f * s1;
@@ -55,139 +45,167 @@ RT_D v3 uniform_sample_sphere(float s0, float s1) {  // Sampling.h:76-88
     return normalize(v3(st * cp, st * sp, ct));
 }
 
+template <class R>
+RT_D vec3t<R> cosine_sample_hemisphere(R s0, R s1) {  // Sampling.h:56-69
+    R r = sqrt_r(s0);
+    R phi = Kc<R>::two_pi * s1;
+    R sp, cp;
+    sincos_r(phi, &sp, &cp);
+    vec3t<R> p(r * cp, r * sp, 0.0f);
+    p.z = sqrt_r(fmax_r(0.0f, 1.0f - p.x * p.x - p.y * p.y));
+    return normalize(p);
+}
+template <class R>
+RT_D R cosine_pdf(R ndotl) { return ndotl * Kc<R>::inv_pi; }
 // ------------------------------------------------------------ frames
-RT_D v3 reflect(v3 v, v3 n) { return normalize(v - 2.0f * dot(v, n) * n); }  // Utils.h:28-30
-RT_D v3 refract(v3 v, v3 n, float eta) {                                       // Utils.h:32-38
-    float ct = fminf(dot(-v, n), 1.0f);
-    v3 perp = eta * (v + ct * n);
-    v3 par = -sqrtf(fabsf(1.0f - dot(perp, perp))) * n;
+template <class R>
+RT_D vec3t<R> reflect(vec3t<R> v, vec3t<R> n) { return normalize(v - 2.0f * dot(v, n) * n); }  // Utils.h:28-30
+template <class R>
+RT_D vec3t<R> refract(vec3t<R> v, vec3t<R> n, sc_t<R> eta) {                                       // Utils.h:32-38
+    R ct = fmin_r(dot(-v, n), 1.0f);
+    vec3t<R> perp = eta * (v + ct * n);
+    vec3t<R> par = -sqrt_r(fabs_r(1.0f - dot(perp, perp))) * n;
     return normalize(perp + par);
 }
-RT_D void frame_axes(v3 up, v3& B, v3& C) {  // Utils.h:99-109
-    if (fabsf(up.x) > fabsf(up.y)) {
-        float inv = 1.0f / sqrtf(up.x * up.x + up.z * up.z);
-        C = v3(up.z * inv, 0.0f, -up.x * inv);
+template <class R>
+RT_D void frame_axes(vec3t<R> up, vec3t<R>& B, vec3t<R>& C) {  // Utils.h:99-109
+    if (fabs_r(up.x) > fabs_r(up.y)) {
+        R inv = 1.0f / sqrt_r(up.x * up.x + up.z * up.z);
+        C = vec3t<R>(up.z * inv, 0.0f, -up.x * inv);
     } else {
-        float inv = 1.0f / sqrtf(up.y * up.y + up.z * up.z);
-        C = v3(0.0f, up.z * inv, -up.y * inv);
+        R inv = 1.0f / sqrt_r(up.y * up.y + up.z * up.z);
+        C = vec3t<R>(0.0f, up.z * inv, -up.y * inv);
     }
     B = cross(C, up);
 }
-RT_D v3 to_local(v3 d, v3 up) {
-    v3 B, C;
+template <class R>
+RT_D vec3t<R> to_local(vec3t<R> d, vec3t<R> up) {
+    vec3t<R> B, C;
     frame_axes(up, B, C);
-    return v3(dot(d, B), dot(d, C), dot(d, up));
+    return vec3t<R>(dot(d, B), dot(d, C), dot(d, up));
 }
-RT_D v3 to_world(v3 d, v3 up) {  // Utils.h:117-129
-    v3 B, C;
+template <class R>
+RT_D vec3t<R> to_world(vec3t<R> d, vec3t<R> up) {  // Utils.h:117-129
+    vec3t<R> B, C;
     frame_axes(up, B, C);
     return normalize(d.x * B + d.y * C + d.z * up);
 }
 
 // ------------------------------------------------------------ microfacet
-RT_D v3 fresnel_conductor(v3 V, v3 H, v3 er, v3 ei) {  // Microfacet.h:22-46
-    float c = dot(V, H), c2 = c * c, s2 = 1.0f - c2, s4 = s2 * s2;
-    v3 t1 = er * er - ei * ei - s2;
-    v3 a2 = t1 * t1 + 4.0f * ei * ei * er * er;
-    a2 = v3(sqrtf(fmaxf(0.0f, a2.x)), sqrtf(fmaxf(0.0f, a2.y)), sqrtf(fmaxf(0.0f, a2.z)));
-    v3 a = 0.5f * (a2 + t1);
-    a = v3(sqrtf(fmaxf(0.0f, a.x)), sqrtf(fmaxf(0.0f, a.y)), sqrtf(fmaxf(0.0f, a.z)));
-    v3 term1 = a2 + s2, term2 = 2.0f * c * a, term3 = a2 * c2 + s4, term4 = term2 * s2;
-    v3 rs = (term1 - term2) / (term1 + term2);
-    v3 rp = rs * (term3 - term4) / (term3 + term4);
+template <class R>
+RT_D vec3t<R> fresnel_conductor(vec3t<R> V, vec3t<R> H, vec3t<R> er, vec3t<R> ei) {  // Microfacet.h:22-46
+    R c = dot(V, H), c2 = c * c, s2 = 1.0f - c2, s4 = s2 * s2;
+    vec3t<R> t1 = er * er - ei * ei - s2;
+    vec3t<R> a2 = t1 * t1 + 4.0f * ei * ei * er * er;
+    a2 = vec3t<R>(sqrt_r(fmax_r(0.0f, a2.x)), sqrt_r(fmax_r(0.0f, a2.y)), sqrt_r(fmax_r(0.0f, a2.z)));
+    vec3t<R> a = 0.5f * (a2 + t1);
+    a = vec3t<R>(sqrt_r(fmax_r(0.0f, a.x)), sqrt_r(fmax_r(0.0f, a.y)), sqrt_r(fmax_r(0.0f, a.z)));
+    vec3t<R> term1 = a2 + s2, term2 = 2.0f * c * a, term3 = a2 * c2 + s4, term4 = term2 * s2;
+    vec3t<R> rs = (term1 - term2) / (term1 + term2);
+    vec3t<R> rp = rs * (term3 - term4) / (term3 + term4);
     return 0.5f * (rs + rp);
 }
-RT_D v3 average_fresnel_conductor(v3 eta, v3 k) {  // Microfacet.h:48-70
-    float rr[3], ee[3];
+template <class R>
+RT_D vec3t<R> average_fresnel_conductor(vec3t<R> eta, vec3t<R> k) {  // Microfacet.h:48-70
+    R rr[3], ee[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        float e = eta[i], kk = k[i];
-        float r = (sqr(e - 1.0f) + sqr(kk)) / (sqr(e + 1.0f) + sqr(kk));
-        float t1 = 1.0f + sqrtf(r), t2 = 1.0f - sqrtf(r), t3 = (1.0f - r) / (1.0f + r);
+        R e = eta[i], kk = k[i];
+        R r = (sqr(e - 1.0f) + sqr(kk)) / (sqr(e + 1.0f) + sqr(kk));
+        R t1 = 1.0f + sqrt_r(r), t2 = 1.0f - sqrt_r(r), t3 = (1.0f - r) / (1.0f + r);
         rr[i] = r;
         ee[i] = (t1 - e * t2) / (t1 - t3 * t2);
     }
-    v3 refl(rr[0], rr[1], rr[2]), edge(ee[0], ee[1], ee[2]);
-    return v3(0.087237f) + 0.0230685f * edge - 0.0864902f * edge * edge + 0.0774594f * edge * edge * edge +
+    vec3t<R> refl(rr[0], rr[1], rr[2]), edge(ee[0], ee[1], ee[2]);
+    return vec3t<R>(0.087237f) + 0.0230685f * edge - 0.0864902f * edge * edge + 0.0774594f * edge * edge * edge +
            0.782654f * refl - 0.136432f * refl * refl + 0.278708f * refl * refl * refl + 0.19744f * edge * refl +
            0.0360605f * edge * edge * refl - 0.2586f * edge * refl * refl;
 }
-RT_D float fresnel_dielectric(v3 V, v3 H, float eta_inv) {  // Microfacet.h:72-85
-    float ci = fabsf(dot(V, H));
-    float ct2 = 1.0f - sqr(eta_inv) * (1.0f - sqr(ci));
+template <class R>
+RT_D R fresnel_dielectric(vec3t<R> V, vec3t<R> H, sc_t<R> eta_inv) {  // Microfacet.h:72-85
+    R ci = fabs_r(dot(V, H));
+    R ct2 = 1.0f - sqr(eta_inv) * (1.0f - sqr(ci));
     if (ct2 <= 0.0f) return 1.0f;
-    float ct = sqrtf(ct2);
-    float rs = (eta_inv * ci - ct) / (eta_inv * ci + ct);
-    float rp = (ci - eta_inv * ct) / (ci + eta_inv * ct);
+    R ct = sqrt_r(ct2);
+    R rs = (eta_inv * ci - ct) / (eta_inv * ci + ct);
+    R rp = (ci - eta_inv * ct) / (ci + eta_inv * ct);
     return (rs * rs + rp * rp) / 2.0f;
 }
-RT_D float average_fresnel_dielectric(float eta) {  // Microfacet.h:87-113
+template <class R>
+RT_D R average_fresnel_dielectric(R eta) {  // Microfacet.h:87-113
     if (eta < 1.0f) return -1.4399f * (eta * eta) + 0.7099f * eta + 0.6681f + 0.0636f / eta;
-    float i1 = 1.0f / eta, i2 = i1 * i1, i3 = i2 * i1, i4 = i3 * i1, i5 = i4 * i1;
+    R i1 = 1.0f / eta, i2 = i1 * i1, i3 = i2 * i1, i4 = i3 * i1, i5 = i4 * i1;
     return 0.919317f - 3.4793f * i1 + 6.75335f * i2 - 7.80989f * i3 + 4.98554f * i4 - 1.36881f * i5;
 }
-RT_D float smith_g1(v3 V, v3 H, v3 N, float au, float av) {  // Microfacet.h:117-142
-    float cvn = dot(V, N);
+template <class R>
+RT_D R smith_g1(vec3t<R> V, vec3t<R> H, vec3t<R> N, sc_t<R> au, sc_t<R> av) {  // Microfacet.h:117-142
+    R cvn = dot(V, N);
     if (cvn * dot(V, H) <= 0.0f) return 0.0f;
-    if (fabsf(cvn - 1.0f) < kEps) return 1.0f;
+    if (fabs_r(cvn - 1.0f) < R(kEps)) return 1.0f;
     if (au == av) {
-        float c2 = sqr(cvn), t2 = (1.0f - c2) / c2;
-        return 2.0f / (1.0f + sqrtf(1.0f + au * au * t2));
+        R c2 = sqr(cvn), t2 = (1.0f - c2) / c2;
+        return 2.0f / (1.0f + sqrt_r(1.0f + au * au * t2));
     }
-    v3 d = to_local(V, N);
-    float t = (sqr(au * d.x) + sqr(av * d.y)) / sqr(d.z);
-    return 2.0f / (1.0f + sqrtf(1.0f + t));
+    vec3t<R> d = to_local(V, N);
+    R t = (sqr(au * d.x) + sqr(av * d.y)) / sqr(d.z);
+    return 2.0f / (1.0f + sqrt_r(1.0f + t));
 }
-RT_D float ggx_d(v3 H, v3 N, float au, float av) {  // Microfacet.h:144-160
-    float c = dot(H, N);
+template <class R>
+RT_D R ggx_d(vec3t<R> H, vec3t<R> N, sc_t<R> au, sc_t<R> av) {  // Microfacet.h:144-160
+    R c = dot(H, N);
     if (c <= 0.0f) return 0.0f;
-    float c2 = sqr(c), t2 = (1.0f - c2) / c2, a2 = au * av;
-    if (au == av) return a2 / (kPi * (c * c) * sqr(a2 + t2));
-    v3 d = to_local(H, N);
-    return 1.0f / (kPi * a2 * sqr(sqr(d.x / au) + sqr(d.y / av) + sqr(d.z)));
+    R c2 = sqr(c), t2 = (1.0f - c2) / c2, a2 = au * av;
+    if (au == av) return a2 / (Kc<R>::pi * (c * c) * sqr(a2 + t2));
+    vec3t<R> d = to_local(H, N);
+    return 1.0f / (Kc<R>::pi * a2 * sqr(sqr(d.x / au) + sqr(d.y / av) + sqr(d.z)));
 }
-RT_D float ggx_dv(v3 V, v3 H, v3 N, float au, float av) {  // Microfacet.h:162-164
+template <class R>
+RT_D R ggx_dv(vec3t<R> V, vec3t<R> H, vec3t<R> N, sc_t<R> au, sc_t<R> av) {  // Microfacet.h:162-164
     return smith_g1(V, H, N, au, av) * dot(V, H) * ggx_d(H, N, au, av) / dot(N, V);
 }
-RT_D v3 sample_vndf(v3 N, v3 Ve, float au, float av, float s0, float s1) {  // Microfacet.h:188-214
-    v3 V = to_local(Ve, N);
-    v3 Vh = normalize(v3(au * V.x, av * V.y, V.z));
-    float len2 = sqr(Vh.x) + sqr(Vh.y);
-    v3 T1 = len2 > 0.0f ? v3(-Vh.y, Vh.x, 0.0f) * sqrtf(1.0f / len2) : v3(1.0f, 0.0f, 0.0f);
-    v3 T2 = cross(Vh, T1);
-    float r = sqrtf(s0), phi = s1 * kTwoPi;
-    float sp, cp;
-    sincosf(phi, &sp, &cp);
-    float t1 = r * cp, t2 = r * sp;
-    float s = 0.5f * (1.0f + Vh.z);
-    t2 = (1.0f - s) * sqrtf(1.0f - sqr(t1)) + s * t2;
-    v3 Nh = t1 * T1 + t2 * T2 + sqrtf(fmaxf(0.0f, 1.0f - sqr(t1) - sqr(t2))) * Vh;
-    return normalize(v3(au * Nh.x, av * Nh.y, fmaxf(0.0f, Nh.z)));
+template <class R>
+RT_D vec3t<R> sample_vndf(vec3t<R> N, vec3t<R> Ve, sc_t<R> au, sc_t<R> av, sc_t<R> s0, sc_t<R> s1) {  // Microfacet.h:188-214
+    vec3t<R> V = to_local(Ve, N);
+    vec3t<R> Vh = normalize(vec3t<R>(au * V.x, av * V.y, V.z));
+    R len2 = sqr(Vh.x) + sqr(Vh.y);
+    vec3t<R> T1 = len2 > 0.0f ? vec3t<R>(-Vh.y, Vh.x, 0.0f) * sqrt_r(1.0f / len2) : vec3t<R>(1.0f, 0.0f, 0.0f);
+    vec3t<R> T2 = cross(Vh, T1);
+    R r = sqrt_r(s0), phi = s1 * Kc<R>::two_pi;
+    R sp, cp;
+    sincos_r(phi, &sp, &cp);
+    R t1 = r * cp, t2 = r * sp;
+    R s = 0.5f * (1.0f + Vh.z);
+    t2 = (1.0f - s) * sqrt_r(1.0f - sqr(t1)) + s * t2;
+    vec3t<R> Nh = t1 * T1 + t2 * T2 + sqrt_r(fmax_r(0.0f, 1.0f - sqr(t1) - sqr(t2))) * Vh;
+    return normalize(vec3t<R>(au * Nh.x, av * Nh.y, fmax_r(0.0f, Nh.z)));
 }
 // Kulla-Conty tables, Microfacet.h:293-346
-RT_D float lut_bsdf_avg(float cos_theta, float rough, const float* t) {
-    const int R = 64;
-    float o1 = sqr(rough) * R, o2 = cos_theta * R;
+template <class R>
+RT_D R lut_bsdf_avg(R cos_theta, R rough, const float* t) {
+    const int kN = 64;
+    R o1 = sqr(rough) * kN, o2 = cos_theta * kN;
     int i1 = int(o1), i2 = int(o2);
-    if (i1 >= R - 1) {
-        if (i2 >= R - 1) return __ldg(t + (R - 1) * R + R - 1);
-        return mixf(__ldg(t + (R - 1) * R + i2), __ldg(t + (R - 1) * R + i2 + 1), o2 - i2);
+    if (i1 >= kN - 1) {
+        if (i2 >= kN - 1) return __ldg(t + (kN - 1) * kN + kN - 1);
+        return mix_r<R>(__ldg(t + (kN - 1) * kN + i2), __ldg(t + (kN - 1) * kN + i2 + 1), o2 - i2);
     }
-    if (i2 >= R - 1) return mixf(__ldg(t + i1 * R + R - 1), __ldg(t + (i1 + 1) * R + R - 1), o1 - i1);
-    return mixf(mixf(__ldg(t + i1 * R + i2), __ldg(t + (i1 + 1) * R + i2), o1 - i1),
-                mixf(__ldg(t + i1 * R + i2 + 1), __ldg(t + (i1 + 1) * R + i2 + 1), o1 - i1), o2 - i2);
+    if (i2 >= kN - 1) return mix_r<R>(__ldg(t + i1 * kN + kN - 1), __ldg(t + (i1 + 1) * kN + kN - 1), o1 - i1);
+    return mix_r<R>(mix_r<R>(__ldg(t + i1 * kN + i2), __ldg(t + (i1 + 1) * kN + i2), o1 - i1),
+                mix_r<R>(__ldg(t + i1 * kN + i2 + 1), __ldg(t + (i1 + 1) * kN + i2 + 1), o1 - i1), o2 - i2);
 }
-RT_D float lut_albedo_avg(float rough, const float* t) {
-    float o = sqr(rough) * 64;
+template <class R>
+RT_D R lut_albedo_avg(R rough, const float* t) {
+    R o = sqr(rough) * 64;
     int i = int(o);
     if (i >= 63) return __ldg(t + 63);
-    return mixf(__ldg(t + i), __ldg(t + i + 1), o - i);
+    return mix_r<R>(__ldg(t + i), __ldg(t + i + 1), o - i);
 }
-RT_D v3 multiple_scatter(const SceneView& sc, float NdotL, float NdotV, float rough, v3 Favg) {
-    float bl = lut_bsdf_avg(NdotL, rough, sc.lut), bv = lut_bsdf_avg(NdotV, rough, sc.lut);
-    float ea = lut_albedo_avg(rough, sc.lut_avg);
-    float fms = (1.0f - bl) * (1.0f - bv) / (kPi * (1.0f - ea));
-    v3 fadd = Favg * Favg * ea / (1.0f - Favg * (1.0f - ea));
+template <class R>
+RT_D vec3t<R> multiple_scatter(const SceneView& sc, sc_t<R> NdotL, sc_t<R> NdotV, sc_t<R> rough, vec3t<R> Favg) {
+    R bl = lut_bsdf_avg(NdotL, rough, sc.lut), bv = lut_bsdf_avg(NdotV, rough, sc.lut);
+    R ea = lut_albedo_avg(rough, sc.lut_avg);
+    R fms = (1.0f - bl) * (1.0f - bv) / (Kc<R>::pi * (1.0f - ea));
+    vec3t<R> fadd = Favg * Favg * ea / (1.0f - Favg * (1.0f - ea));
     return fms * fadd;
 }
 
@@ -198,14 +216,15 @@ struct Surf {
     const DevMaterial* mat;   // nullptr: no material (evaluates to zero)
 };
 
-struct MatParams {
-    v3 albedo, eta, k, specular;
-    float rough, aniso, int_ior, ext_ior, metallic, coat_weight, cru, crv;
+template <class R>
+struct MatParamsT {
+    vec3t<R> albedo, eta, k, specular;
+    R rough, aniso, int_ior, ext_ior, metallic, coat_weight, cru, crv;
     bool nonlinear;
     int type;
 };
-RT_D MatParams load_material(const DevMaterial* m) {
-    MatParams p;
+RT_D MatParamsT<float> load_material(const DevMaterial* m) {
+    MatParamsT<float> p;
     // plain loads: `m` may be a path's textured copy written earlier in the same kernel
     const float4* q = reinterpret_cast<const float4*>(m);
     float4 w0 = q[0], w1 = q[1], w2 = q[2], w3 = q[3], w4 = q[4], w5 = q[5];
@@ -226,335 +245,383 @@ RT_D MatParams load_material(const DevMaterial* m) {
     return p;
 }
 
+// The material parameters in the sampler's precision.
+template <class R>
+RT_D MatParamsT<R> mat_cast(const MatParamsT<float>& a) {
+    MatParamsT<R> p;
+    p.albedo = vec3t<R>(a.albedo.x, a.albedo.y, a.albedo.z);
+    p.eta = vec3t<R>(a.eta.x, a.eta.y, a.eta.z);
+    p.k = vec3t<R>(a.k.x, a.k.y, a.k.z);
+    p.specular = vec3t<R>(a.specular.x, a.specular.y, a.specular.z);
+    p.rough = a.rough, p.aniso = a.aniso, p.int_ior = a.int_ior, p.ext_ior = a.ext_ior;
+    p.metallic = a.metallic, p.coat_weight = a.coat_weight, p.cru = a.cru, p.crv = a.crv;
+    p.nonlinear = a.nonlinear;
+    p.type = a.type;
+    return p;
+}
+template <class R>
+RT_D vec3t<R> cvt(v3 a) {
+    return vec3t<R>(a.x, a.y, a.z);
+}
+using MatParams = MatParamsT<float>;
+
 // Diffuse, Material.h:7-72
-RT_D v3 diffuse_f(const MatParams& m, v3 N, v3 V, v3 L, float NdotL, float& pdf) {
-    v3 H = normalize(V + L);
-    float NdotV = dot(N, V), VdotH = dot(V, H);
-    if (NdotL <= 0.0f || NdotV <= 0.0f) return v3(0.0f);
-    float a = m.rough * m.rough, s2 = a * a;
-    float VdotL = 2.0f * VdotH * VdotH - 1.0f;
-    float cosri = VdotL - NdotV * NdotL;
-    float C1 = 1.0f - 0.5f * s2 / (s2 + 0.33f);
-    float C2 = 0.45f * s2 / (s2 + 0.09f) * cosri * (cosri >= 0.0f ? fmaxf(NdotL, NdotV) : 1.0f);
+template <class R>
+RT_D vec3t<R> diffuse_f(const MatParamsT<R>& m, vec3t<R> N, vec3t<R> V, vec3t<R> L, sc_t<R> NdotL, R& pdf) {
+    vec3t<R> H = normalize(V + L);
+    R NdotV = dot(N, V), VdotH = dot(V, H);
+    if (NdotL <= 0.0f || NdotV <= 0.0f) return vec3t<R>(0.0f);
+    R a = m.rough * m.rough, s2 = a * a;
+    R VdotL = 2.0f * VdotH * VdotH - 1.0f;
+    R cosri = VdotL - NdotV * NdotL;
+    R C1 = 1.0f - 0.5f * s2 / (s2 + 0.33f);
+    R C2 = 0.45f * s2 / (s2 + 0.09f) * cosri * (cosri >= 0.0f ? fmax_r(NdotL, NdotV) : 1.0f);
     pdf = cosine_pdf(NdotL);
-    return m.albedo * kInvPi * (C1 + C2) * (1.0f + m.rough * 0.5f);
+    return m.albedo * Kc<R>::inv_pi * (C1 + C2) * (1.0f + m.rough * 0.5f);
 }
 // Conductor, Material.h:76-146
-RT_D v3 conductor_f(const SceneView& sc, const MatParams& m, v3 N, v3 V, v3 L, v3 H, float& pdf) {
-    float au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
-    v3 Favg = average_fresnel_conductor(m.eta, m.k);
-    float Dv = ggx_dv(V, H, N, au, av);
-    pdf = Dv * fabsf(1.0f / (4.0f * dot(V, H)));
-    float NdotV = dot(N, V), NdotL = dot(N, L);
-    if (NdotV <= 0.0f || NdotL <= 0.0f) return v3(0.0f);
-    v3 F = fresnel_conductor(V, H, m.eta, m.k);
-    float G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
-    float D = ggx_d(H, N, au, av);
+template <class R>
+RT_D vec3t<R> conductor_f(const SceneView& sc, const MatParamsT<R>& m, vec3t<R> N, vec3t<R> V, vec3t<R> L, vec3t<R> H, R& pdf) {
+    R au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
+    vec3t<R> Favg = average_fresnel_conductor(m.eta, m.k);
+    R Dv = ggx_dv(V, H, N, au, av);
+    pdf = Dv * fabs_r(1.0f / (4.0f * dot(V, H)));
+    R NdotV = dot(N, V), NdotL = dot(N, L);
+    if (NdotV <= 0.0f || NdotL <= 0.0f) return vec3t<R>(0.0f);
+    vec3t<R> F = fresnel_conductor(V, H, m.eta, m.k);
+    R G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
+    R D = ggx_d(H, N, au, av);
     return m.albedo * (F * D * G / (4.0f * NdotV * NdotL) + multiple_scatter(sc, NdotL, NdotV, m.rough, Favg));
 }
 // Dielectric, Material.h:150-269 (shared tail of evaluate and sample)
-RT_D v3 dielectric_f(const MatParams& m, v3 N, v3 V, v3 L, v3 H, float e, bool refl, float Dv, float F, float D,
-                     float au, float av, float& pdf) {
-    float NdotV = fabsf(dot(N, V)), NdotL = fabsf(dot(N, L));
-    float G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
+template <class R>
+RT_D vec3t<R> dielectric_f(const MatParamsT<R>& m, vec3t<R> N, vec3t<R> V, vec3t<R> L, vec3t<R> H, sc_t<R> e, bool refl, sc_t<R> Dv, sc_t<R> F, sc_t<R> D,
+                     sc_t<R> au, sc_t<R> av, R& pdf) {
+    R NdotV = fabs_r(dot(N, V)), NdotL = fabs_r(dot(N, L));
+    R G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
     if (refl) {
-        float dwh = fabsf(1.0f / (4.0f * dot(V, H)));
+        R dwh = fabs_r(1.0f / (4.0f * dot(V, H)));
         pdf = F * Dv * dwh;
         return m.albedo * F * D * G / (4.0f * NdotV * NdotL);
     }
-    float HdotV = dot(H, V), HdotL = dot(H, L);
-    float sd = e * HdotV + HdotL;
-    float factor = fabsf(HdotL * HdotV / (NdotL * NdotV));
-    float dwh = fabsf(HdotL) / sqr(sd);
+    R HdotV = dot(H, V), HdotL = dot(H, L);
+    R sd = e * HdotV + HdotL;
+    R factor = fabs_r(HdotL * HdotV / (NdotL * NdotV));
+    R dwh = fabs_r(HdotL) / sqr(sd);
     pdf = (1.0f - F) * Dv * dwh;
-    v3 f = m.albedo * (1.0f - F) * D * G * factor / sqr(sd);
+    vec3t<R> f = m.albedo * (1.0f - F) * D * G * factor / sqr(sd);
     f *= sqr(1.0f / e);
     return f;
 }
 // Plastic, Material.h:273-403 (shared tail)
-RT_D v3 plastic_f(const SceneView& sc, const MatParams& m, v3 N, v3 V, v3 L, v3 H, float Fo, float Fi, float ps,
-                  float& pdf) {
-    float au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
-    float eta = m.int_ior / m.ext_ior;
-    float Favg = average_fresnel_dielectric(eta);
-    float NdotV = dot(N, V), NdotL = dot(N, L);
-    float Dv = ggx_dv(V, H, N, au, av);
-    float G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
-    float D = ggx_d(H, N, au, av);
-    float F = fresnel_dielectric(L, H, 1.0f / eta);
-    v3 f = m.nonlinear ? m.albedo / (1.0f - m.albedo * Favg) : m.albedo / (1.0f - Favg);
-    f *= (1.0f - Fi) * (1.0f - Fo) * kInvPi;
-    f += m.specular * (v3(F) * D * G / (4.0f * NdotL * NdotV) + multiple_scatter(sc, NdotL, NdotV, m.rough, v3(Favg)));
-    pdf = ps * Dv * fabsf(1.0f / (4.0f * dot(V, H))) + (1.0f - ps) * cosine_pdf(NdotL);
+template <class R>
+RT_D vec3t<R> plastic_f(const SceneView& sc, const MatParamsT<R>& m, vec3t<R> N, vec3t<R> V, vec3t<R> L, vec3t<R> H, sc_t<R> Fo, sc_t<R> Fi, sc_t<R> ps,
+                  R& pdf) {
+    R au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
+    R eta = m.int_ior / m.ext_ior;
+    R Favg = average_fresnel_dielectric(eta);
+    R NdotV = dot(N, V), NdotL = dot(N, L);
+    R Dv = ggx_dv(V, H, N, au, av);
+    R G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
+    R D = ggx_d(H, N, au, av);
+    R F = fresnel_dielectric(L, H, 1.0f / eta);
+    vec3t<R> f = m.nonlinear ? m.albedo / (1.0f - m.albedo * Favg) : m.albedo / (1.0f - Favg);
+    f *= (1.0f - Fi) * (1.0f - Fo) * Kc<R>::inv_pi;
+    f += m.specular * (vec3t<R>(F) * D * G / (4.0f * NdotL * NdotV) + multiple_scatter(sc, NdotL, NdotV, m.rough, vec3t<R>(Favg)));
+    pdf = ps * Dv * fabs_r(1.0f / (4.0f * dot(V, H))) + (1.0f - ps) * cosine_pdf(NdotL);
     return f;
 }
-RT_D float plastic_weight(const MatParams& m) {
-    float d = m.albedo.x + m.albedo.y + m.albedo.z, s = m.specular.x + m.specular.y + m.specular.z;
+template <class R>
+RT_D R plastic_weight(const MatParamsT<R>& m) {
+    R d = m.albedo.x + m.albedo.y + m.albedo.z, s = m.specular.x + m.specular.y + m.specular.z;
     return s / (s + d);
 }
 // Metal workflow, Material.h:407-516 (shared tail)
-RT_D v3 metal_f(const MatParams& m, v3 N, v3 V, v3 L, v3 H, float& pdf) {
-    float au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
-    float NdotV = dot(N, V), NdotL = dot(N, L);
-    float diel = 1.0f - m.metallic, spec = m.metallic + diel, pdiff = diel / (diel + spec);
-    float Dv = ggx_dv(V, H, N, au, av);
-    float G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
-    float D = ggx_d(H, N, au, av);
-    v3 F0 = v3(0.04f) * (1.0f - m.metallic) + m.albedo * m.metallic;
-    float vdh = dot(V, H);
-    float tmp = 1.0f - fminf(1.0f, fmaxf(0.0f, vdh));
-    float tmp2 = tmp * tmp, Fc = tmp2 * tmp2 * tmp;
-    v3 F = F0 + (1.0f - F0) * Fc;
-    v3 sb = D * F * G / (4.0f * NdotL * NdotV);
-    v3 db = m.albedo * kInvPi;
-    pdf = (1.0f - pdiff) * Dv * fabsf(1.0f / (4.0f * vdh)) + pdiff * cosine_pdf(NdotL);
+template <class R>
+RT_D vec3t<R> metal_f(const MatParamsT<R>& m, vec3t<R> N, vec3t<R> V, vec3t<R> L, vec3t<R> H, R& pdf) {
+    R au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
+    R NdotV = dot(N, V), NdotL = dot(N, L);
+    R diel = 1.0f - m.metallic, spec = m.metallic + diel, pdiff = diel / (diel + spec);
+    R Dv = ggx_dv(V, H, N, au, av);
+    R G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
+    R D = ggx_d(H, N, au, av);
+    vec3t<R> F0 = vec3t<R>(0.04f) * (1.0f - m.metallic) + m.albedo * m.metallic;
+    R vdh = dot(V, H);
+    R tmp = 1.0f - fmin_r(1.0f, fmax_r(0.0f, vdh));
+    R tmp2 = tmp * tmp, Fc = tmp2 * tmp2 * tmp;
+    vec3t<R> F = F0 + (1.0f - F0) * Fc;
+    vec3t<R> sb = D * F * G / (4.0f * NdotL * NdotV);
+    vec3t<R> db = m.albedo * Kc<R>::inv_pi;
+    pdf = (1.0f - pdiff) * Dv * fabs_r(1.0f / (4.0f * vdh)) + pdiff * cosine_pdf(NdotL);
     return pdiff * db + (1.0f - pdiff) * sb;
 }
-RT_D float thin_fresnel(v3 V, v3 H, float eta) {  // Material.h:548-551
-    float F = fresnel_dielectric(V, H, 1.0f / eta);
+template <class R>
+RT_D R thin_fresnel(vec3t<R> V, vec3t<R> H, sc_t<R> eta) {  // Material.h:548-551
+    R F = fresnel_dielectric(V, H, 1.0f / eta);
     if (F < 1.0f) F *= 2.0f / (1.0f + F);
     return F;
 }
 // Clear-coated conductor coat term, Material.h:634-734
-RT_D v3 clearcoat_mix(const SceneView& sc, const MatParams& m, v3 N, v3 V, v3 L, v3 H, v3 cond, float cpdf,
-                      float& pdf) {
-    float au = sqr(m.cru), av = sqr(m.crv);
-    float NdotV = dot(N, V), NdotL = dot(N, L);
-    float Dv = ggx_dv(V, H, N, au, av);
-    float F = fresnel_dielectric(V, H, 1.0f / 1.5f);
-    float cw = m.coat_weight * F;
-    float G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
-    float D = ggx_d(H, N, au, av);
-    float coat_pdf = Dv * fabsf(1.0f / (4.0f * dot(V, H)));
-    v3 coat(D * G / (4.0f * NdotV * NdotL));
+template <class R>
+RT_D vec3t<R> clearcoat_mix(const SceneView& sc, const MatParamsT<R>& m, vec3t<R> N, vec3t<R> V, vec3t<R> L, vec3t<R> H, vec3t<R> cond, sc_t<R> cpdf,
+                      R& pdf) {
+    R au = sqr(m.cru), av = sqr(m.crv);
+    R NdotV = dot(N, V), NdotL = dot(N, L);
+    R Dv = ggx_dv(V, H, N, au, av);
+    R F = fresnel_dielectric(V, H, 1.0f / 1.5f);
+    R cw = m.coat_weight * F;
+    R G = smith_g1(V, H, N, au, av) * smith_g1(L, H, N, au, av);
+    R D = ggx_d(H, N, au, av);
+    R coat_pdf = Dv * fabs_r(1.0f / (4.0f * dot(V, H)));
+    vec3t<R> coat(D * G / (4.0f * NdotV * NdotL));
     pdf = cw * coat_pdf + (1.0f - cw) * cpdf;
     return cw * coat + (1.0f - cw) * cond;
 }
 
 // EvaluateMaterial, Material.h:783-813
-RT_D v3 eval_material(const SceneView& sc, const Surf& s, v3 V, v3 L, float& pdf) {
+template <class R>
+RT_D vec3t<R> eval_material(const SceneView& sc, const Surf& s, vec3t<R> V, vec3t<R> L, R& pdf) {
     pdf = 0.0f;
-    if (!s.mat) return v3(0.0f);
-    const MatParams m = load_material(s.mat);
-    const v3 N = s.sn;
+    if (!s.mat) return vec3t<R>(0.0f);
+    const MatParamsT<R> m = mat_cast<R>(load_material(s.mat));
+    const vec3t<R> N = cvt<R>(s.sn);
     switch (m.type) {
         case RT_MAT_DIFFUSE: {
-            v3 lL = to_local(L, N);
+            vec3t<R> lL = to_local(L, N);
             return diffuse_f(m, N, V, L, lL.z, pdf);
         }
         case RT_MAT_CONDUCTOR: return conductor_f(sc, m, N, V, L, normalize(V + L), pdf);
         case RT_MAT_DIELECTRIC: {
-            float au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
-            float eta = m.int_ior / m.ext_ior;
-            float e = s.front ? (1.0f / eta) : eta;
+            R au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
+            R eta = m.int_ior / m.ext_ior;
+            R e = s.front ? (1.0f / eta) : eta;
             bool refl = dot(N, L) * dot(N, V) > 0.0f;
-            v3 H;
+            vec3t<R> H;
             if (refl) {
                 H = normalize(V + L);
             } else {
                 H = -normalize(e * V + L);
                 if (dot(N, H) < 0.0f) H = -H;
             }
-            float Dv = ggx_dv(V, H, N, au, av);
-            pdf = Dv * fabsf(1.0f / (4.0f * dot(V, H)));
-            float F = fresnel_dielectric(V, H, e);
-            float D = ggx_d(H, N, au, av);
+            R Dv = ggx_dv(V, H, N, au, av);
+            pdf = Dv * fabs_r(1.0f / (4.0f * dot(V, H)));
+            R F = fresnel_dielectric(V, H, e);
+            R D = ggx_d(H, N, au, av);
             return dielectric_f(m, N, V, L, H, e, refl, Dv, F, D, au, av, pdf);
         }
         case RT_MAT_PLASTIC: {
-            float eta = m.int_ior / m.ext_ior;
-            v3 H = normalize(V + L);
-            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return v3(0.0f);
-            float Fo = fresnel_dielectric(V, N, 1.0f / eta), Fi = fresnel_dielectric(L, N, 1.0f / eta);
-            float w = plastic_weight(m);
-            float ps = Fi * w, pd = (1.0f - Fi) * (1.0f - w);
+            R eta = m.int_ior / m.ext_ior;
+            vec3t<R> H = normalize(V + L);
+            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
+            R Fo = fresnel_dielectric(V, N, 1.0f / eta), Fi = fresnel_dielectric(L, N, 1.0f / eta);
+            R w = plastic_weight(m);
+            R ps = Fi * w, pd = (1.0f - Fi) * (1.0f - w);
             ps = ps / (ps + pd);
             return plastic_f(sc, m, N, V, L, H, Fo, Fi, ps, pdf);
         }
         case RT_MAT_METAL_WORKFLOW: {
-            v3 H = normalize(L + V);
-            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return v3(0.0f);
+            vec3t<R> H = normalize(L + V);
+            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
             return metal_f(m, N, V, L, H, pdf);
         }
         case RT_MAT_THIN_DIELECTRIC: {
-            float eta = m.int_ior / m.ext_ior, a = sqr(m.rough);
+            R eta = m.int_ior / m.ext_ior, a = sqr(m.rough);
             bool refl = dot(N, L) * dot(N, V) > 0.0f;
-            v3 H;
+            vec3t<R> H;
             if (refl) {
                 H = normalize(V + L);
             } else {
-                v3 Vr = to_world(to_local(V, -N), N);
+                vec3t<R> Vr = to_world(to_local(V, -N), N);
                 H = normalize(Vr + L);
                 if (dot(N, H) < 0.0f) H = -H;
             }
-            float Dv = ggx_dv(V, H, N, a, a);
-            float F = thin_fresnel(V, H, eta);
-            float D = ggx_d(H, N, a, a);
-            float dwh = fabsf(1.0f / (4.0f * dot(V, H)));
-            float NdotV = fabsf(dot(N, V)), NdotL = fabsf(dot(N, L));
-            float G = smith_g1(V, H, N, a, a) * smith_g1(L, H, N, a, a);
+            R Dv = ggx_dv(V, H, N, a, a);
+            R F = thin_fresnel(V, H, eta);
+            R D = ggx_d(H, N, a, a);
+            R dwh = fabs_r(1.0f / (4.0f * dot(V, H)));
+            R NdotV = fabs_r(dot(N, V)), NdotL = fabs_r(dot(N, L));
+            R G = smith_g1(V, H, N, a, a) * smith_g1(L, H, N, a, a);
             if (refl) {
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
                 pdf = F * Dv * dwh;
                 return m.albedo * F * D * G / (4.0f * NdotV * NdotL);
             }
-            if (dot(N, L) * dot(N, V) >= 0.0f) return v3(0.0f);
+            if (dot(N, L) * dot(N, V) >= 0.0f) return vec3t<R>(0.0f);
             pdf = (1.0f - F) * Dv * dwh;
             return m.albedo * (1.0f - F) * D * G / (4.0f * NdotV * NdotL);
         }
         case RT_MAT_CLEARCOATED_CONDUCTOR: {
-            v3 H = normalize(V + L);
-            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return v3(0.0f);
-            float cpdf = 0.0f;
-            v3 cond = conductor_f(sc, m, N, V, L, H, cpdf);
+            vec3t<R> H = normalize(V + L);
+            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
+            R cpdf = 0.0f;
+            vec3t<R> cond = conductor_f(sc, m, N, V, L, H, cpdf);
             return clearcoat_mix(sc, m, N, V, L, H, cond, cpdf, pdf);
         }
         case RT_MAT_DIFFUSE_TRANSMITTER: {
-            v3 Nn = -N;
-            v3 lL = to_local(L, Nn);
-            float NdotL = lL.z, NdotV = dot(Nn, V);
-            if (NdotL * NdotV >= 0.0f) return v3(0.0f);
-            pdf = cosine_pdf(fabsf(NdotL));
-            return m.albedo * kInvPi;
+            vec3t<R> Nn = -N;
+            vec3t<R> lL = to_local(L, Nn);
+            R NdotL = lL.z, NdotV = dot(Nn, V);
+            if (NdotL * NdotV >= 0.0f) return vec3t<R>(0.0f);
+            pdf = cosine_pdf(fabs_r(NdotL));
+            return m.albedo * Kc<R>::inv_pi;
         }
     }
-    return v3(0.0f);
+    return vec3t<R>(0.0f);
 }
 
 // SampleMaterial, Material.h:815-845
-template <class RNG>
-RT_D v3 sample_material(const SceneView& sc, const Surf& s, RNG& rng, v3 V, v3& L, float& pdf) {
+template <class R, class RNG>
+RT_D vec3t<R> sample_material_t(const SceneView& sc, const Surf& s, RNG& rng, vec3t<R> V, vec3t<R>& L, R& pdf) {
     pdf = 0.0f;
-    if (!s.mat) return v3(0.0f);
-    const MatParams m = load_material(s.mat);
-    const v3 N = s.sn;
-    float au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
+    if (!s.mat) return vec3t<R>(0.0f);
+    const MatParamsT<R> m = mat_cast<R>(load_material(s.mat));
+    const vec3t<R> N = cvt<R>(s.sn);
+    R au = sqr(m.rough) * (1.0f + m.aniso), av = sqr(m.rough) * (1.0f - m.aniso);
     switch (m.type) {
         case RT_MAT_DIFFUSE: {
-            float u0 = rng.next(), u1 = rng.next();
-            v3 lL = cosine_sample_hemisphere(u0, u1);
+            R u0 = rng.next(), u1 = rng.next();
+            vec3t<R> lL = cosine_sample_hemisphere(u0, u1);
             L = to_world(lL, N);
             return diffuse_f(m, N, V, L, lL.z, pdf);
         }
         case RT_MAT_CONDUCTOR: {
-            float u0 = rng.next(), u1 = rng.next();
-            v3 H = to_world(sample_vndf(N, V, au, av, u0, u1), N);
+            R u0 = rng.next(), u1 = rng.next();
+            vec3t<R> H = to_world(sample_vndf(N, V, au, av, u0, u1), N);
             L = reflect(-V, H);
             return conductor_f(sc, m, N, V, L, H, pdf);
         }
         case RT_MAT_DIELECTRIC: {
-            float eta = m.int_ior / m.ext_ior;
-            float e = s.front ? (1.0f / eta) : eta;
-            float u0 = rng.next(), u1 = rng.next();
-            v3 H = to_world(sample_vndf(N, V, au, av, u0, u1), N);
-            float Dv = ggx_dv(V, H, N, au, av);
-            float F = fresnel_dielectric(V, H, e);
-            float D = ggx_d(H, N, au, av);
+            R eta = m.int_ior / m.ext_ior;
+            R e = s.front ? (1.0f / eta) : eta;
+            R u0 = rng.next(), u1 = rng.next();
+            vec3t<R> H = to_world(sample_vndf(N, V, au, av, u0, u1), N);
+            R Dv = ggx_dv(V, H, N, au, av);
+            R F = fresnel_dielectric(V, H, e);
+            R D = ggx_d(H, N, au, av);
             if (rng.next() < F) {
                 L = reflect(-V, H);
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
                 return dielectric_f(m, N, V, L, H, e, true, Dv, F, D, au, av, pdf);
             }
             L = refract(-V, H, e);
-            if (dot(N, L) * dot(N, V) >= 0.0f) return v3(0.0f);
+            if (dot(N, L) * dot(N, V) >= 0.0f) return vec3t<R>(0.0f);
             return dielectric_f(m, N, V, L, H, e, false, Dv, F, D, au, av, pdf);
         }
         case RT_MAT_PLASTIC: {
-            float eta = m.int_ior / m.ext_ior;
-            if (dot(N, V) <= 0.0f) return v3(0.0f);
-            float Fo = fresnel_dielectric(V, N, 1.0f / eta), Fi = Fo;
-            float w = plastic_weight(m);
-            float ps = Fi * w, pd = (1.0f - Fi) * (1.0f - w);
+            R eta = m.int_ior / m.ext_ior;
+            if (dot(N, V) <= 0.0f) return vec3t<R>(0.0f);
+            R Fo = fresnel_dielectric(V, N, 1.0f / eta), Fi = Fo;
+            R w = plastic_weight(m);
+            R ps = Fi * w, pd = (1.0f - Fi) * (1.0f - w);
             ps = ps / (ps + pd);
-            v3 H;
+            vec3t<R> H;
             if (rng.next() < ps) {
-                float u0 = rng.next(), u1 = rng.next();
+                R u0 = rng.next(), u1 = rng.next();
                 H = to_world(sample_vndf(N, V, au, av, u0, u1), N);
                 L = reflect(-V, H);
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
             } else {
-                float u0 = rng.next(), u1 = rng.next();
+                R u0 = rng.next(), u1 = rng.next();
                 L = to_world(cosine_sample_hemisphere(u0, u1), N);
                 H = normalize(V + L);
                 Fi = fresnel_dielectric(L, N, 1.0f / eta);
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
             }
             return plastic_f(sc, m, N, V, L, H, Fo, Fi, ps, pdf);
         }
         case RT_MAT_METAL_WORKFLOW: {
-            if (dot(N, V) <= 0.0f) return v3(0.0f);
-            float diel = 1.0f - m.metallic, spec = m.metallic + diel, pdiff = diel / (diel + spec);
-            v3 H;
+            if (dot(N, V) <= 0.0f) return vec3t<R>(0.0f);
+            R diel = 1.0f - m.metallic, spec = m.metallic + diel, pdiff = diel / (diel + spec);
+            vec3t<R> H;
             if (rng.next() < pdiff) {
-                float u0 = rng.next(), u1 = rng.next();
+                R u0 = rng.next(), u1 = rng.next();
                 L = to_world(cosine_sample_hemisphere(u0, u1), N);
                 H = normalize(V + L);
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
             } else {
-                float u0 = rng.next(), u1 = rng.next();
+                R u0 = rng.next(), u1 = rng.next();
                 H = to_world(sample_vndf(N, V, au, av, u0, u1), N);
                 L = reflect(-V, H);
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
             }
             return metal_f(m, N, V, L, H, pdf);
         }
         case RT_MAT_THIN_DIELECTRIC: {
-            float eta = m.int_ior / m.ext_ior, a = sqr(m.rough);
-            float u0 = rng.next(), u1 = rng.next();
-            v3 H = to_world(sample_vndf(N, V, a, a, u0, u1), N);
-            float Dv = ggx_dv(V, H, N, a, a);
-            float F = thin_fresnel(V, H, eta);
-            float D = ggx_d(H, N, a, a);
-            float dwh = fabsf(1.0f / (4.0f * dot(V, H)));
+            R eta = m.int_ior / m.ext_ior, a = sqr(m.rough);
+            R u0 = rng.next(), u1 = rng.next();
+            vec3t<R> H = to_world(sample_vndf(N, V, a, a, u0, u1), N);
+            R Dv = ggx_dv(V, H, N, a, a);
+            R F = thin_fresnel(V, H, eta);
+            R D = ggx_d(H, N, a, a);
+            R dwh = fabs_r(1.0f / (4.0f * dot(V, H)));
             if (rng.next() < F) {
                 L = reflect(-V, H);
-                if (dot(N, L) <= 0.0f) return v3(0.0f);
-                float NdotV = fabsf(dot(N, V)), NdotL = fabsf(dot(N, L));
-                float G = smith_g1(V, H, N, a, a) * smith_g1(L, H, N, a, a);
+                if (dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
+                R NdotV = fabs_r(dot(N, V)), NdotL = fabs_r(dot(N, L));
+                R G = smith_g1(V, H, N, a, a) * smith_g1(L, H, N, a, a);
                 pdf = F * Dv * dwh;
                 return m.albedo * F * D * G / (4.0f * NdotV * NdotL);
             }
             L = -V;
-            if (dot(N, L) * dot(N, V) >= 0.0f) return v3(0.0f);
-            float NdotV = fabsf(dot(N, V)), NdotL = fabsf(dot(N, L));
-            float G = smith_g1(V, H, N, a, a) * smith_g1(L, H, N, a, a);
+            if (dot(N, L) * dot(N, V) >= 0.0f) return vec3t<R>(0.0f);
+            R NdotV = fabs_r(dot(N, V)), NdotL = fabs_r(dot(N, L));
+            R G = smith_g1(V, H, N, a, a) * smith_g1(L, H, N, a, a);
             pdf = (1.0f - F) * Dv * dwh;
             return m.albedo * (1.0f - F) * D * G / (4.0f * NdotV * NdotL);
         }
         case RT_MAT_CLEARCOATED_CONDUCTOR: {
-            float cau = sqr(m.cru), cav = sqr(m.crv);
-            float F = fresnel_dielectric(V, N, 1.0f / 1.5f);
-            float cw = m.coat_weight * F;
+            R cau = sqr(m.cru), cav = sqr(m.crv);
+            R F = fresnel_dielectric(V, N, 1.0f / 1.5f);
+            R cw = m.coat_weight * F;
             if (rng.next() < cw) {
-                float u0 = rng.next(), u1 = rng.next();
-                v3 H = to_world(sample_vndf(N, V, cau, cav, u0, u1), N);
+                R u0 = rng.next(), u1 = rng.next();
+                vec3t<R> H = to_world(sample_vndf(N, V, cau, cav, u0, u1), N);
                 L = reflect(-V, H);
-                if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return v3(0.0f);
-                float cpdf = 0.0f;
-                v3 cond = conductor_f(sc, m, N, V, L, normalize(V + L), cpdf);
+                if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
+                R cpdf = 0.0f;
+                vec3t<R> cond = conductor_f(sc, m, N, V, L, normalize(V + L), cpdf);
                 return clearcoat_mix(sc, m, N, V, L, H, cond, cpdf, pdf);
             }
-            float u0 = rng.next(), u1 = rng.next();
-            v3 Hc = to_world(sample_vndf(N, V, au, av, u0, u1), N);
+            R u0 = rng.next(), u1 = rng.next();
+            vec3t<R> Hc = to_world(sample_vndf(N, V, au, av, u0, u1), N);
             L = reflect(-V, Hc);
-            float cpdf = 0.0f;
-            v3 cond = conductor_f(sc, m, N, V, L, Hc, cpdf);
-            v3 H = normalize(V + L);
-            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return v3(0.0f);
+            R cpdf = 0.0f;
+            vec3t<R> cond = conductor_f(sc, m, N, V, L, Hc, cpdf);
+            vec3t<R> H = normalize(V + L);
+            if (dot(N, V) <= 0.0f || dot(N, L) <= 0.0f) return vec3t<R>(0.0f);
             return clearcoat_mix(sc, m, N, V, L, H, cond, cpdf, pdf);
         }
         case RT_MAT_DIFFUSE_TRANSMITTER: {
-            float u0 = rng.next(), u1 = rng.next();
-            v3 lL = cosine_sample_hemisphere(u0, u1);
-            v3 Nn = -N;
+            R u0 = rng.next(), u1 = rng.next();
+            vec3t<R> lL = cosine_sample_hemisphere(u0, u1);
+            vec3t<R> Nn = -N;
             L = to_world(lL, Nn);
-            float NdotL = lL.z, NdotV = dot(Nn, V);
-            if (NdotL * NdotV >= 0.0f) return v3(0.0f);
-            pdf = cosine_pdf(fabsf(NdotL));
-            return m.albedo * kInvPi;
+            R NdotL = lL.z, NdotV = dot(Nn, V);
+            if (NdotL * NdotV >= 0.0f) return vec3t<R>(0.0f);
+            pdf = cosine_pdf(fabs_r(NdotL));
+            return m.albedo * Kc<R>::inv_pi;
         }
     }
-    return v3(0.0f);
+    return vec3t<R>(0.0f);
+}
+
+
+// SampleMaterial in double precision: the sampled direction and the f and
+// pdf reported for it come from the double instantiation of the material
+// code above, fed the FP32 inputs and the FP32 random numbers, and are
+// rounded once at the end.  The visible-normal map and the f / pdf chains
+// amplify FP32 rounding well past 1e-5 relative (by 1 / alpha^2 in the
+// (1 - cos^2) / cos^2 of a sharp GGX lobe, and near the rim of the
+// projected disk), which double arithmetic keeps at the output rounding.
+// Random numbers are consumed as by the FP32 code.
+template <class RNG>
+RT_D v3 sample_material(const SceneView& sc, const Surf& s, RNG& rng, v3 V, v3& L, float& pdf) {
+    v3d Ld = to_d(L);
+    double pd = 0.0;
+    const v3d f = sample_material_t<double>(sc, s, rng, to_d(V), Ld, pd);
+    L = to_f(Ld);
+    pdf = float(pd);
+    return to_f(f);
 }
 
 // The isotropic GGX distribution with the cos^4 of its definition (the

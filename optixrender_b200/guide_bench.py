@@ -42,11 +42,13 @@ def reference(spec, spp, frame_spp=256, seed=1000):
     return acc / frames, frames * min(frame_spp, spp), ms
 
 
-def curve(spec, ref, guided, step, max_spp, seed, train_spp):
+def curve(spec, ref, guided, step, max_spp, seed, train_spp, guide_prob=0.5, max_resolution=0, max_log_kappa=0.0):
     over = dict(spp=step, progressive=1, seed=seed)
     if guided:
-        over.update(guided=1, guide_train_spp=train_spp)
+        over.update(guided=1, guide_train_spp=train_spp, guide_prob=guide_prob)
     s, r = scenes.build_renderer(spec, **over)
+    if guided and (max_resolution or max_log_kappa):
+        r.guide().set_hyperparameters(max_resolution=max_resolution, max_log_kappa=max_log_kappa)
     pts = []
     ms = 0.0
     spp = 0
@@ -84,17 +86,42 @@ def main(argv=None):
     ap.add_argument("--step", type=int, default=16)
     ap.add_argument("--train-spp", type=int, default=32)
     ap.add_argument("--target", type=float, default=1e-3)
+    ap.add_argument("--guide-prob", type=float, default=0.5, help="mixture selection probability")
+    ap.add_argument("--max-resolution", type=int, default=0, help="finest hash-grid level (0: the network's default)")
+    ap.add_argument("--max-log-kappa", type=float, default=0.0, help="sharpest lobe (0: the network's default)")
+    ap.add_argument("--ablations", default="",
+                    help="extra guided runs sharing the reference, ';'-separated, each 'key=value,...' over "
+                         "guide_prob, max_resolution, max_log_kappa, train_spp")
     a = ap.parse_args(argv)
     spec = scenes.SCENES[a.scene](a.width, a.height, 1)
     ref, ref_spp, ref_ms = reference(spec, a.ref_spp)
     plain = curve(spec, ref, False, a.step, a.max_spp, 7, a.train_spp)
-    guided = curve(spec, ref, True, a.step, a.max_spp, 8, a.train_spp)
-    tp, tg = time_to(plain, a.target), time_to(guided, a.target)
+    base = dict(guide_prob=a.guide_prob, max_resolution=a.max_resolution, max_log_kappa=a.max_log_kappa,
+                train_spp=a.train_spp)
+
+    def guided_run(cfg):
+        pts = curve(spec, ref, True, a.step, a.max_spp, 8, cfg["train_spp"], cfg["guide_prob"],
+                    cfg["max_resolution"], cfg["max_log_kappa"])
+        tg = time_to(pts, a.target)
+        return pts, tg
+
+    guided, tg = guided_run(base)
+    tp = time_to(plain, a.target)
     line = {"metric": f"time-to-relMSE {a.target:g}", "unit": "ms", "higher_is_better": False,
             "plain_ms": tp, "guided_ms": tg, "speedup": (tp / tg) if (tp and tg) else None,
             "scene": a.scene, "width": a.width, "height": a.height, "reference_spp": ref_spp,
-            "reference_ms": ref_ms, "train_spp": a.train_spp, "step_spp": a.step,
+            "reference_ms": ref_ms, "train_spp": a.train_spp, "step_spp": a.step, "guide": base,
             "plain": plain, "guided": guided, "data": "synthetic"}
+    abl = []
+    for spec_txt in [x for x in a.ablations.split(";") if x.strip()]:
+        cfg = dict(base)
+        for kv in spec_txt.split(","):
+            k, v = kv.split("=")
+            cfg[k.strip()] = type(base[k.strip()])(float(v)) if k.strip() != "train_spp" else int(float(v))
+        pts, t = guided_run(cfg)
+        abl.append({"guide": cfg, "guided_ms": t, "speedup": (tp / t) if (tp and t) else None, "guided": pts})
+    if abl:
+        line["ablations"] = abl
     print(json.dumps(line))
     return line
 

@@ -371,7 +371,7 @@ void trace_sample(const Scene<R>& sc, const float* tv, const float* tn, const Ca
                 }
             }
             // BSDF sampling, devicePrograms.cu:474-477
-            bsdf = sample_material(it, lut, rng, V, L, bsdf_pdf);
+            bsdf = sample_material_device(it, lut, rng, V, L, bsdf_pdf);
             R ct = std::fabs(dot(it.sn, L));
             history *= (bsdf * ct / bsdf_pdf);
             pre_pdf = bsdf_pdf;

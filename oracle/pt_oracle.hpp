@@ -881,6 +881,49 @@ template <class R> inline V3<R> sample_material(const Isect<R>& it, const Lut<R>
     return V3<R>(R(0));
 }
 
+// The renderer's BSDF sampler: SampleMaterial evaluated in double precision on
+// the FP32 inputs and random numbers, rounded once (optixrender_b200's
+// sample_material).  The FP32 render oracle samples with it so that the same
+// random streams trace the same paths; the FP32 shading ops keep the
+// reference's own FP32 sampler (the golden-vector pins).
+inline V3<double> sample_material_device(const Isect<double>& it, const Lut<double>& lut, Rng& rng,
+                                         const V3<double>& V, V3<double>& L, double& pdf) {
+    return sample_material(it, lut, rng, V, L, pdf);
+}
+inline V3<float> sample_material_device(const Isect<float>& it, const Lut<float>& lut, Rng& rng, const V3<float>& V,
+                                        V3<float>& L, float& pdf) {
+    auto d3 = [](const V3<float>& v) { return V3<double>(double(v.x), double(v.y), double(v.z)); };
+    Mat<double> md;
+    if (it.mat) {
+        const Mat<float>& m = *it.mat;
+        md.type = m.type;
+        md.albedo = d3(m.albedo);
+        md.eta = d3(m.eta);
+        md.k = d3(m.k);
+        md.specular = d3(m.specular);
+        md.roughness = m.roughness, md.anisotropy = m.anisotropy, md.int_ior = m.int_ior, md.ext_ior = m.ext_ior;
+        md.metallic = m.metallic, md.coat_weight = m.coat_weight, md.cru = m.cru, md.crv = m.crv;
+        md.nonlinear = m.nonlinear;
+        for (int t = 0; t < 8; t++) md.tex[t] = m.tex[t];
+        md.textured = m.textured;
+    }
+    Isect<double> id;
+    id.distance = it.distance;
+    id.position = d3(it.position);
+    id.sn = d3(it.sn);
+    id.front = it.front;
+    id.mat = it.mat ? &md : nullptr;
+    id.in_medium = it.in_medium;
+    id.out_medium = it.out_medium;
+    const Lut<double> ld{lut.bsdf, lut.avg};
+    V3<double> Ld = d3(L);
+    double pd = 0.0;
+    const V3<double> f = sample_material(id, ld, rng, d3(V), Ld, pd);
+    L = V3<float>(float(Ld.x), float(Ld.y), float(Ld.z));
+    pdf = float(pd);
+    return V3<float>(float(f.x), float(f.y), float(f.z));
+}
+
 // ---------------------------------------------------------------- lights
 template <class R> struct Lt {
     int type;

@@ -106,6 +106,8 @@ class StructDefaults:
             d = np.ascontiguousarray(density, dtype=np.float32)
             m._density_keepalive = d
             m.density = d.ctypes.data_as(C.POINTER(C.c_float))
+            if type == self.rt.MEDIUM_GRID and "grid_res" not in kw:  # x fastest: (z, y, x) array
+                m.grid_res = (C.c_int32 * 3)(d.shape[2], d.shape[1], d.shape[0])
         return m
 
 

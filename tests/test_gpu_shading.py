@@ -2,20 +2,19 @@
 code (rt_verify_shading) against the FP64 oracle, which is itself pinned to
 the reference's shading code (tests/test_oracle_pins.py).
 
-Tolerance.  The reference's own FP32 code (the FP32 oracle is bit-identical to
-it) is not within 1e-5 relative of FP64 on every query: sampled low-roughness
-GGX lobes evaluate 1 - cos^2(theta_h) by cancellation, and about a fifth of
-those queries land between 1e-5 and a few 1e-4.  The GPU is held to the same
-accuracy profile as the reference:
-  * its share of queries within 1e-5 relative of FP64 is at least the
-    reference FP32 share minus two percentage points (three binomial
-    standard errors);
-  * its 99th-percentile relative error is at most twice the reference's
-    (and never required below 1e-5);
-  * evaluation-only ops (BSDF, light and phase evaluation) are within 1e-5 on
-    at least 99.5% of queries.
-Sampling ops take their random numbers from the query; queries whose FP32 and
-FP64 evaluations took different branches are ties and are left out.
+Tolerance: 1e-5 relative to the FP64 oracle on at least 99.5% of queries for
+BSDF evaluation and BSDF sampling (and for every material type when
+sampling), and on light and phase evaluation.  BSDF sampling meets it because
+the renderer samples in double precision: the reference's own FP32 sampler
+(the FP32 oracle is bit-identical to it) is within 1e-5 on only about 84% of
+the sampled queries, since the visible-normal map and the f / pdf chains
+amplify FP32 rounding (by 1 / alpha^2 in the (1 - cos^2) / cos^2 of a sharp
+lobe, and near the rim of the projected disk).  The other sampling ops are
+held to the reference's own FP32 accuracy profile: a share within 1e-5 at
+least the reference's minus two percentage points (three binomial standard
+errors) and a 99th-percentile error at most twice the reference's.  Sampling
+ops take their random numbers from the query; queries whose FP32 reference
+and FP64 evaluations took different branches are ties and are left out.
 """
 import ctypes as C
 import os
@@ -80,8 +79,15 @@ def test_device_shading_matches_fp64(op, key):
         np.savez_compressed(Path(dump) / f"verify_{key}.npz", x=x, gpu=gpu, f32=f32, f64=f64)
     assert share_g >= share_c - 0.02  # 3 binomial standard errors at 4000 queries
     assert p99_g <= max(2 * p99_c, 1e-5)
-    if key in ("bsdf_eval", "light_eval", "phase_eval"):
+    if key in ("bsdf_eval", "bsdf_sample", "light_eval", "phase_eval"):
         assert share_g >= 0.995
+    if key.startswith("bsdf"):
+        mcol = 10 if key == "bsdf_eval" else 13
+        mt = np.array([MATS[int(i)].type for i in x[:, mcol]])[~tie]
+        per = {t: float((eg[mt == t] <= 1e-5).mean()) for t in range(8)}
+        print(f"{key} per material type within 1e-5: {per}")
+        if key == "bsdf_sample":
+            assert min(per.values()) >= 0.995
 
 
 @pytest.mark.gpu

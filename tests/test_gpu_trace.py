@@ -204,7 +204,7 @@ def test_wavefront_any_hit_full_size_spheres(spheres_full, extent):
     and from free space, against the FP64 oracle."""
     spec, s, r, orc = spheres_full
     rng = np.random.default_rng(31 if extent == "finite" else 37)
-    rays = np.concatenate([random_rays(rng, 30000, -2.5, 2.5), surface_rays(spec, orc, rng)])
+    rays = np.concatenate([random_rays(rng, 35000, -2.5, 2.5), surface_rays(spec, orc, rng, n_cam=(320, 180))])
     if extent == "finite":
         rays[:, 7] = rng.uniform(0.02, 3.0, len(rays)).astype(np.float32)
     assert len(rays) >= 50000

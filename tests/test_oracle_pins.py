@@ -203,3 +203,33 @@ def test_point_light_is_the_small_sphere_limit_of_the_reference():
     rel = np.abs(e_sphere - e_point) / e_point
     print(f"point vs sphere: max rel {rel.max():.2e}, mean {rel.mean():.2e} over {n_pts} points")
     assert rel.max() < 2e-3
+
+
+@pytest.mark.parametrize("name", ["cornell", "media", "textured", "portal"])
+def test_oracle_scene_structs_equal_the_products(name):
+    """The oracle builds its scenes without the product library; every
+    material, light and medium it makes from a scene spec must be the one the
+    product's constructors make (field for field, grid resolution included)."""
+    from optixrender_b200 import scenes
+    spec = {"cornell": lambda: scenes.cornell(8, 8, 1), "media": lambda: scenes.media(8, 8, 1, grid_res=16, env_size=(16, 8)),
+            "textured": lambda: scenes.textured(8, 8, 1), "portal": lambda: scenes.portal(8, 8, 1)}[name]()
+    st = pyoracle.oracle_structs()
+
+    def raw(o):
+        b = bytearray(bytes(o))
+        if isinstance(o, rt.Medium):  # the density pointer and the library's majorant default (0 means 8)
+            off = rt.Medium.density.offset
+            b[off:off + 8] = bytes(8)
+            mo = rt.Medium.majorant_res.offset
+            if int.from_bytes(b[mo:mo + 4], "little") == 8:
+                b[mo:mo + 4] = bytes(4)
+        return bytes(b)
+
+    for m in spec.meshes:
+        assert raw(st.material(**m.material)) == raw(rt.material(**m.material))
+    for l in spec.lights:
+        assert raw(st.light(**l)) == raw(rt.light(**l))
+    for md in spec.media:
+        a, b = st.medium(**md), rt.medium(**md)
+        assert raw(a) == raw(b)
+        assert list(a.grid_res) == list(b.grid_res)
