@@ -217,6 +217,8 @@ typedef struct rt_render_stats {
     int64_t h2d_bytes;         /* bytes copied host to device by the last Render() */
     int64_t watchdog_walks;    /* grid-medium walks that hit the device step budget (see rt_renderer_synchronize) */
     int64_t stack_overflows;   /* traversal node groups that found the stack full (0 unless the BVH depth check fails) */
+    float ms_sample;           /* per-kernel device time of BSDF sampling (k_sample; collect_stats only) */
+    float pad;
 } rt_render_stats;
 
 /* AOV kinds for rt_renderer_download_aov. */

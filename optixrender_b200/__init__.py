@@ -88,7 +88,8 @@ class RenderStats(C.Structure):
                 ("launches", C.c_int32), ("ms_total", C.c_float), ("ms_extend", C.c_float),
                 ("ms_shade", C.c_float), ("ms_shadow", C.c_float), ("ms_other", C.c_float),
                 ("extend_launches", C.c_int64), ("nan_throughput_paths", C.c_int64), ("wave_paths", C.c_int64),
-                ("h2d_bytes", C.c_int64), ("watchdog_walks", C.c_int64), ("stack_overflows", C.c_int64)]
+                ("h2d_bytes", C.c_int64), ("watchdog_walks", C.c_int64), ("stack_overflows", C.c_int64),
+                ("ms_sample", C.c_float), ("pad", C.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1,5 +1,10 @@
 // rt_guide.cu - fused kernels of the path-guiding network.
 //
+// Inference (the renderer's per-vertex mixtures and rt_guide_forward) runs
+// on the 5th-generation tensor cores: tcgen05.mma with FP32 accumulators in
+// tensor memory, 128 queries per CTA (k_guide_forward_tc, k_guide_infer_tc).
+// Training runs on warp-level MMA as follows.
+//
 // One warp runs 16 queries at a time through the whole network with
 // mma.sync.m16n8k16 (FP16 operands, FP32 accumulation): the hash-grid
 // features are gathered straight into the A fragments of the first layer,
@@ -23,8 +28,6 @@ namespace rtg {
 
 namespace {
 
-constexpr int kWarps = 4;
-constexpr int kBlock = kWarps * 32;
 constexpr int kBwdWarps = 8;  // training pass: 2 blocks of 8 warps per SM (registers, shared weights)
 // padded shared-memory rows (halves)
 constexpr int kS32 = kIn + 8;   // rows of 32 inputs
@@ -257,19 +260,6 @@ RT_D void load_weights(const __half* __restrict__ mlp, __half* fw, __half* bw) {
 
 RT_D float3 ld_pos(const float* p, int64_t i) { return make_float3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
 
-// Forward of 16 rows: returns the output accumulators (4 n-tiles of 8 outputs).
-RT_D void forward_tile(const __half* sw, const uint32_t (&ax)[2][4], float (&out)[4][4]) {
-    float d64[8][4];
-    uint32_t h[4][4];
-    layer<kIn, kHid, kS32>(ax, sw + kOffW0, d64);
-    pack_relu<kHid>(d64, h);
-    layer<kHid, kHid, kS64>(h, sw + kOffW1, d64);
-    pack_relu<kHid>(d64, h);
-    layer<kHid, kHid, kS64>(h, sw + kOffW2, d64);
-    pack_relu<kHid>(d64, h);
-    layer<kHid, kOut, kS64>(h, sw + kOffW3, out);
-}
-
 RT_D void stage_outputs(const float (&out)[4][4], float* tile) {
     const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
 #pragma unroll
@@ -283,43 +273,6 @@ RT_D void stage_outputs(const float (&out)[4][4], float* tile) {
 }
 
 }  // namespace
-
-// Raw outputs (mode 0) or mixtures (mode 1) of n normalised positions.
-__global__ void __launch_bounds__(kBlock) k_guide_forward(NetView net, const float* __restrict__ pos, int n, int mode,
-                                                          float* __restrict__ raw, Mixture* __restrict__ mix) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __half* sw = reinterpret_cast<__half*>(smem);
-    float* tiles = reinterpret_cast<float*>(smem + kFwdHalves * sizeof(__half));
-    load_weights(net.mlp, sw, nullptr);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2;
-    float* tile = tiles + warp * 16 * kTileStride;
-    const int tiles_total = (n + 15) / 16;
-    for (int tt = blockIdx.x * kWarps + warp; tt < tiles_total; tt += gridDim.x * kWarps) {
-        const int r0 = tt * 16 + g, r1 = r0 + 8;
-        const bool v0 = r0 < n, v1 = r1 < n;
-        float3 x0 = v0 ? ld_pos(pos, r0) : make_float3(0.f, 0.f, 0.f);
-        float3 x1 = v1 ? ld_pos(pos, r1) : make_float3(0.f, 0.f, 0.f);
-        uint32_t ax[2][4];
-        encode_tile(net, x0, x1, v0, v1, ax);
-        float out[4][4];
-        forward_tile(sw, ax, out);
-        stage_outputs(out, tile);
-        __syncwarp();
-        if (lane < 16 && tt * 16 + lane < n) {
-            const int64_t row = int64_t(tt) * 16 + lane;
-            const float* o = tile + lane * kTileStride;
-            if (mode == 0) {
-                for (int k = 0; k < kOut; k++) raw[row * kOut + k] = o[k];
-            } else {
-                Mixture m;
-                head_from_outputs(o, m, net.kappa_hi);
-                mix[row] = m;
-            }
-        }
-        __syncwarp();
-    }
-}
 
 // One vMF lobe of a row's raw outputs o4 = (weight logit, log kappa, theta
 // and phi logits), evaluated at the unit direction d: everything the loss and
@@ -640,46 +593,245 @@ RT_D float3 hit_position(const rtd::Ctx& c, int slot) {
     return guide_input(p, rtd::v3(p0.x, p0.y, p0.z), rtd::v3(p1.x, p1.y, p1.z), rtd::v3(p2.x, p2.y, p2.z), dd, c.G);
 }
 
+// ======================================================================
+// Inference on the 5th-generation tensor cores (tcgen05, accumulators in
+// tensor memory).  A CTA of kTcRows = 128 threads runs 128 queries, one per
+// thread and per TMEM lane, through the 32-64-64-64-32 MLP:
+//   * thread t gathers its query's 16 hash-grid levels and writes row t of
+//     the A operand in shared memory: K-major, the canonical no-swizzle
+//     layout of 8-row x 16-byte core matrices (LBO = 128 B between the two
+//     core matrices of a 16-wide K step, SBO = K * 2 * 8 B between 8-row
+//     groups);
+//   * thread 0 issues the layer's tcgen05.mma.kind::f16 (M = 128, N = 64 or
+//     32, K = 16 per instruction, FP16 operands from shared memory, FP32
+//     accumulators in 64 TMEM columns) and commits them to an mbarrier;
+//   * every warp reads its 32 TMEM lanes back (tcgen05.ld 32x32b), applies
+//     ReLU, rounds to FP16 and writes the next layer's A rows;
+//   * the last layer's 32 outputs, in registers, become the mixture.
+// The weights (B operands, [out][in] = N x K, K-major) are written once per
+// CTA in the same layout.  Every wait on the mbarrier is bounded: a timeout
+// is counted in g_tc_timeouts (reported by the host as a watchdog error),
+// and the CTA stops issuing, frees its TMEM and returns.
+// ======================================================================
+constexpr int kTcRows = 128;
+constexpr int kTcCols = 64;  // TMEM columns: the widest layer's accumulators
+constexpr uint32_t kTcA = 0, kTcW0 = kTcA + kTcRows * kHid * 2, kTcW1 = kTcW0 + kHid * kIn * 2,
+                   kTcW2 = kTcW1 + kHid * kHid * 2, kTcW3 = kTcW2 + kHid * kHid * 2, kTcBar = kTcW3 + kOut * kHid * 2,
+                   kTcSlot = kTcBar + 8, kTcSmem = kTcSlot + 8;
+constexpr long long kTcWaitLimit = 1ll << 22;  // mbarrier polls before a wait is given up
+__device__ int g_tc_timeouts;
+
+// Byte offset of element (row r, column k) of an R x K FP16 operand in the
+// canonical K-major no-swizzle layout.
+RT_D uint32_t tc_off(int r, int k, int K) {
+    return uint32_t(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+// Shared-memory matrix descriptor (sm_100): start, leading (K) and stride
+// (row-group) byte offsets >> 4, descriptor version 1, no swizzle.
+RT_D uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulators, FP16 A and B, both
+// K-major, M = 128, N.
+RT_HD constexpr uint32_t tc_idesc(int n) { return (1u << 4) | (uint32_t(n >> 3) << 17) | (uint32_t(kTcRows >> 4) << 24); }
+
+RT_D uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+RT_D void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+RT_D void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+RT_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+RT_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+// generic-proxy writes of shared memory made visible to the tensor cores' reads
+RT_D void tc_fence_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+RT_D bool tc_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kTcWaitLimit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+RT_D void tmem_ld_x64(uint32_t taddr, float (&v)[64]) {
+    uint32_t r[64];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
+}
+
+RT_D void tmem_ld_x32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+
+// Weights -> shared memory, B operands in the canonical layout.
+RT_D void tc_load_weights(const __half* __restrict__ mlp, unsigned char* sm) {
+    const __half* W[4] = {mlp, mlp + kW0, mlp + kW0 + kW1, mlp + kW0 + kW1 + kW2};
+    const uint32_t off[4] = {kTcW0, kTcW1, kTcW2, kTcW3};
+    const int rows[4] = {kHid, kHid, kHid, kOut}, cols[4] = {kIn, kHid, kHid, kHid};
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+        for (int i = threadIdx.x; i < rows[l] * cols[l]; i += blockDim.x) {
+            const int o = i / cols[l], k = i % cols[l];
+            *reinterpret_cast<__half*>(sm + off[l] + tc_off(o, k, cols[l])) = W[l][i];
+        }
+}
+
+// Row `row` of the first layer's A operand: the 16 levels' features of x.
+RT_D void tc_encode_row(const NetView& net, float3 x, bool valid, unsigned char* sm, int row) {
+    uint32_t f[kLevels];
+#pragma unroll
+    for (int l = 0; l < kLevels; l++) f[l] = valid ? encode_level(net.table, net.res[l], l, x) : 0u;
+#pragma unroll
+    for (int j = 0; j < kIn / 8; j++)
+        *reinterpret_cast<uint4*>(sm + kTcA + tc_off(row, 8 * j, kIn)) =
+            make_uint4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+}
+
+// The four layers for the 128 rows staged in A; this thread's 32 outputs.
+// Returns false when a wait timed out (outputs undefined).
+RT_D bool tc_mlp(unsigned char* sm, uint32_t tmem, uint32_t& parity, float (&out)[kOut]) {
+    const uint32_t bar = smem_u32(sm + kTcBar), a_base = smem_u32(sm + kTcA);
+    const uint32_t taddr = tmem + (uint32_t(threadIdx.x >> 5) * 32u << 16);
+    const uint32_t w_off[4] = {kTcW0, kTcW1, kTcW2, kTcW3};
+#pragma unroll
+    for (int layer = 0; layer < 4; layer++) {
+        const int K = layer == 0 ? kIn : kHid, N = layer == 3 ? kOut : kHid;
+        tc_fence_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (threadIdx.x == 0) {
+            const uint32_t w_base = smem_u32(sm + w_off[layer]);
+#pragma unroll
+            for (int ks = 0; ks < K / 16; ks++)
+                tc_mma(tmem, tc_desc(a_base + 256u * ks, 128u, uint32_t(K) * 16u),
+                       tc_desc(w_base + 256u * ks, 128u, uint32_t(K) * 16u), tc_idesc(N), ks > 0 ? 1u : 0u);
+            tc_commit(bar);
+        }
+        // the CTA agrees on the outcome, so no thread is left at a barrier
+        const bool ok = __syncthreads_and(tc_wait(bar, parity)) != 0;
+        parity ^= 1u;
+        if (!ok) return false;
+        tc_fence_after();
+        if (layer < 3) {
+            float v[kHid];
+            tmem_ld_x64(taddr, v);
+#pragma unroll
+            for (int j = 0; j < kHid / 8; j++)
+                *reinterpret_cast<uint4*>(sm + kTcA + tc_off(threadIdx.x, 8 * j, kHid)) = make_uint4(
+                    pack_h2(fmaxf(v[8 * j], 0.f), fmaxf(v[8 * j + 1], 0.f)),
+                    pack_h2(fmaxf(v[8 * j + 2], 0.f), fmaxf(v[8 * j + 3], 0.f)),
+                    pack_h2(fmaxf(v[8 * j + 4], 0.f), fmaxf(v[8 * j + 5], 0.f)),
+                    pack_h2(fmaxf(v[8 * j + 6], 0.f), fmaxf(v[8 * j + 7], 0.f)));
+        } else {
+            tmem_ld_x32(taddr, out);
+        }
+    }
+    return true;
+}
+
+// Set-up shared by the kernels: weights, mbarrier, TMEM columns.
+RT_D uint32_t tc_setup(const NetView& net, unsigned char* sm) {
+    tc_load_weights(net.mlp, sm);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(sm + kTcBar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     ::"r"(smem_u32(sm + kTcSlot)), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    tc_fence_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return *reinterpret_cast<volatile uint32_t*>(sm + kTcSlot);
+}
+RT_D void tc_teardown(uint32_t tmem, bool ok) {
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols) : "memory");
+    if (!ok && threadIdx.x == 0) atomicAdd(&g_tc_timeouts, 1);
+}
+
+// Raw outputs (mode 0) or mixtures (mode 1) of n normalised positions.
+__global__ void __launch_bounds__(kTcRows) k_guide_forward_tc(NetView net, const float* __restrict__ pos, int n,
+                                                              int mode, float* __restrict__ raw,
+                                                              Mixture* __restrict__ mix) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const uint32_t tmem = tc_setup(net, sm);
+    uint32_t parity = 0;
+    bool ok = true;
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const int row = t * kTcRows + int(threadIdx.x);
+        const bool valid = row < n;
+        tc_encode_row(net, valid ? ld_pos(pos, row) : make_float3(0.f, 0.f, 0.f), valid, sm, threadIdx.x);
+        float out[kOut];
+        ok = tc_mlp(sm, tmem, parity, out);
+        if (ok && valid) {
+            if (mode == 0) {
+#pragma unroll
+                for (int k = 0; k < kOut; k++) raw[int64_t(row) * kOut + k] = out[k];
+            } else {
+                Mixture m;
+                head_from_outputs(out, m, net.kappa_hi);
+                mix[row] = m;
+            }
+        }
+    }
+    tc_teardown(tmem, ok);
+}
+
 // Mixtures of this bounce's guided vertices (surface hits of guided material
 // types), written per slot for the shade kernel.
-// Warps per block of k_guide_infer, which share the weights in shared memory.
-// 16 warps x 2 blocks per SM (register-limited) keep 32 warps per SM in the
-// latency-bound hash-grid gathers: 25% less time per guided sample than
-// 4 x 4 or 4 x 6, on the portal scene.
-constexpr int kInferWarps = 16;
-constexpr int kInferBlocksPerSm = 2;
-__global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(rtd::Ctx c, NetView net) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __half* sw = reinterpret_cast<__half*>(smem);
-    float* tiles = reinterpret_cast<float*>(smem + kFwdHalves * sizeof(__half));
-    load_weights(net.mlp, sw, nullptr);
-    __syncthreads();
+__global__ void __launch_bounds__(kTcRows) k_guide_infer_tc(rtd::Ctx c, NetView net) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const uint32_t tmem = tc_setup(net, sm);
     const rtd::WaveBufs& B = c.wb;
     const GuidedItems gi = guided_items(B.ctl);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2;
-    float* tile = tiles + warp * 16 * kTileStride;
     const int n = gi.n;
-    const int tiles_total = (n + 15) / 16;
-    for (int tt = blockIdx.x * kInferWarps + warp; tt < tiles_total; tt += gridDim.x * kInferWarps) {
-        const int r0 = tt * 16 + g, r1 = r0 + 8;
-        const bool v0 = r0 < n, v1 = r1 < n;
-        const int s0 = v0 ? guided_slot(gi, B, r0) : 0, s1 = v1 ? guided_slot(gi, B, r1) : 0;
-        const float3 x0 = v0 ? hit_position(c, s0) : make_float3(0.f, 0.f, 0.f);
-        const float3 x1 = v1 ? hit_position(c, s1) : make_float3(0.f, 0.f, 0.f);
-        uint32_t ax[2][4];
-        encode_tile(net, x0, x1, v0, v1, ax);
-        float out[4][4];
-        forward_tile(sw, ax, out);
-        stage_outputs(out, tile);
-        __syncwarp();
-        if (lane < 16 && tt * 16 + lane < n) {
-            const int slot = guided_slot(gi, B, tt * 16 + lane);
+    uint32_t parity = 0;
+    bool ok = true;
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const int r = t * kTcRows + int(threadIdx.x);
+        const bool valid = r < n;
+        const int slot = valid ? guided_slot(gi, B, r) : 0;
+        tc_encode_row(net, valid ? hit_position(c, slot) : make_float3(0.f, 0.f, 0.f), valid, sm, threadIdx.x);
+        float out[kOut];
+        ok = tc_mlp(sm, tmem, parity, out);
+        if (ok && valid) {
             Mixture m;
-            head_from_outputs(tile + lane * kTileStride, m, net.kappa_hi);
+            head_from_outputs(out, m, net.kappa_hi);
             c.G.mix[slot] = m;
         }
-        __syncwarp();
     }
+    tc_teardown(tmem, ok);
 }
 
 // End of a training wave: turns each path's records into training samples
@@ -856,35 +1008,34 @@ __global__ void k_guide_pdf_sample(const Mixture* __restrict__ mix, const float*
 
 namespace rtgh {
 
-size_t forward_smem() { return size_t(rtg::kFwdHalves) * 2 + size_t(rtg::kWarps) * 16 * rtg::kTileStride * 4; }
-static size_t infer_smem() {
-    return size_t(rtg::kFwdHalves) * 2 + size_t(rtg::kInferWarps) * 16 * rtg::kTileStride * 4;
-}
 size_t backward_smem() {
     return size_t(rtg::kFwdHalves + rtg::kBwdHalves) * 2 + size_t(rtg::kBwdWarps) * 16 * (rtg::kTileStride + 3) * 4 +
            size_t(rtg::kLevels) * 4;
 }
 
 cudaError_t prepare_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(rtg::k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(forward_smem()));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(rtg::k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(infer_smem()));
-    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(rtg::k_guide_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(backward_smem()));
 }
 
-static int grid_for_tiles(int n, int sms) {
-    const int tiles = (n + 15) / 16;
-    const int blocks = (tiles + rtg::kWarps - 1) / rtg::kWarps;
-    return blocks < sms * 8 ? (blocks > 0 ? blocks : 1) : sms * 8;
-}
+// Inference CTAs per SM: 4 of 128 threads (122 registers each); with 64 TMEM
+// columns a CTA, at most 256 of the SM's 512 columns are allocated, so no
+// CTA waits for tensor memory.
+constexpr int kTcBlocksPerSm = 4;
 
 void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, float* raw, rtg::Mixture* mix, int sms,
                     cudaStream_t st) {
     if (n <= 0) return;
-    rtg::k_guide_forward<<<grid_for_tiles(n, sms), rtg::kBlock, forward_smem(), st>>>(net, pos, n, mode, raw, mix);
+    const int tiles = (n + rtg::kTcRows - 1) / rtg::kTcRows;
+    rtg::k_guide_forward_tc<<<std::min(tiles, sms * kTcBlocksPerSm), rtg::kTcRows, rtg::kTcSmem, st>>>(net, pos, n,
+                                                                                                      mode, raw, mix);
+}
+
+int take_tc_timeouts() {
+    int n = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&n, rtg::g_tc_timeouts, sizeof(int)) != cudaSuccess) return 0;
+    if (n) cudaMemcpyToSymbol(rtg::g_tc_timeouts, &zero, sizeof(int));
+    return n;
 }
 
 size_t frag_bytes_per_tile() { return size_t(rtg::kFragWords) * 32 * 4; }
@@ -909,7 +1060,7 @@ void launch_backward(const rtg::NetView& net, const float* pos, const float* dir
 }
 
 void launch_infer(const rtd::Ctx& c, const rtg::NetView& net, int sms, cudaStream_t st) {
-    rtg::k_guide_infer<<<sms * rtg::kInferBlocksPerSm, rtg::kInferWarps * 32, infer_smem(), st>>>(c, net);
+    rtg::k_guide_infer_tc<<<sms * kTcBlocksPerSm, rtg::kTcRows, rtg::kTcSmem, st>>>(c, net);
 }
 
 void launch_collect(const rtd::Ctx& c, float4* buf, int* count, int cap, cudaStream_t st) {

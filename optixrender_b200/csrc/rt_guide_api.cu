@@ -253,6 +253,14 @@ rt_status rt_guide_set_params(rt_guide* g, const float* table, const float* mlp)
     return RT_OK;
 }
 
+// The inference kernels' bounded waits on the tensor cores, after a synchronize.
+static rt_status tc_status(const char* what) {
+    const int n = rtgh::take_tc_timeouts();
+    if (n == 0) return RT_OK;
+    return fail(RT_ERR_DEVICE_WATCHDOG, std::string(what) + ": " + std::to_string(n) +
+                                            " inference blocks gave up waiting for their tensor-core work");
+}
+
 rt_status rt_guide_forward(rt_guide* g, const float* pos, int64_t n, float* raw) {
     if (!g || n < 0 || (n > 0 && (!pos || !raw)) || n > (int64_t(1) << 28))
         return fail(RT_ERR_INVALID_ARG, "rt_guide_forward: bad argument");
@@ -265,7 +273,7 @@ rt_status rt_guide_forward(rt_guide* g, const float* pos, int64_t n, float* raw)
     GD_CUDA(cudaGetLastError(), "rt_guide_forward");
     GD_CUDA(cudaMemcpyAsync(raw, dr.ptr, dr.bytes, cudaMemcpyDeviceToHost, g->stream), "rt_guide_forward");
     GD_CUDA(cudaStreamSynchronize(g->stream), "rt_guide_forward");
-    return RT_OK;
+    return tc_status("rt_guide_forward");
 }
 
 rt_status rt_guide_gradients(rt_guide* g, const float* pos, const float* dir, const float* weight, int64_t n,
@@ -362,7 +370,7 @@ rt_status rt_guide_pdf(rt_guide* g, const float* pos, const float* dir, const fl
     GD_CUDA(cudaMemcpyAsync(pdf, dpdf.ptr, dpdf.bytes, cudaMemcpyDeviceToHost, g->stream), "rt_guide_pdf");
     if (u) GD_CUDA(cudaMemcpyAsync(out_dir, dout.ptr, dout.bytes, cudaMemcpyDeviceToHost, g->stream), "rt_guide_pdf");
     GD_CUDA(cudaStreamSynchronize(g->stream), "rt_guide_pdf");
-    return RT_OK;
+    return tc_status("rt_guide_pdf");
 }
 
 }  // extern "C"

@@ -8,9 +8,11 @@
 
 namespace rtgh {
 
-size_t forward_smem();
 size_t backward_smem();
 cudaError_t prepare_kernels();
+// Inference CTAs that gave up waiting on their tensor-core work since the
+// last call (the counter is cleared); each is reported as a watchdog error.
+int take_tc_timeouts();
 // mode 0: raw outputs (n x 32 floats); mode 1: one Mixture per position.
 void launch_forward(const rtg::NetView& net, const float* pos, int n, int mode, float* raw, rtg::Mixture* mix, int sms,
                     cudaStream_t st);

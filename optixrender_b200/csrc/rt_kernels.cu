@@ -79,6 +79,8 @@ __global__ void k_raygen(Ctx c) {
         ctl->fetch_ext = 0;
         ctl->fetch_shade = 0;
         ctl->fetch_shadow = 0;
+        ctl->sample_count = 0;
+        ctl->fetch_sample = 0;
         for (int b = 0; b < kShadeBuckets; b++) ctl->bucket[b] = 0;
     }
     if (slot >= W.wave_count) return;
@@ -161,6 +163,8 @@ __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_extend(Ctx c) {
         ctl->count[nxt] = 0;
         ctl->shadow_count = 0;
         ctl->fetch_shade = 0;
+        ctl->sample_count = 0;
+        ctl->fetch_sample = 0;
     }
     const int total = ctl->count[cur];
     uint32_t nodes = 0, tris = 0, rays = 0, overflows = 0;
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
         int base = warp_fetch(&ctl->fetch_shade, lane);
         if (base >= total) break;
         int i = base + lane;
-        bool cont = false;
+        bool cont = false, defer = false;
         bool sh0 = false, sh1 = false;
         int slot = 0;
         v3 s0o, s0d, s1o, s1d;
@@ -536,7 +540,6 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                         }
                     }
                     // BSDF sampling, devicePrograms.cu:474-477
-                    float bpdf = 0.0f;
                     if (Full && gp > 0.0f) {
                         // one-sample MIS of the mixture and the BSDF: the direction comes
                         // from the mixture with probability gp, and is weighted by the
@@ -545,8 +548,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                             float u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
                             L = rtg::mixture_sample(gmix, u0, u1, u2);
                         } else {
+                            // only the direction is used (the weight comes from
+                            // guide_bsdf), so the FP32 sampler serves here
                             float unused;
-                            sample_material(sc, s, rng, V, L, unused);
+                            sample_material_t<float>(sc, s, rng, V, L, unused);
                         }
                         // weighted by what plain BSDF sampling integrates over the combined
                         // real density; the emission MIS weight at the next vertex uses the
@@ -562,14 +567,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                         rec_pdf = pm;
                         rec_cos = ct;
                     } else {
-                        v3 f = sample_material(sc, s, rng, V, L, bpdf);
-                        float ct = fabsf(dot(s.sn, L));
-                        history *= (f * ct / bpdf);
-                        pre_pdf = bpdf;
+                        // SampleMaterial, the path weight, Russian roulette and
+                        // the next ray follow in k_sample
+                        defer = true;
                     }
                 }
             }
-            if (alive) {
+            if (alive && !defer) {
                 // Russian roulette, devicePrograms.cu:480-489
                 if (bounce >= jp.rr_depth) {
                     float prr = fminf((history.x + history.y + history.z) / 3.0f, 0.95f);
@@ -584,7 +588,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                     nan_paths++;
                 }
             }
-            cont = alive && (bounce + 1 < jp.max_depth);
+            cont = alive && !defer && (bounce + 1 < jp.max_depth);
             if (Full && G.rec != nullptr && cont && rec_pdf > 0.0f && rec_cos > 0.0f && bounce < rtg::kGuideRec) {
                 // training record: network input, pdf, direction, |cos|, throughput after this vertex
                 float4* R = G.rec + size_t(bounce) * 4 * cap + slot;
@@ -600,10 +604,15 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
                 B.ray_o[slot] = f4(pos, 0.0f);
                 B.ray_d[slot] = f4(L, 0.0f);
                 B.thr[slot] = f4(history, pre_pdf);
+            } else if (defer) {  // k_sample's inputs: origin of the next ray and the front-face flag
+                B.ray_o[slot] = f4(pos, s.front ? 1.0f : 0.0f);
+                B.thr[slot] = f4(history, pre_pdf);
             }
         }
         int qp = warp_append(&ctl->count[nxt], cont, lane);
         if (cont) B.queue[nxt][qp] = slot;
+        int sp = warp_append(&ctl->sample_count, defer, lane);
+        if (defer) B.squeue[sp] = slot;
         int p0 = warp_append(&ctl->shadow_count, sh0, lane);
         if (sh0) {
             B.sh_o[p0] = f4(s0o, s0t);
@@ -617,6 +626,86 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
     }
     if (Stats) warp_stat(&ctl->stats[7], nan_paths);
     if (budget_hits) atomicAdd(&ctl->error, budget_hits);
+}
+
+// ------------------------------------------------------------------ BSDF sampling
+// The paths k_shade leaves at a surface's BSDF sampling (devicePrograms.cu:
+// 474-489): SampleMaterial in double precision (sample_material), the path
+// weight, Russian roulette and the next ray.  A kernel of its own, so that
+// the double-precision sampler's registers do not lower the occupancy of the
+// much larger shade kernel.  Per slot it reads the origin of the next ray and
+// the front-face flag (ray_o), the incoming direction (ray_d), the
+// throughput and pdf (thr), the shading normal and mesh of the hit (stale)
+// and the random state, which continues where k_shade left it.
+template <bool Stats>
+__global__ void __launch_bounds__(kBlock) k_sample(Ctx c) {
+    WaveCtl* ctl = c.wb.ctl;
+    const int nxt = (c.bounce & 1) ^ 1;
+    const int bounce = c.bounce;
+    const int total = ctl->sample_count;
+    const WaveBufs& B = c.wb;
+    const WaveParams& W = wave_of(c);
+    const int lane = threadIdx.x & 31;
+    uint32_t nan_paths = 0;
+    while (true) {
+        const int base = warp_fetch(&ctl->fetch_sample, lane);
+        if (base >= total) break;
+        const int i = base + lane;
+        bool cont = false;
+        int slot = 0;
+        if (i < total) {
+            slot = B.squeue[i];
+            const Segment& sgm = W.seg[find_segment(W, slot)];
+            const JobDesc* jd = c.jobs + sgm.job;
+            const SceneView& sc = jd->sc;
+            const JobParams& jp = jd->job;
+            const float4 o4 = B.ray_o[slot], d4 = B.ray_d[slot], th = B.thr[slot], st = B.stale[slot];
+            const uint2 rs = B.rng[slot];
+            Rng rng;
+            rng.state = uint64_t(rs.x) | (uint64_t(rs.y) << 32);
+            rng.inc = jp.rng == RT_RNG_LCG ? 0 : pcg_inc(uint64_t(sgm.path_begin + (slot - sgm.slot_begin)));
+            Surf s;
+            s.sn = xyz(st);
+            s.front = o4.w != 0.0f;
+            const int mesh = __float_as_int(st.w);
+            if (mesh < 0)
+                s.mat = nullptr;
+            else if (mesh & kStaleTextured)
+                s.mat = B.mat_tex + slot;
+            else
+                s.mat = sc.materials + sc.meshes[mesh].material;
+            const v3 d = xyz(d4);
+            const v3 V = -d;
+            v3 L = d, history = xyz(th);
+            float bpdf = 0.0f;
+            const v3 f = sample_material(sc, s, rng, V, L, bpdf);
+            const float ct = fabsf(dot(s.sn, L));
+            history *= (f * ct / bpdf);
+            bool alive = true;
+            // Russian roulette, devicePrograms.cu:480-489
+            if (bounce >= jp.rr_depth) {
+                float prr = fminf((history.x + history.y + history.z) / 3.0f, 0.95f);
+                if (rng.next() > prr) {
+                    alive = false;
+                } else {
+                    history /= prr;
+                }
+            }
+            if (alive && any_nan(history)) {
+                alive = false;
+                nan_paths++;
+            }
+            cont = alive && (bounce + 1 < jp.max_depth);
+            B.rng[slot] = make_uint2(uint32_t(rng.state), uint32_t(rng.state >> 32));
+            if (cont) {
+                B.ray_d[slot] = f4(L, 0.0f);
+                B.thr[slot] = f4(history, bpdf);
+            }
+        }
+        const int qp = warp_append(&ctl->count[nxt], cont, lane);
+        if (cont) B.queue[nxt][qp] = slot;
+    }
+    if (Stats) warp_stat(&ctl->stats[7], nan_paths);
 }
 
 // ------------------------------------------------------------------ shadow
@@ -1080,6 +1169,8 @@ void query_shape(LaunchShape& s) {
     s.blocks_shade_plain = s.sms * (b > 0 ? b : 1);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shadow<false>, kBlock, 0);
     s.blocks_shadow = s.sms * (b > 0 ? b : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sample<false>, kBlock, 0);
+    s.blocks_sample = s.sms * (b > 0 ? b : 1);
 }
 
 static unsigned grid_for(int64_t n, int block) { return unsigned((n + block - 1) / block); }
@@ -1108,6 +1199,12 @@ void launch_shade(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t s
         else
             k_shade<false, false><<<blocks, kBlock, 0, st>>>(c);
     }
+}
+void launch_sample(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
+    if (stats)
+        k_sample<true><<<s.blocks_sample, kBlock, 0, st>>>(c);
+    else
+        k_sample<false><<<s.blocks_sample, kBlock, 0, st>>>(c);
 }
 void launch_shadow(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
     if (stats)

@@ -60,7 +60,9 @@ struct WaveCtl {
     unsigned long long stats[8];  // extend rays, shadow rays, ext nodes, ext tris, sh nodes, sh tris,
                                   // NaN samples, paths ended by a NaN throughput
     int bucket[kShadeBuckets];    // extend results per shade bucket
-    int pad2[3];
+    int sample_count;             // paths k_shade left at BSDF sampling (k_sample's queue)
+    int fetch_sample;
+    int pad2;
 };
 
 // Structure-of-arrays path state, one entry per slot of a wave.
@@ -77,6 +79,7 @@ struct WaveBufs {
     float2* aov_n;   // normal.y, normal.z
     uint2* rng;      // random state
     int* queue[2];   // active slots
+    int* squeue;     // slots waiting for BSDF sampling (k_sample)
     float4* sh_o;    // shadow ray origin, tmax
     float4* sh_d;    // shadow ray direction, slot * 2 + channel (bits)
     int* sorted;     // kShadeBuckets regions of `capacity` slots: extend results by material type (or null)
@@ -128,6 +131,7 @@ struct LaunchShape {
     int sms;
     int blocks_extend, blocks_shade, blocks_shadow;
     int blocks_shade_plain;  // the shade kernel without media, guiding and textures
+    int blocks_sample;
 };
 void query_shape(LaunchShape& s);
 // The a-trous denoiser: colour, albedo and normal AOVs (W x H float4) in;
@@ -154,6 +158,8 @@ void launch_begin(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cud
 void launch_raygen(const rtd::Ctx& c, cudaStream_t st);
 void launch_extend(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
 void launch_shade(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
+// BSDF sampling of the paths k_shade left at a surface (runs between shade and shadow).
+void launch_sample(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
 void launch_shadow(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
 void launch_resolve(const rtd::Ctx& c, cudaStream_t st);
 void launch_next_wave(const rtd::Ctx& c, cudaStream_t st);

@@ -223,7 +223,7 @@ struct rt_renderer {
     int pw = 0, ph = 0;
     DevBuf acc_color, acc_albedo, acc_normal, lcg_state, color, albedo, normal, rgba8;
     int capacity = 0;
-    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, ctl, segs, job;
+    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sq, sh_o, sh_d, ctl, segs, job;
     DevBuf sorted;            // shade queue by material type
     DevBuf dn_tmp0, dn_tmp1, dn_out;  // denoiser scratch and output (rt_options.denoise)
     int dn_pixels = 0;                // pixels covered by the denoiser buffers
@@ -303,6 +303,7 @@ rt_status ensure_waves(rt_renderer* r, int cap) {
     RT_CUDA(r->rng.alloc(n * sizeof(uint2)), "allocate path state");
     RT_CUDA(r->q0.alloc(n * sizeof(int)), "allocate queues");
     RT_CUDA(r->q1.alloc(n * sizeof(int)), "allocate queues");
+    RT_CUDA(r->sq.alloc(n * sizeof(int)), "allocate queues");
     RT_CUDA(r->sh_o.alloc(2 * n * sizeof(float4)), "allocate shadow queue");
     RT_CUDA(r->sh_d.alloc(2 * n * sizeof(float4)), "allocate shadow queue");
     if (r->sort_shade) RT_CUDA(r->sorted.alloc(size_t(kShadeBuckets) * n * sizeof(int)), "allocate shade buckets");
@@ -326,6 +327,7 @@ void wave_bufs(rt_renderer* r, WaveBufs& b) {
     b.rng = r->rng.as<uint2>();
     b.queue[0] = r->q0.as<int>();
     b.queue[1] = r->q1.as<int>();
+    b.squeue = r->sq.as<int>();
     b.sh_o = r->sh_o.as<float4>();
     b.sh_d = r->sh_d.as<float4>();
     b.sorted = r->sort_shade ? r->sorted.as<int>() : nullptr;
@@ -337,7 +339,7 @@ void wave_bufs(rt_renderer* r, WaveBufs& b) {
 int auto_capacity(const rt_options& o, int64_t npix, int64_t total) {
     // Large waves: the last bounces of a wave carry few paths and run at the
     // latency of a handful of rays, so fewer, larger waves spend less time
-    // there.  Automatic: up to 2^26 slots (268 B each, 18 GB), at most a
+    // there.  Automatic: up to 2^26 slots (272 B each, 18 GB), at most a
     // quarter of the free device memory.
     int64_t cap = o.wave_paths > 0 ? int64_t(o.wave_paths) : std::max<int64_t>(npix, int64_t(1) << 26);
     if (o.wave_paths <= 0) {
@@ -646,12 +648,15 @@ rt_status rt_renderer_render(rt_renderer* r) {
             if (guided) rtgh::launch_infer(c, net, gsms, s);
             rth::launch_shade(c, r->shape, timed, s);
             if (timed) cudaEventRecord(r->timer.next(), s);
+            rth::launch_sample(c, r->shape, timed, s);
+            if (timed) cudaEventRecord(r->timer.next(), s);
             rth::launch_shadow(c, r->shape, timed, s);
             if (timed) {
                 cudaEventRecord(r->timer.next(), s);
                 r->timer.marks.push_back({0, i0});
                 r->timer.marks.push_back({1, i0 + 1});
-                r->timer.marks.push_back({2, i0 + 2});
+                r->timer.marks.push_back({3, i0 + 2});
+                r->timer.marks.push_back({2, i0 + 3});
             }
         }
         rth::launch_resolve(c, s);
@@ -698,7 +703,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
         }
         for (int64_t w = 0; w < plain_waves; w++) RT_CUDA(cudaGraphLaunch(r->graph, s), "launch wave graph");
     }
-    launches += int(nwaves) * (3 * o.max_depth + 3) + (guided ? int(nwaves) * o.max_depth : 0) +
+    launches += int(nwaves) * (4 * o.max_depth + 3) + (guided ? int(nwaves) * o.max_depth : 0) +
                 int(train_waves) * (1 + 3 * o.guide_steps);
     ext = int(nwaves) * o.max_depth;
     rth::launch_finalize(hj, dj, s);
@@ -777,6 +782,12 @@ rt_status rt_renderer_synchronize(rt_renderer* r) {
                             std::to_string(kMaxTrackingSteps) + "-step budget and were ended with zero weight");
         if (hits[1] > 0) return overflow_status(hits[1], "the last render");
     }
+    if (r->opt.guided) {  // bounded waits of the guide network's tensor-core inference
+        const int n = rtgh::take_tc_timeouts();
+        if (n > 0)
+            return fail(RT_ERR_DEVICE_WATCHDOG,
+                        std::to_string(n) + " guide inference blocks gave up waiting for their tensor-core work");
+    }
     return RT_OK;
 }
 
@@ -853,7 +864,7 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, r->ev0, r->ev1);
     out->ms_total = ms;
-    float cls[3] = {0.f, 0.f, 0.f};
+    float cls[4] = {0.f, 0.f, 0.f, 0.f};
     for (auto& m : r->timer.marks) {
         float t = 0.0f;
         cudaEventElapsedTime(&t, r->timer.pool[m.second], r->timer.pool[m.second + 1]);
@@ -862,7 +873,8 @@ rt_status rt_renderer_get_stats(const rt_renderer* rc, rt_render_stats* out) {
     out->ms_extend = cls[0];
     out->ms_shade = cls[1];
     out->ms_shadow = cls[2];
-    out->ms_other = r->timer.marks.empty() ? 0.0f : ms - cls[0] - cls[1] - cls[2];
+    out->ms_sample = cls[3];
+    out->ms_other = r->timer.marks.empty() ? 0.0f : ms - cls[0] - cls[1] - cls[2] - cls[3];
     return RT_OK;
 }
 

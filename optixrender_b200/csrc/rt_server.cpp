@@ -115,7 +115,7 @@ struct rt_server {
     int64_t bytes_in_use = 0;
     // device state
     DevBuf job_table, ring, wave_index, ctl;
-    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sh_o, sh_d, sorted;
+    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sq, sh_o, sh_d, sorted;
     DevBuf mat_tex;  // per-slot textured materials, once a scene with textures is resident
     // guiding: per-slot mixtures, training records and samples, one batch
     DevBuf g_mix, g_rec, g_buf, g_count, g_wsum, g_bpos, g_bdir, g_bw;
@@ -186,6 +186,7 @@ rt_status setup(rt_server* s) {
     SV_CUDA(s->rng.alloc(cap * sizeof(uint2)), "allocate path state");
     SV_CUDA(s->q0.alloc(cap * sizeof(int)), "allocate queues");
     SV_CUDA(s->q1.alloc(cap * sizeof(int)), "allocate queues");
+    SV_CUDA(s->sq.alloc(cap * sizeof(int)), "allocate queues");
     SV_CUDA(s->sh_o.alloc(2 * cap * sizeof(float4)), "allocate shadow queue");
     SV_CUDA(s->sh_d.alloc(2 * cap * sizeof(float4)), "allocate shadow queue");
     SV_CUDA(s->sorted.alloc(size_t(kShadeBuckets) * cap * sizeof(int)), "allocate shade buckets");
@@ -261,6 +262,7 @@ Ctx make_ctx(rt_server* s, int group) {
     b.rng = s->rng.as<uint2>();
     b.queue[0] = s->q0.as<int>();
     b.queue[1] = s->q1.as<int>();
+    b.squeue = s->sq.as<int>();
     b.sh_o = s->sh_o.as<float4>();
     b.sh_d = s->sh_d.as<float4>();
     b.sorted = s->sorted.as<int>();
@@ -304,6 +306,7 @@ void issue_wave(rt_server* s, const Ctx& c0, int depth, int gscene, bool trainin
         rth::launch_extend(c, s->shape, false, s->stream);
         if (gscene >= 0) rtgh::launch_infer(c, net, gsms, s->stream);
         rth::launch_shade(c, s->shape, false, s->stream);
+        rth::launch_sample(c, s->shape, false, s->stream);
         rth::launch_shadow(c, s->shape, false, s->stream);
     }
     rth::launch_resolve(c, s->stream);
