@@ -71,6 +71,18 @@ RT_HD double fmax_r(float a, double b) { return fmax(double(a), b); }
 RT_HD double fmax_r(double a, float b) { return fmax(a, double(b)); }
 RT_HD void sincos_r(float a, float* s, float* c) { sincosf(a, s, c); }
 RT_HD void sincos_r(double a, double* s, double* c) { sincos(a, s, c); }
+// sin and cos of 2 pi u for u in [0, 1): FP32 keeps the reference's
+// sincosf(2 pi u); FP64 takes sincospi(2 u), which reduces its argument
+// exactly (no wide-range reduction path) and differs from sin(2 pi u)
+// evaluated in double only by the rounding of 2 pi u (~1e-16).
+RT_HD void sincos_2pi_r(float u, float* s, float* c) { sincosf(6.28318530717958647692f * u, s, c); }
+RT_HD void sincos_2pi_r(double u, double* s, double* c) {
+#ifdef __CUDA_ARCH__
+    sincospi(2.0 * u, s, c);
+#else
+    sincos_r(6.28318530717958647692 * u, s, c);
+#endif
+}
 template <class R> RT_HD R length(vec3t<R> v) { return sqrt_r(dot(v, v)); }
 // Component-wise division by the length, as gdt's normalize (vec.h:306-310).
 template <class R> RT_HD vec3t<R> normalize(vec3t<R> v) { return v / sqrt_r(dot(v, v)); }

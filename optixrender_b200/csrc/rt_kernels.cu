@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
 // throughput and pdf (thr), the shading normal and mesh of the hit (stale)
 // and the random state, which continues where k_shade left it.
 template <bool Stats>
-__global__ void __launch_bounds__(kBlock) k_sample(Ctx c) {
+__global__ void __launch_bounds__(kBlock, 4) k_sample(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
     const int nxt = (c.bounce & 1) ^ 1;
     const int bounce = c.bounce;

@@ -48,9 +48,8 @@ RT_D v3 uniform_sample_sphere(float s0, float s1) {  // Sampling.h:76-88
 template <class R>
 RT_D vec3t<R> cosine_sample_hemisphere(R s0, R s1) {  // Sampling.h:56-69
     R r = sqrt_r(s0);
-    R phi = Kc<R>::two_pi * s1;
     R sp, cp;
-    sincos_r(phi, &sp, &cp);
+    sincos_2pi_r(s1, &sp, &cp);
     vec3t<R> p(r * cp, r * sp, 0.0f);
     p.z = sqrt_r(fmax_r(0.0f, 1.0f - p.x * p.x - p.y * p.y));
     return normalize(p);
@@ -170,9 +169,9 @@ RT_D vec3t<R> sample_vndf(vec3t<R> N, vec3t<R> Ve, sc_t<R> au, sc_t<R> av, sc_t<
     R len2 = sqr(Vh.x) + sqr(Vh.y);
     vec3t<R> T1 = len2 > 0.0f ? vec3t<R>(-Vh.y, Vh.x, 0.0f) * sqrt_r(1.0f / len2) : vec3t<R>(1.0f, 0.0f, 0.0f);
     vec3t<R> T2 = cross(Vh, T1);
-    R r = sqrt_r(s0), phi = s1 * Kc<R>::two_pi;
+    R r = sqrt_r(s0);
     R sp, cp;
-    sincos_r(phi, &sp, &cp);
+    sincos_2pi_r(R(s1), &sp, &cp);
     R t1 = r * cp, t2 = r * sp;
     R s = 0.5f * (1.0f + Vh.z);
     t2 = (1.0f - s) * sqrt_r(1.0f - sqr(t1)) + s * t2;
