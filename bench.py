@@ -53,9 +53,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library's choice)")
-    p.add_argument("--ref-spp", type=int, default=16384,
+    p.add_argument("--ref-spp", type=int, default=None,
                    help="samples per pixel of the FP64-accumulated plain reference the frame's relMSE is measured "
-                        "against (0: no relMSE)")
+                        "against (0: no relMSE; default 65536 on one GPU, none on more, where every rank renders "
+                        "the same workload and the reference would hold all GPUs for two minutes)")
     return p.parse_args()
 
 
@@ -362,12 +363,13 @@ def main():
     # image error of the benchmarked frame (after every timed region): relMSE
     # against a plain render of ref_spp samples per pixel with independent
     # seeds, accumulated in FP64; the reference's own noise adds about
-    # spp / ref_spp of the value (0.4% at 64 / 16384)
+    # spp / ref_spp of the value (0.1% at 64 / 65536)
     quality = None
-    if args.ref_spp > 0 and rank == 0:
+    ref_spp_arg = args.ref_spp if args.ref_spp is not None else (65536 if world == 1 else 0)
+    if ref_spp_arg > 0 and rank == 0:
         from optixrender_b200.guide_bench import reference, relmse
         frame = r.download_linear()
-        ref_img, ref_spp, ref_ms = reference(spec, args.ref_spp)
+        ref_img, ref_spp, ref_ms = reference(spec, ref_spp_arg)
         quality = {"relmse": relmse(frame, ref_img), "reference_spp": ref_spp,
                    "reference": "plain render, frames of 256 spp with independent seeds accumulated in FP64",
                    "reference_device_ms": ref_ms}

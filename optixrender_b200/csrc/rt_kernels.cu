@@ -68,22 +68,10 @@ __global__ void k_begin(const JobDesc* __restrict__ jd) {
 }
 
 // ------------------------------------------------------------------ raygen
-__global__ void k_raygen(Ctx c) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    WaveCtl* ctl = c.wb.ctl;
-    const WaveParams& W = wave_of(c);
-    if (slot == 0) {
-        ctl->count[0] = W.wave_count;
-        ctl->count[1] = 0;
-        ctl->shadow_count = 0;
-        ctl->fetch_ext = 0;
-        ctl->fetch_shade = 0;
-        ctl->fetch_shadow = 0;
-        ctl->sample_count = 0;
-        ctl->fetch_sample = 0;
-        for (int b = 0; b < kShadeBuckets; b++) ctl->bucket[b] = 0;
-    }
-    if (slot >= W.wave_count) return;
+// The camera ray of the path in `slot` (devicePrograms.cu:178-180, 214-227): its slot
+// record goes to `rec`, its random state and queue entry to their arrays.
+RT_D void raygen_slot(const Ctx& c, const WaveParams& W, int slot, float4* rec) {
+    const WaveBufs& b = c.wb;
     const Segment sg = W.seg[find_segment(W, slot)];
     const JobDesc* jd = c.jobs + sg.job;
     const JobParams& j = jd->job;
@@ -105,19 +93,56 @@ __global__ void k_raygen(Ctx c) {
     float sx = (float(ix) + 0.5f + jx) / float(j.width);
     float sy = (float(iy) + 0.5f + jy) / float(j.height);
     v3 dir = normalize(ld3(cam.dir) + (sx - 0.5f) * ld3(cam.hor) + (sy - 0.5f) * ld3(cam.ver));
-    const WaveBufs& b = c.wb;
-    b.ray_o[slot] = f4(ld3(cam.pos), 0.0f);
-    b.ray_d[slot] = f4(dir, 0.0f);
-    b.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
-    b.rad[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    b.nee0[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    b.nee1[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    b.stale[slot] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    rec[kRecRayO / 16] = f4(ld3(cam.pos), 0.0f);
+    rec[kRecRayD / 16] = f4(dir, 0.0f);
+    rec[kRecHit / 16] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    rec[kRecThr / 16] = make_float4(1.f, 1.f, 1.f, 0.f);
+    rec[kRecRad / 16] = make_float4(0.f, 0.f, 0.f, 0.f);
+    rec[kRecNee0 / 16] = make_float4(0.f, 0.f, 0.f, 0.f);
+    rec[kRecNee1 / 16] = make_float4(0.f, 0.f, 0.f, 0.f);
+    rec[kRecStale / 16] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
     b.rng[slot] = make_uint2(uint32_t(rng.state), uint32_t(rng.state >> 32));
     b.queue[0][slot] = slot;
     if (c.G.rec != nullptr)
         for (int r = 0; r < rtg::kGuideRec; r++)
             c.G.rec[(size_t(r) * 4 + 1) * size_t(b.capacity) + slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+constexpr int kRaygenBlock = 256;
+constexpr int kRecF4 = int(kSlotRecord / 16);  // float4s per slot record
+constexpr int kStagePad = kRecF4 + 1;          // per staged record: the 16-byte stores of a warp hit distinct banks
+__global__ void __launch_bounds__(kRaygenBlock) k_raygen(Ctx c) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    WaveCtl* ctl = c.wb.ctl;
+    const WaveParams& W = wave_of(c);
+    if (slot == 0) {
+        ctl->count[0] = W.wave_count;
+        ctl->count[1] = 0;
+        ctl->shadow_count = 0;
+        ctl->fetch_ext = 0;
+        ctl->fetch_shade = 0;
+        ctl->fetch_shadow = 0;
+        ctl->sample_count = 0;
+        ctl->fetch_sample = 0;
+        for (int b = 0; b < kShadeBuckets; b++) ctl->bucket[b] = 0;
+    }
+    // A warp's 32 slot records are 4 KB of contiguous memory: they are built
+    // in shared memory and stored as 16-byte pieces by consecutive lanes, so
+    // that every store instruction writes whole lines.
+    __shared__ float4 stage[kRaygenBlock / 32][32 * kStagePad];
+    const int lane = threadIdx.x & 31;
+    const int slot0 = slot - lane;
+    if (slot0 >= W.wave_count) return;  // the whole warp
+    float4* st = stage[threadIdx.x >> 5];
+    if (slot < W.wave_count) raygen_slot(c, W, slot, st + lane * kStagePad);
+    __syncwarp();
+    float4* dst = reinterpret_cast<float4*>(c.wb.ray_o.base - kRecRayO) + size_t(slot0) * kRecF4;
+#pragma unroll
+    for (int k = 0; k < kRecF4; k++) {
+        const int idx = k * 32 + lane;  // float4 index in the warp's records
+        const int r = idx / kRecF4;
+        if (slot0 + r < W.wave_count) dst[idx] = st[r * kStagePad + idx % kRecF4];
+    }
 }
 
 // ------------------------------------------------------------------ extend
@@ -1178,7 +1203,7 @@ static unsigned grid_for(int64_t n, int block) { return unsigned((n + block - 1)
 void launch_begin(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_begin<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
 }
-void launch_raygen(const Ctx& c, cudaStream_t st) { k_raygen<<<grid_for(c.wb.capacity, 256), 256, 0, st>>>(c); }
+void launch_raygen(const Ctx& c, cudaStream_t st) { k_raygen<<<grid_for(c.wb.capacity, kRaygenBlock), kRaygenBlock, 0, st>>>(c); }
 void launch_extend(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
     if (stats)
         k_extend<true><<<s.blocks_extend, kBlock, 0, st>>>(c);

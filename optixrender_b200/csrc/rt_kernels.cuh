@@ -66,15 +66,30 @@ struct WaveCtl {
 };
 
 // Structure-of-arrays path state, one entry per slot of a wave.
+// A slot's eight float4 fields of path state lie together in one 128-byte
+// record (one cache line), so that the shade and sample kernels, which touch
+// most of a slot's state, read one line per slot instead of eight lines of
+// eight arrays; the slots are visited in the scattered order of the material
+// sort.  A field is the record array at the field's byte offset.
+constexpr size_t kSlotRecord = 128;
+enum SlotOffset : size_t {
+    kRecRayO = 0, kRecRayD = 16, kRecHit = 32, kRecThr = 48, kRecRad = 64, kRecNee0 = 80, kRecNee1 = 96, kRecStale = 112
+};
+struct SlotField {
+    char* base;  // record array + the field's offset
+    RT_HD float4& operator[](size_t slot) const { return *reinterpret_cast<float4*>(base + slot * kSlotRecord); }
+};
+RT_HD SlotField slot_field(void* records, SlotOffset off) { return SlotField{static_cast<char*>(records) + off}; }
+
 struct WaveBufs {
-    float4* ray_o;   // origin
-    float4* ray_d;   // direction
-    float4* hit;     // t, b1, b2, triangle (bits; -1 = miss)
-    float4* thr;     // throughput (history), pre_pdf
-    float4* rad;     // radiance
-    float4* nee0;    // pending environment NEE contribution
-    float4* nee1;    // pending light NEE contribution
-    float4* stale;   // shading normal and mesh of the last hit
+    SlotField ray_o;   // origin
+    SlotField ray_d;   // direction
+    SlotField hit;     // t, b1, b2, triangle (bits; -1 = miss)
+    SlotField thr;     // throughput (history), pre_pdf
+    SlotField rad;     // radiance
+    SlotField nee0;    // pending environment NEE contribution
+    SlotField nee1;    // pending light NEE contribution
+    SlotField stale;   // shading normal and mesh of the last hit
     float4* aov_a;   // albedo, normal.x
     float2* aov_n;   // normal.y, normal.z
     uint2* rng;      // random state

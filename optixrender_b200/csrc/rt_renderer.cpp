@@ -223,7 +223,7 @@ struct rt_renderer {
     int pw = 0, ph = 0;
     DevBuf acc_color, acc_albedo, acc_normal, lcg_state, color, albedo, normal, rgba8;
     int capacity = 0;
-    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sq, sh_o, sh_d, ctl, segs, job;
+    DevBuf slots, aov_a, aov_n, rng, q0, q1, sq, sh_o, sh_d, ctl, segs, job;  // slots: kSlotRecord bytes per slot
     DevBuf sorted;            // shade queue by material type
     DevBuf dn_tmp0, dn_tmp1, dn_out;  // denoiser scratch and output (rt_options.denoise)
     int dn_pixels = 0;                // pixels covered by the denoiser buffers
@@ -297,8 +297,8 @@ rt_status ensure_denoiser(rt_renderer* r) {
 rt_status ensure_waves(rt_renderer* r, int cap) {
     if (cap <= r->capacity) return RT_OK;
     size_t n = size_t(cap);
-    DevBuf* f4s[] = {&r->ray_o, &r->ray_d, &r->hit, &r->thr, &r->rad, &r->nee0, &r->nee1, &r->stale, &r->aov_a};
-    for (DevBuf* b : f4s) RT_CUDA(b->alloc(n * sizeof(float4)), "allocate path state");
+    RT_CUDA(r->slots.alloc(n * kSlotRecord), "allocate path state");
+    RT_CUDA(r->aov_a.alloc(n * sizeof(float4)), "allocate path state");
     RT_CUDA(r->aov_n.alloc(n * sizeof(float2)), "allocate path state");
     RT_CUDA(r->rng.alloc(n * sizeof(uint2)), "allocate path state");
     RT_CUDA(r->q0.alloc(n * sizeof(int)), "allocate queues");
@@ -314,14 +314,14 @@ rt_status ensure_waves(rt_renderer* r, int cap) {
 
 // The renderer's per-slot path state as the kernels see it.
 void wave_bufs(rt_renderer* r, WaveBufs& b) {
-    b.ray_o = r->ray_o.as<float4>();
-    b.ray_d = r->ray_d.as<float4>();
-    b.hit = r->hit.as<float4>();
-    b.thr = r->thr.as<float4>();
-    b.rad = r->rad.as<float4>();
-    b.nee0 = r->nee0.as<float4>();
-    b.nee1 = r->nee1.as<float4>();
-    b.stale = r->stale.as<float4>();
+    b.ray_o = slot_field(r->slots.ptr, kRecRayO);
+    b.ray_d = slot_field(r->slots.ptr, kRecRayD);
+    b.hit = slot_field(r->slots.ptr, kRecHit);
+    b.thr = slot_field(r->slots.ptr, kRecThr);
+    b.rad = slot_field(r->slots.ptr, kRecRad);
+    b.nee0 = slot_field(r->slots.ptr, kRecNee0);
+    b.nee1 = slot_field(r->slots.ptr, kRecNee1);
+    b.stale = slot_field(r->slots.ptr, kRecStale);
     b.aov_a = r->aov_a.as<float4>();
     b.aov_n = r->aov_n.as<float2>();
     b.rng = r->rng.as<uint2>();

@@ -115,7 +115,7 @@ struct rt_server {
     int64_t bytes_in_use = 0;
     // device state
     DevBuf job_table, ring, wave_index, ctl;
-    DevBuf ray_o, ray_d, hit, thr, rad, nee0, nee1, stale, aov_a, aov_n, rng, q0, q1, sq, sh_o, sh_d, sorted;
+    DevBuf slots, aov_a, aov_n, rng, q0, q1, sq, sh_o, sh_d, sorted;  // slots: kSlotRecord bytes per slot
     DevBuf mat_tex;  // per-slot textured materials, once a scene with textures is resident
     // guiding: per-slot mixtures, training records and samples, one batch
     DevBuf g_mix, g_rec, g_buf, g_count, g_wsum, g_bpos, g_bdir, g_bw;
@@ -180,8 +180,8 @@ rt_status setup(rt_server* s) {
         s->ring_timed.push_back(0);
     }
     const size_t cap = size_t(s->opt.wave_paths);
-    DevBuf* f4s[] = {&s->ray_o, &s->ray_d, &s->hit, &s->thr, &s->rad, &s->nee0, &s->nee1, &s->stale, &s->aov_a};
-    for (DevBuf* b : f4s) SV_CUDA(b->alloc(cap * sizeof(float4)), "allocate path state");
+    SV_CUDA(s->slots.alloc(cap * kSlotRecord), "allocate path state");
+    SV_CUDA(s->aov_a.alloc(cap * sizeof(float4)), "allocate path state");
     SV_CUDA(s->aov_n.alloc(cap * sizeof(float2)), "allocate path state");
     SV_CUDA(s->rng.alloc(cap * sizeof(uint2)), "allocate path state");
     SV_CUDA(s->q0.alloc(cap * sizeof(int)), "allocate queues");
@@ -249,14 +249,14 @@ Ctx make_ctx(rt_server* s, int group) {
     std::memset(&c, 0, sizeof(c));
     c.jobs = s->job_table.as<JobDesc>();
     WaveBufs& b = c.wb;
-    b.ray_o = s->ray_o.as<float4>();
-    b.ray_d = s->ray_d.as<float4>();
-    b.hit = s->hit.as<float4>();
-    b.thr = s->thr.as<float4>();
-    b.rad = s->rad.as<float4>();
-    b.nee0 = s->nee0.as<float4>();
-    b.nee1 = s->nee1.as<float4>();
-    b.stale = s->stale.as<float4>();
+    b.ray_o = slot_field(s->slots.ptr, kRecRayO);
+    b.ray_d = slot_field(s->slots.ptr, kRecRayD);
+    b.hit = slot_field(s->slots.ptr, kRecHit);
+    b.thr = slot_field(s->slots.ptr, kRecThr);
+    b.rad = slot_field(s->slots.ptr, kRecRad);
+    b.nee0 = slot_field(s->slots.ptr, kRecNee0);
+    b.nee1 = slot_field(s->slots.ptr, kRecNee1);
+    b.stale = slot_field(s->slots.ptr, kRecStale);
     b.aov_a = s->aov_a.as<float4>();
     b.aov_n = s->aov_n.as<float2>();
     b.rng = s->rng.as<uint2>();
