@@ -114,8 +114,22 @@ def test_spheres_same_streams_small():
     agree = pixel_agreement(gpu, cpu)
     mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
     print(f"spheres: agreeing {agree:.4f} means {mg:.5f} / {mc:.5f}")
-    assert agree >= 0.95
-    assert abs(mg - mc) <= 2e-2 * abs(mc)
+    assert agree >= 0.97
+    assert abs(mg - mc) <= 1e-3 * abs(mc)
+
+
+@pytest.mark.gpu
+def test_c1_full_resolution_same_streams():
+    """The benchmark configuration itself at 4 spp: 1920x1080, depth 16, the
+    2.59M-triangle scene with its 2048x1024 sky (the spp is what the
+    oracle's time bounds: about 5 s on 8 host threads)."""
+    spec = scenes.spheres(1920, 1080, 4)
+    r, gpu, cpu, alb, nrm = render_both(spec)
+    agree = pixel_agreement(gpu, cpu)
+    mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
+    print(f"C1 full resolution: agreeing {agree:.5f} means {mg:.5f} / {mc:.5f}")
+    assert agree >= 0.97
+    assert abs(mg - mc) <= 1e-3 * abs(mc)
 
 
 @pytest.mark.gpu
@@ -142,8 +156,8 @@ def test_media_scene_same_streams():
     agree = pixel_agreement(gpu, cpu)
     mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
     print(f"media: agreeing {agree:.4f} means {mg:.5f} / {mc:.5f}")
-    assert agree >= 0.90
-    assert abs(mg - mc) <= 2e-2 * abs(mc)
+    assert agree >= 0.97
+    assert abs(mg - mc) <= 1e-3 * abs(mc)
 
 
 @pytest.mark.gpu
@@ -225,8 +239,8 @@ def test_c2_media_full_grid_same_streams():
     agree = pixel_agreement(gpu, cpu)
     mg, mc = gpu[..., :3].mean(), cpu[..., :3].mean()
     print(f"C2 full grid: agreeing {agree:.4f} means {mg:.5f} / {mc:.5f}")
-    assert agree >= 0.90
-    assert abs(mg - mc) <= 2e-2 * abs(mc)
+    assert agree >= 0.97
+    assert abs(mg - mc) <= 1e-3 * abs(mc)
     r.synchronize()  # no walk ran out of its step budget
 
 
