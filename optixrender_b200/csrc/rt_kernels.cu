@@ -186,7 +186,6 @@ __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_extend(Ctx c) {
     const int cur = c.bounce & 1, nxt = cur ^ 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->count[nxt] = 0;
-        ctl->shadow_count = 0;
         ctl->fetch_shade = 0;
         ctl->sample_count = 0;
         ctl->fetch_sample = 0;
@@ -668,6 +667,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_sample(Ctx c) {
     const int nxt = (c.bounce & 1) ^ 1;
     const int bounce = c.bounce;
     const int total = ctl->sample_count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // k_shade is done with these: this bounce's shadow queue length moves
+        // to shadow_total for k_shadow, and the counters the next k_extend and
+        // k_shade append to start from zero here, so that k_shadow and the next
+        // k_extend share no counter and may run side by side
+        ctl->shadow_total = ctl->shadow_count;
+        ctl->shadow_count = 0;
+        for (int b = 0; b < kShadeBuckets; b++) ctl->bucket[b] = 0;
+    }
     const WaveBufs& B = c.wb;
     const WaveParams& W = wave_of(c);
     const int lane = threadIdx.x & 31;
@@ -759,8 +767,7 @@ struct ShadowSrc {
 template <bool Stats>
 __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_shadow(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
-    if (blockIdx.x == 0 && threadIdx.x < kShadeBuckets) ctl->bucket[threadIdx.x] = 0;  // for the next extend
-    const int total = ctl->shadow_count;
+    const int total = ctl->shadow_total;
     uint32_t nodes = 0, tris = 0, rays = 0, overflows = 0;
     ShadowSrc src{&c};
     traverse_queue<true, Stats>(src, &ctl->fetch_shadow, total, nodes, tris, rays, overflows);
@@ -1032,7 +1039,8 @@ __global__ void k_query_stage(Ctx c, const float4* __restrict__ rays, int n, int
     if (i == 0) {
         ctl->count[0] = any_hit ? 0 : n;
         ctl->count[1] = 0;
-        ctl->shadow_count = any_hit ? n : 0;
+        ctl->shadow_count = 0;
+        ctl->shadow_total = any_hit ? n : 0;
         ctl->fetch_ext = 0;
         ctl->fetch_shade = 0;
         ctl->fetch_shadow = 0;
@@ -1203,6 +1211,38 @@ static unsigned grid_for(int64_t n, int block) { return unsigned((n + block - 1)
 void launch_begin(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_begin<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
 }
+void launch_shadow_and_next_extend(Ctx c, const LaunchShape& s, cudaStream_t st, const WaveFork* f) {
+    if (f == nullptr) {
+        launch_shadow(c, s, false, st);
+        c.bounce += 1;
+        launch_extend(c, s, false, st);
+        return;
+    }
+    cudaEventRecord(f->fork, st);
+    cudaStreamWaitEvent(f->side, f->fork, 0);
+    launch_shadow(c, s, false, f->side);
+    cudaEventRecord(f->join, f->side);
+    c.bounce += 1;
+    launch_extend(c, s, false, st);
+    cudaStreamWaitEvent(st, f->join, 0);
+}
+
+cudaError_t create_fork(WaveFork& f) {
+    f = WaveFork{};
+    cudaError_t e = cudaStreamCreateWithFlags(&f.side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming);
+    if (e != cudaSuccess) destroy_fork(f);
+    return e;
+}
+
+void destroy_fork(WaveFork& f) {
+    if (f.side) cudaStreamDestroy(f.side);
+    if (f.fork) cudaEventDestroy(f.fork);
+    if (f.join) cudaEventDestroy(f.join);
+    f = WaveFork{};
+}
+
 void launch_raygen(const Ctx& c, cudaStream_t st) { k_raygen<<<grid_for(c.wb.capacity, kRaygenBlock), kRaygenBlock, 0, st>>>(c); }
 void launch_extend(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st) {
     if (stats)

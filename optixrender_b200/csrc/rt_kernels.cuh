@@ -62,11 +62,10 @@ struct WaveCtl {
     int bucket[kShadeBuckets];    // extend results per shade bucket
     int sample_count;             // paths k_shade left at BSDF sampling (k_sample's queue)
     int fetch_sample;
-    int pad2;
+    int shadow_total;             // length of this bounce's shadow queue, taken by k_sample from shadow_count
 };
 
-// Structure-of-arrays path state, one entry per slot of a wave.
-// A slot's eight float4 fields of path state lie together in one 128-byte
+// Per-slot path state of a wave.  A slot's eight float4 fields of path state lie together in one 128-byte
 // record (one cache line), so that the shade and sample kernels, which touch
 // most of a slot's state, read one line per slot instead of eight lines of
 // eight arrays; the slots are visited in the scattered order of the material
@@ -176,6 +175,25 @@ void launch_shade(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStrea
 // BSDF sampling of the paths k_shade left at a surface (runs between shade and shadow).
 void launch_sample(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
 void launch_shadow(const rtd::Ctx& c, const LaunchShape& s, bool stats, cudaStream_t st);
+// A second stream and two events (created with cudaEventDisableTiming) for
+// the two branches of a wave below.
+struct WaveFork {
+    cudaStream_t side;
+    cudaEvent_t fork, join;
+};
+// The shadow rays of bounce c.bounce and the closest hits of the next bounce
+// share no data: k_shadow reads the shadow queue and its length
+// (shadow_total) and clears the NEE fields of occluded slots; k_extend reads
+// the path queue and writes the hit fields, the shade buckets and the
+// counters of the next k_shade and k_sample; the counters either used to
+// reset for the other (shadow_count, the buckets) are reset by k_sample
+// before both.  So with `f` k_shadow runs on f->side as a parallel branch of
+// the stream (or of the wave's graph when capturing), joined back before the
+// next k_shade, and the tail of one kernel overlaps the other.  Without `f`
+// the two run one after the other on `st`.
+void launch_shadow_and_next_extend(rtd::Ctx c, const LaunchShape& s, cudaStream_t st, const WaveFork* f);
+cudaError_t create_fork(WaveFork& f);  // on the current device; on failure nothing stays allocated
+void destroy_fork(WaveFork& f);
 void launch_resolve(const rtd::Ctx& c, cudaStream_t st);
 void launch_next_wave(const rtd::Ctx& c, cudaStream_t st);
 void launch_finalize(const rtd::JobDesc& host_job, const rtd::JobDesc* dev_job, cudaStream_t st);

@@ -216,6 +216,8 @@ struct rt_renderer {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    rth::WaveFork fork{};  // side stream and events: k_shadow beside the next k_extend
+    bool have_fork = false;
     DeviceScene ds;
     rt_options opt{};
     rt_camera cam{};
@@ -425,10 +427,13 @@ rt_status rt_renderer_create(const rt_scene* s, const rt_options* opts, rt_rende
     if (!r) return fail(RT_ERR_OUT_OF_MEMORY, "rt_renderer_create: out of host memory");
     cudaError_t e = cudaGetDevice(&r->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = rth::create_fork(r->fork);
     if (e != cudaSuccess) {
+        if (r->stream) cudaStreamDestroy(r->stream);
         delete r;
         return cuda_fail(e, "rt_renderer_create");
     }
+    r->have_fork = true;
     r->own_stream = true;
     r->opt = o;
     if (const char* v = std::getenv("RT_SORT_SHADE")) r->sort_shade = std::atoi(v) != 0;
@@ -467,6 +472,8 @@ rt_status rt_renderer_destroy(rt_renderer* r) {
     if (r->guide) rt_guide_destroy(r->guide);
     if (r->ev0) cudaEventDestroy(r->ev0);
     if (r->ev1) cudaEventDestroy(r->ev1);
+    if (r->fork.side) cudaStreamSynchronize(r->fork.side);
+    rth::destroy_fork(r->fork);
     if (r->own_stream && r->stream) cudaStreamDestroy(r->stream);
     delete r;
     return RT_OK;
@@ -639,24 +646,36 @@ rt_status rt_renderer_render(rt_renderer* r) {
         if (training) cudaMemsetAsync(r->g_count.ptr, 0, sizeof(int), s);
         c.bounce = 0;
         rth::launch_raygen(c, s);
-        for (int bnc = 0; bnc < o.max_depth; bnc++) {
-            c.bounce = bnc;
-            size_t i0 = r->timer.used;
-            if (timed) cudaEventRecord(r->timer.next(), s);
-            rth::launch_extend(c, r->shape, timed, s);
-            if (timed) cudaEventRecord(r->timer.next(), s);
-            if (guided) rtgh::launch_infer(c, net, gsms, s);
-            rth::launch_shade(c, r->shape, timed, s);
-            if (timed) cudaEventRecord(r->timer.next(), s);
-            rth::launch_sample(c, r->shape, timed, s);
-            if (timed) cudaEventRecord(r->timer.next(), s);
-            rth::launch_shadow(c, r->shape, timed, s);
-            if (timed) {
+        if (timed) {  // one kernel after the other, each between two timing events
+            for (int bnc = 0; bnc < o.max_depth; bnc++) {
+                c.bounce = bnc;
+                size_t i0 = r->timer.used;
+                cudaEventRecord(r->timer.next(), s);
+                rth::launch_extend(c, r->shape, true, s);
+                cudaEventRecord(r->timer.next(), s);
+                if (guided) rtgh::launch_infer(c, net, gsms, s);
+                rth::launch_shade(c, r->shape, true, s);
+                cudaEventRecord(r->timer.next(), s);
+                rth::launch_sample(c, r->shape, true, s);
+                cudaEventRecord(r->timer.next(), s);
+                rth::launch_shadow(c, r->shape, true, s);
                 cudaEventRecord(r->timer.next(), s);
                 r->timer.marks.push_back({0, i0});
                 r->timer.marks.push_back({1, i0 + 1});
                 r->timer.marks.push_back({3, i0 + 2});
                 r->timer.marks.push_back({2, i0 + 3});
+            }
+        } else {  // a bounce's k_shadow beside the next bounce's k_extend
+            rth::launch_extend(c, r->shape, false, s);
+            for (int bnc = 0; bnc < o.max_depth; bnc++) {
+                c.bounce = bnc;
+                if (guided) rtgh::launch_infer(c, net, gsms, s);
+                rth::launch_shade(c, r->shape, false, s);
+                rth::launch_sample(c, r->shape, false, s);
+                if (bnc + 1 < o.max_depth)
+                    rth::launch_shadow_and_next_extend(c, r->shape, s, r->have_fork ? &r->fork : nullptr);
+                else
+                    rth::launch_shadow(c, r->shape, false, s);
             }
         }
         rth::launch_resolve(c, s);

@@ -99,6 +99,7 @@ struct rt_server {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t dl_stream = nullptr;  // downloads of finished images
+    rth::WaveFork fork{};              // side stream and events: k_shadow beside the next k_extend
     cudaMemPool_t pool = nullptr;      // job buffers, stream-ordered on `stream`
     JobDesc* host_jobs = nullptr;      // pinned staging of the job table
     std::chrono::steady_clock::time_point t0;
@@ -152,6 +153,7 @@ rt_status setup(rt_server* s) {
     SV_CUDA(cudaGetDevice(&s->device), "rt_server_create");
     SV_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "rt_server_create");
     SV_CUDA(cudaStreamCreateWithFlags(&s->dl_stream, cudaStreamNonBlocking), "rt_server_create");
+    SV_CUDA(rth::create_fork(s->fork), "rt_server_create");
     cudaMemPoolProps pp;
     std::memset(&pp, 0, sizeof(pp));
     pp.allocType = cudaMemAllocationTypePinned;
@@ -301,13 +303,16 @@ void issue_wave(rt_server* s, const Ctx& c0, int depth, int gscene, bool trainin
     if (training) cudaMemsetAsync(s->g_count.ptr, 0, sizeof(int), s->stream);
     c.bounce = 0;
     rth::launch_raygen(c, s->stream);
+    rth::launch_extend(c, s->shape, false, s->stream);
     for (int b = 0; b < depth; b++) {
         c.bounce = b;
-        rth::launch_extend(c, s->shape, false, s->stream);
         if (gscene >= 0) rtgh::launch_infer(c, net, gsms, s->stream);
         rth::launch_shade(c, s->shape, false, s->stream);
         rth::launch_sample(c, s->shape, false, s->stream);
-        rth::launch_shadow(c, s->shape, false, s->stream);
+        if (b + 1 < depth)  // this bounce's k_shadow beside the next bounce's k_extend
+            rth::launch_shadow_and_next_extend(c, s->shape, s->stream, &s->fork);
+        else
+            rth::launch_shadow(c, s->shape, false, s->stream);
     }
     rth::launch_resolve(c, s->stream);
     if (training)
@@ -678,6 +683,8 @@ rt_status rt_server_destroy(rt_server* s) {
     for (cudaEvent_t e : s->ring_start) cudaEventDestroy(e);
     if (s->host_ring) cudaFreeHost(s->host_ring);
     if (s->host_jobs) cudaFreeHost(s->host_jobs);
+    if (s->fork.side) cudaStreamSynchronize(s->fork.side);
+    rth::destroy_fork(s->fork);
     if (s->dl_stream) cudaStreamDestroy(s->dl_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
