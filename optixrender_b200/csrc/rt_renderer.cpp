@@ -338,21 +338,27 @@ void wave_bufs(rt_renderer* r, WaveBufs& b) {
     b.capacity = r->capacity;
 }
 
-int auto_capacity(const rt_options& o, int64_t npix, int64_t total) {
+int auto_capacity(const rt_options& o, int64_t npix, int64_t total, int64_t allocated) {
     // Large waves: the last bounces of a wave carry few paths and run at the
     // latency of a handful of rays, so fewer, larger waves spend less time
     // there.  Automatic: up to 2^26 slots (272 B each, 18 GB), at most a
-    // quarter of the free device memory.
+    // quarter of the free device memory.  The free memory is asked for only
+    // when the renderer's wave buffers (`allocated` slots) are too small for
+    // the frame: the query goes to the driver and, on a busy host, took tens
+    // of milliseconds, which a Render() that only launches work must not spend.
     int64_t cap = o.wave_paths > 0 ? int64_t(o.wave_paths) : std::max<int64_t>(npix, int64_t(1) << 26);
-    if (o.wave_paths <= 0) {
+    auto clamp = [&](int64_t c) {
+        c = std::min<int64_t>(c, int64_t(1) << 26);
+        if (o.rng == RT_RNG_LCG) c = std::min<int64_t>(c, npix);
+        return std::max<int64_t>(std::min<int64_t>(c, total), 1);
+    };
+    if (o.wave_paths <= 0 && clamp(cap) > allocated) {
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
-            cap = std::min<int64_t>(cap, std::max<int64_t>(int64_t(1) << 20, int64_t(fr / 4) / 400));
+            cap = std::min<int64_t>(cap, std::max<int64_t>(std::max<int64_t>(int64_t(1) << 20, allocated),
+                                                           int64_t(fr / 4) / 400));
     }
-    cap = std::min<int64_t>(cap, int64_t(1) << 26);
-    if (o.rng == RT_RNG_LCG) cap = std::min<int64_t>(cap, npix);
-    cap = std::min<int64_t>(cap, total);
-    return int(std::max<int64_t>(cap, 1));
+    return int(clamp(cap));
 }
 
 // Guiding network and its per-slot buffers: mixtures for `cap` slots, and
@@ -542,7 +548,7 @@ rt_status rt_renderer_render(rt_renderer* r) {
     const int64_t npix = int64_t(o.width) * o.height;
     const int64_t total = npix * o.spp;
     const bool guided = o.guided != 0;
-    int cap = auto_capacity(o, npix, total);
+    int cap = auto_capacity(o, npix, total, r->capacity);
     if (guided) cap = std::min(cap, kGuidedWaveMax);
     // guided: the first training samples run one sample per pixel per wave
     const int64_t train_waves =

@@ -87,6 +87,9 @@ RT_D float u8f15(uint32_t w, int byte) {
     return __uint_as_float(__byte_perm(w, 0x47000000u, sel));
 }
 
+// Byte `byte` of w, zero-extended.
+RT_D uint32_t byte_of(uint32_t w, int byte) { return __byte_perm(w, 0u, 0x4440u | uint32_t(byte)); }
+
 // Three-input minimum / maximum (PTX ISA 8.8, sm_100).
 RT_D float max3f(float a, float b, float c) {
     float d;
@@ -132,36 +135,37 @@ RT_D uint32_t intersect_children(const CwNode* nodes, uint32_t idx, const TravRa
     const float cx = fmaf(-32768.0f, sx, ox), cy = fmaf(-32768.0f, sy, oy), cz = fmaf(-32768.0f, sz, oz);
     const float wx = fabsf(sx) * (1.0f / 128.0f), wy = fabsf(sy) * (1.0f / 128.0f), wz = fabsf(sz) * (1.0f / 128.0f);
     const float cxn = cx - wx, cxf = cx + wx, cyn = cy - wy, cyf = cy + wy, czn = cz - wz, czf = cz + wz;
-    uint32_t node_bits = 0, tbits = 0;
+    uint32_t hits = 0;
 #pragma unroll
     for (int half = 0; half < 2; half++) {
-        uint32_t mlo = half == 0 ? meta_lo : meta_hi;
+        // A child's meta byte is (bits << 5) | index: an internal child has
+        // bits 1 and index 24 + slot, a leaf child its triangles' unary mask
+        // and the bit of its first triangle (< 24), an empty slot 0.  Internal
+        // children (index >= 24: bits 3 and 4 set, which no leaf index has)
+        // get the ray octant XORed into the slot, so bits 24..31 of the hit
+        // mask come out in near-to-far order.  Four children per 32-bit word.
+        const uint32_t m = half == 0 ? meta_lo : meta_hi;
+        const uint32_t inner = m & (m << 1) & 0x10101010u;
+        const uint32_t idx4 = (m ^ ((inner >> 4) * r.oct)) & 0x1F1F1F1Fu;
+        const uint32_t bits4 = (m >> 5) & 0x07070707u;
         uint32_t xn = nx ? lox[half] : hix[half], xf = nx ? hix[half] : lox[half];
         uint32_t yn = ny ? loy[half] : hiy[half], yf = ny ? hiy[half] : loy[half];
         uint32_t zn = nz ? loz[half] : hiz[half], zf = nz ? hiz[half] : loz[half];
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-            uint32_t meta = (mlo >> (8 * b)) & 0xFFu;
             float tx0 = fmaf(u8f15(xn, b), sx, cxn), tx1 = fmaf(u8f15(xf, b), sx, cxf);
             float ty0 = fmaf(u8f15(yn, b), sy, cyn), ty1 = fmaf(u8f15(yf, b), sy, cyf);
             float tz0 = fmaf(u8f15(zn, b), sz, czn), tz1 = fmaf(u8f15(zf, b), sz, czf);
             float tn = max3f(tx0, ty0, fmaxf(tz0, r.tmin));
             float tf = min3f(tx1, ty1, fminf(tz1, tmax));
             // conservative: the far distance is widened by 1.6e-6 relative
-            // (tn >= tmin >= 0), covering the rounding of the slab distances
-            bool hit = meta != 0u && tn <= tf * 1.0000016f;
-            if (hit) {
-                const int slot = half * 4 + b;
-                if ((imask >> slot) & 1u) {
-                    node_bits |= 1u << (24 + (uint32_t(slot) ^ r.oct));
-                } else {
-                    tbits |= (meta >> 5) << (meta & 31u);
-                }
-            }
+            // (tn >= tmin >= 0), covering the rounding of the slab distances;
+            // an empty slot adds no bits whatever its planes
+            if (tn <= tf * 1.0000016f) hits |= byte_of(bits4, b) << byte_of(idx4, b);
         }
     }
-    tri_bits = tbits;
-    return node_bits | imask;
+    tri_bits = hits & 0x00FFFFFFu;
+    return (hits & 0xFF000000u) | imask;
 }
 
 // Returns the index of the closest hit triangle (or -1) in [tmin, tmax).
