@@ -140,7 +140,7 @@ RT_D void pack_masked(const float (&d)[N / 8][4], uint32_t mask, uint32_t (&a)[N
 // need: output delta (2 x 4 words), then the input and delta of each hidden
 // layer, then the encoded input.  Word w of lane l sits at
 // [w / 4][l][w % 4], so one A fragment (4 words) is one 16-byte store or
-// load per lane and 512 contiguous bytes per warp.  k_guide_wgrad forms
+// load per lane and 512 contiguous bytes per warp.  k_guide_wgrad_tc forms
 // dW_l = E^T X from them.
 constexpr int kFragAdo = 0, kFragH3 = 8, kFragE3 = 24, kFragH2 = 40, kFragE2 = 56, kFragH1 = 72, kFragE1 = 88,
               kFragAx = 104, kFragWords = 112;
@@ -490,57 +490,6 @@ __global__ void __launch_bounds__(kBwdWarps * 32, 2) k_guide_backward(NetView ne
     if (lane == 0 && lsum != 0.f) atomicAdd(loss, lsum);
 }
 
-// Weight gradients dW_l[M][N] += E^T X from the fragments of `tiles` tiles.
-// Warp w of a block plays role w: a 16-row block of one layer's outputs
-// (layer 3: 2 blocks, layers 2, 1, 0: 4 each), whose 16 x N gradient stays in
-// registers across the block's chunk of tiles and is added to global memory
-// once.  The 14 warps of a block read the same tiles, so those loads hit L1.
-constexpr int kWgradRoles = 14;
-template <int M, int N>
-RT_D void wgrad_role(const uint32_t* __restrict__ frags, int t0, int t1, int offE, int offX, int mt, float* gW) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-    float acc[N / 8][4];
-#pragma unroll
-    for (int j = 0; j < N / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
-    for (int tt = t0; tt < t1; tt++) {
-        const uint32_t* tf = frags + size_t(tt) * kFragWords * 32;
-        uint32_t x[N / 16][4];
-#pragma unroll
-        for (int t = 0; t < N / 16; t++) frag_load(tf, offX + 4 * t, lane, x[t]);
-        uint32_t e4[4];
-        frag_load(tf, offE + 4 * mt, lane, e4);
-        const uint32_t at[4] = {trans8x8(e4[0]), trans8x8(e4[2]), trans8x8(e4[1]), trans8x8(e4[3])};
-#pragma unroll
-        for (int j = 0; j < N / 8; j++) {
-            const int t = j >> 1, hi = j & 1;
-            mma16816(acc[j], at, trans8x8(x[t][hi ? 2 : 0]), trans8x8(x[t][hi ? 3 : 1]));
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < N / 8; j++) {
-        float* p = gW + (16 * mt + g) * N + 8 * j + 2 * tig;
-        if (acc[j][0] != 0.f) atomicAdd(p, acc[j][0]);
-        if (acc[j][1] != 0.f) atomicAdd(p + 1, acc[j][1]);
-        if (acc[j][2] != 0.f) atomicAdd(p + 8 * N, acc[j][2]);
-        if (acc[j][3] != 0.f) atomicAdd(p + 8 * N + 1, acc[j][3]);
-    }
-}
-
-__global__ void __launch_bounds__(kWgradRoles * 32, 2) k_guide_wgrad(const uint32_t* __restrict__ frags, int tiles,
-                                                                  int chunk, float* __restrict__ grad_mlp) {
-    const int role = threadIdx.x >> 5;
-    const int t0 = blockIdx.x * chunk, t1 = min(tiles, t0 + chunk);
-    if (t0 >= t1) return;
-    if (role < 2)
-        wgrad_role<kOut, kHid>(frags, t0, t1, kFragAdo, kFragH3, role, grad_mlp + kW0 + kW1 + kW2);
-    else if (role < 6)
-        wgrad_role<kHid, kHid>(frags, t0, t1, kFragE3, kFragH2, role - 2, grad_mlp + kW0 + kW1);
-    else if (role < 10)
-        wgrad_role<kHid, kHid>(frags, t0, t1, kFragE2, kFragH1, role - 6, grad_mlp + kW0);
-    else
-        wgrad_role<kHid, kIn>(frags, t0, t1, kFragE1, kFragAx, role - 10, grad_mlp);
-}
-
 // ------------------------------------------------------------------ renderer side
 // Items of the sorted shade queue whose material type is guided, in bucket order.
 struct GuidedItems {
@@ -775,6 +724,199 @@ RT_D void tc_teardown(uint32_t tmem, bool ok) {
     tc_fence_after();
     if (threadIdx.x < 32)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols) : "memory");
+    if (!ok && threadIdx.x == 0) atomicAdd(&g_tc_timeouts, 1);
+}
+
+// ----------------------------------------------------------- weight gradients
+// dW_l = E_l^T X_l, summed over the samples of a training pass, on the
+// tensor cores.  For layer l, E_l holds the output deltas and X_l the inputs
+// of every sample (k_guide_backward stores both per 16-sample tile as mma
+// fragments: word r of lane 4g + t of a 16-unit block is units 8(r >> 1) +
+// 2t, +1 of sample g + 8(r & 1); a tile is 28 such blocks, "pieces").  One
+// CTA of 16 warps per SM takes four tiles (64 samples, a chunk) at a time,
+// in a pipeline over two staging buffers and two operand buffers:
+//   * chunk c + 2 is copied to shared memory with cp.async while chunk c is
+//     transposed (56 KB per SM always in flight from HBM);
+//   * warp w transposes 7 pieces of tile w & 3 (w >> 2 chooses which), each
+//     8x8 block with movmatrix (lane 4g + t then holds unit g, samples 2t and
+//     2t + 1) and one 32-bit store into the K-major canonical operands of
+//     chunk c's buffer (K = the chunk's 64 samples):
+//       A_l = E_l^T, the layer's 32 or 64 output units as rows;
+//       B_l = X_l^T, the layer's 64 (or 32) input units as rows;
+//   * one thread issues, per layer, four tcgen05.mma.kind::f16 (M = 128,
+//     N = 64 or 32, K = 16) accumulating into the layer's TMEM columns
+//     (layer 3 in 0..63, 2 in 64..127, 1 in 128..191, 0 in 192..223) and
+//     commits them to the buffer's mbarrier; the warps go on to chunk c + 1
+//     in the other buffer, and wait for that mbarrier only before they
+//     overwrite this buffer with chunk c + 2.
+// The MMA's rows are independent, so A rows past the layer's outputs are
+// whatever follows in shared memory (the next operand): they only make
+// accumulator rows that are never read.  At the end warps 0 and 1 read rows
+// 0..63 back (tcgen05.ld 32x32b) and add them to the FP32 gradients.  Waits
+// on the mbarriers are bounded as in the inference kernel: a CTA that gives
+// up adds nothing, frees its TMEM and is counted in g_tc_timeouts.
+constexpr int kWgK = 64;                   // samples per chunk
+constexpr int kWgTiles = kWgK / 16;        // tiles per chunk
+constexpr int kWgParts = 4;                // warps per tile
+constexpr int kWgWarps = kWgTiles * kWgParts;
+constexpr int kWgCols = 256;               // TMEM columns (224 used)
+constexpr int kWgPieces = kFragWords / 4;  // 16-byte pieces of a tile per lane
+constexpr int kWgPartPieces = kWgPieces / kWgParts;
+static_assert(kWgPieces % kWgParts == 0, "pieces per warp");
+constexpr uint32_t kWgTileBytes = uint32_t(kFragWords) * 32u * 4u;
+constexpr uint32_t kWgRow = kWgK * 2u;  // bytes per operand row
+// operands of one buffer, in fragment order; an M = 128 A operand reads 128
+// rows from its start, so A0 needs 128 rows of shared memory after it
+constexpr uint32_t kWgA3 = 0, kWgB3 = kWgA3 + kOut * kWgRow, kWgA2 = kWgB3 + kHid * kWgRow,
+                   kWgB2 = kWgA2 + kHid * kWgRow, kWgA1 = kWgB2 + kHid * kWgRow, kWgB1 = kWgA1 + kHid * kWgRow,
+                   kWgA0 = kWgB1 + kHid * kWgRow, kWgB0 = kWgA0 + kHid * kWgRow, kWgOps = kWgB0 + kIn * kWgRow;
+constexpr uint32_t kWgStage = 2 * kWgOps, kWgBar = kWgStage + 2u * kWgTiles * kWgTileBytes, kWgSlot = kWgBar + 16,
+                   kWgSmem = kWgSlot + 8;
+static_assert(kWgStage % 16 == 0 && kWgBar % 8 == 0 && kWgSmem <= 227 * 1024, "shared memory layout");
+static_assert(kWgOps + kWgA0 + 128 * kWgRow <= kWgBar, "the second buffer's A0 reads 128 rows inside the allocation");
+
+RT_D void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+RT_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+RT_D void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Operand offset of fragment piece i (the operands follow the fragment order:
+// A3 2 pieces, B3 4, A2 4, B2 4, A1 4, B1 4, A0 4, B0 2; a piece is a
+// 16-unit block, 16 rows of its operand).
+RT_D uint32_t wg_piece_rows(int i) {
+    static_assert(kFragAdo == 0 && kFragH3 == 8 && kFragE3 == 24 && kFragH2 == 40 && kFragE2 == 56 &&
+                      kFragH1 == 72 && kFragE1 == 88 && kFragAx == 104,
+                  "fragment order");
+    return uint32_t(i) * 16u * kWgRow;  // every piece is 16 rows of K-major operand in fragment order
+}
+
+// The staged pieces [p0, p0 + kWgPartPieces) of one tile (or zeros) into
+// the operand buffer `ops`, samples 16 * tile .. 16 * tile + 15.  Rows m
+// of piece i's operand: 16 (i - first piece of the operand) + 0..15; as the
+// operands are stored back to back in fragment order and a piece is a
+// 16-row block, the canonical offset of (operand row, k) within the buffer
+// is that of the piece's own 16-row block.
+RT_D void wg_stage(const unsigned char* stage, int p0, unsigned char* ops, int tile, int lane, bool valid) {
+#pragma unroll
+    for (int j = 0; j < kWgPartPieces; j++) {
+        const int i = p0 + j;
+        const uint4 q = valid ? *reinterpret_cast<const uint4*>(stage + (i * 32 + lane) * 16) : make_uint4(0u, 0u, 0u, 0u);
+        const uint32_t f[4] = {q.x, q.y, q.z, q.w};
+        unsigned char* blk = ops + wg_piece_rows(i);
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int m = 8 * (r >> 1) + (lane >> 2);
+            const int k = 16 * tile + 8 * (r & 1) + 2 * (lane & 3);
+            *reinterpret_cast<uint32_t*>(blk + tc_off(m, k, kWgK)) = trans8x8(f[r]);
+        }
+    }
+}
+
+// Rows 32 w .. 32 w + 31 of one layer's accumulators (N columns from `col`)
+// added to gW [M][N]; rows >= M are not the layer's.
+template <int M, int N>
+RT_D void wg_flush(uint32_t tmem, int col, int warp, int lane, float* __restrict__ gW) {
+    float v[N];
+    const uint32_t taddr = tmem + (uint32_t(32 * warp) << 16) + uint32_t(col);
+    if constexpr (N == 64)
+        tmem_ld_x64(taddr, v);
+    else
+        tmem_ld_x32(taddr, v);
+    const int m = 32 * warp + lane;
+    if (m >= M) return;
+    // one 16-byte reduction per four columns: the CTAs of the grid all add
+    // their partial sums at about the same time, and scalar atomics made
+    // this a third of the kernel's time
+#pragma unroll
+    for (int n = 0; n < N; n += 4)
+        if (v[n] != 0.f || v[n + 1] != 0.f || v[n + 2] != 0.f || v[n + 3] != 0.f)
+            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(gW + m * N + n), "f"(v[n]),
+                         "f"(v[n + 1]), "f"(v[n + 2]), "f"(v[n + 3])
+                         : "memory");
+}
+
+__global__ void __launch_bounds__(kWgWarps * 32, 1) k_guide_wgrad_tc(const uint32_t* __restrict__ frags, int tiles,
+                                                                     int chunk, float* __restrict__ grad_mlp) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int t0 = blockIdx.x * chunk, t1 = min(tiles, t0 + chunk);
+    if (t0 >= t1) return;  // the whole CTA
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = warp % kWgTiles, p0 = (warp / kWgTiles) * kWgPartPieces;
+    const uint32_t bar0 = smem_u32(sm + kWgBar), stage0 = smem_u32(sm + kWgStage);
+    auto stage_off = [&](int c) { return (uint32_t(c & 1) * kWgTiles + uint32_t(tile)) * kWgTileBytes; };
+    auto copy = [&](int c, int nchunks) {  // this lane's pieces of its tile of chunk c
+        const int tl = t0 + c * kWgTiles + tile;
+        if (c < nchunks && tl < t1) {
+            const uint4* src = reinterpret_cast<const uint4*>(frags + size_t(tl) * kFragWords * 32);
+            const uint32_t dst = stage0 + stage_off(c);
+            for (int i = p0; i < p0 + kWgPartPieces; i++) cp_async16(dst + uint32_t(i * 32 + lane) * 16u, src + i * 32 + lane);
+        }
+        cp_async_commit();  // one group per chunk, empty or not
+    };
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8u) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     ::"r"(smem_u32(sm + kWgSlot)), "r"(kWgCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    const int nchunks = (t1 - t0 + kWgTiles - 1) / kWgTiles;
+    copy(0, nchunks);
+    copy(1, nchunks);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kWgSlot);
+    bool ok = true;
+    for (int c = 0; c < nchunks && ok; c++) {
+        const int b = c & 1;
+        if (c >= 2) {  // the MMAs of chunk c - 2 have read this operand buffer
+            ok = __syncthreads_and(tc_wait(bar0 + 8u * uint32_t(b), uint32_t((c / 2 - 1) & 1))) != 0;
+            if (!ok) break;
+            tc_fence_after();
+        }
+        cp_async_wait_1();  // this lane's copies of chunk c have landed
+        wg_stage(sm + kWgStage + stage_off(c), p0, sm + b * kWgOps, tile, lane, t0 + c * kWgTiles + tile < t1);
+        copy(c + 2, nchunks);  // into the staging buffer this lane has just read
+        tc_fence_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (threadIdx.x == 0) {
+            const uint32_t ops = smem_u32(sm + b * kWgOps);
+            const uint32_t a[4] = {kWgA3, kWgA2, kWgA1, kWgA0}, bo[4] = {kWgB3, kWgB2, kWgB1, kWgB0};
+            const int n[4] = {kHid, kHid, kHid, kIn};
+#pragma unroll
+            for (int l = 0; l < 4; l++)
+#pragma unroll
+                for (int ks = 0; ks < kWgK / 16; ks++)
+                    tc_mma(tmem + uint32_t(64 * l), tc_desc(ops + a[l] + 256u * ks, 128u, kWgK * 16u),
+                           tc_desc(ops + bo[l] + 256u * ks, 128u, kWgK * 16u), tc_idesc(n[l]),
+                           (c > 0 || ks > 0) ? 1u : 0u);
+            tc_commit(bar0 + 8u * uint32_t(b));
+        }
+    }
+    if (ok) {  // the last commit arrives once every MMA of the CTA is done
+        const int last = nchunks - 1;
+        ok = __syncthreads_and(tc_wait(bar0 + 8u * uint32_t(last & 1), uint32_t((last / 2) & 1))) != 0;
+        tc_fence_after();
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy outlives the CTA
+    if (ok && warp < 2) {
+        wg_flush<kOut, kHid>(tmem, 0, warp, lane, grad_mlp + kW0 + kW1 + kW2);
+        wg_flush<kHid, kHid>(tmem, 64, warp, lane, grad_mlp + kW0 + kW1);
+        wg_flush<kHid, kHid>(tmem, 128, warp, lane, grad_mlp + kW0);
+        wg_flush<kHid, kIn>(tmem, 192, warp, lane, grad_mlp);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kWgCols) : "memory");
     if (!ok && threadIdx.x == 0) atomicAdd(&g_tc_timeouts, 1);
 }
 
@@ -1014,8 +1156,12 @@ size_t backward_smem() {
 }
 
 cudaError_t prepare_kernels() {
-    return cudaFuncSetAttribute(rtg::k_guide_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(backward_smem()));
+    cudaError_t e = cudaFuncSetAttribute(rtg::k_guide_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(backward_smem()));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(rtg::k_guide_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(rtg::kWgSmem));
+    return e;
 }
 
 // Inference CTAs per SM: 4 of 128 threads (122 registers each); with 64 TMEM
@@ -1044,7 +1190,7 @@ void launch_backward(const rtg::NetView& net, const float* pos, const float* dir
                      float scale, const float* weight_sum, float* grad_table, float* grad_mlp, float* loss,
                      uint32_t* frags, int frag_tiles, int sms, cudaStream_t st) {
     // chunks of at most frag_tiles tiles: the fused pass stores their
-    // fragments, then k_guide_wgrad turns them into weight gradients
+    // fragments, then k_guide_wgrad_tc turns them into weight gradients
     for (int begin = 0; begin < n; begin += frag_tiles * 16) {
         const int m = std::min(n - begin, frag_tiles * 16);
         const int tiles = (m + 15) / 16;
@@ -1053,9 +1199,12 @@ void launch_backward(const rtg::NetView& net, const float* pos, const float* dir
         rtg::k_guide_backward<<<blocks, rtg::kBwdWarps * 32, backward_smem(), st>>>(
             net, pos + size_t(begin) * 3, dir + size_t(begin) * 3, weight + begin, m, scale, weight_sum, grad_table,
             frags, loss);
-        const int chunk = std::max(4, (tiles + 2 * sms - 1) / (2 * sms));
-        rtg::k_guide_wgrad<<<(tiles + chunk - 1) / chunk, rtg::kWgradRoles * 32, 0, st>>>(frags, tiles, chunk,
-                                                                                          grad_mlp);
+        // one CTA per SM (224 KB of operands and staging, 256 TMEM columns),
+        // a multiple of four tiles each
+        int chunk = (tiles + sms - 1) / sms;
+        chunk = std::max(rtg::kWgTiles, (chunk + rtg::kWgTiles - 1) / rtg::kWgTiles * rtg::kWgTiles);
+        rtg::k_guide_wgrad_tc<<<(tiles + chunk - 1) / chunk, rtg::kWgWarps * 32, rtg::kWgSmem, st>>>(frags, tiles,
+                                                                                                    chunk, grad_mlp);
     }
 }
 

@@ -103,13 +103,17 @@ def test_forward_matches_oracle(n_max):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n_max", [64, 2048])
-def test_gradients_match_oracle(n_max):
+@pytest.mark.parametrize("n_max,n", [(64, 1024), (2048, 1024), (64, 1000), (2048, 40000)])
+def test_gradients_match_oracle(n_max, n):
+    """Weight and table gradients of n samples.  The weight gradients are
+    summed over 64-sample chunks on the tensor cores: 1000 samples end in a
+    partial tile and a chunk of three tiles, 40000 give every CTA several
+    chunks."""
     import optixrender_b200 as rt
     table, ws = _params(21, table_scale=0.5, out_scale=0.3)
     g = rt.Guide(max_resolution=n_max)
     g.set_params(table.reshape(-1), np.concatenate([w.reshape(-1) for w in ws]))
-    pos, d, w = _samples(1024, 22)
+    pos, d, w = _samples(n, 22)
     loss, gt, gm = g.gradients(pos, d, w)
     t16, w16 = _to16(table, ws)
     rloss, rgt, rgw, _ = go.loss_and_grads(t16, w16, pos, d, w.astype(np.float64), go.level_resolutions(n_max))
