@@ -86,9 +86,13 @@ def main(argv=None):
     ap.add_argument("--step", type=int, default=16)
     ap.add_argument("--train-spp", type=int, default=32)
     ap.add_argument("--target", type=float, default=1e-3)
-    ap.add_argument("--guide-prob", type=float, default=0.5, help="mixture selection probability")
+    # Mixture probability 0.15 and lobes up to kappa = e^6 instead of the
+    # library's 0.5 and e^4: on the 1080p spheres scene the time to relMSE
+    # 1e-3 was 16.1 s against 23.4 s (plain 11.8 s); a smaller probability
+    # gives the caustic directions only BSDF sampling finds less weight.
+    ap.add_argument("--guide-prob", type=float, default=0.15, help="mixture selection probability")
     ap.add_argument("--max-resolution", type=int, default=0, help="finest hash-grid level (0: the network's default)")
-    ap.add_argument("--max-log-kappa", type=float, default=0.0, help="sharpest lobe (0: the network's default)")
+    ap.add_argument("--max-log-kappa", type=float, default=6.0, help="sharpest lobe (0: the network's default, 4)")
     ap.add_argument("--ablations", default="",
                     help="extra guided runs sharing the reference, ';'-separated, each 'key=value,...' over "
                          "guide_prob, max_resolution, max_log_kappa, train_spp")
