@@ -233,9 +233,13 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
 // `src.finish(fin, i, tri, t, b1, b2, tri_v)` is called by the whole warp after
 // every step and stores the result of the lanes whose `fin` is set.
 // Measured on the 2.59M-triangle scene: refilling at 12 idle lanes beat 4, 8
-// and 16; postponing triangles below 20% of the lanes beat 10, 15, 30 and 40.
+// and 16; postponing triangles below 20% of the lanes beat 10, 15, 30 and 40
+// with one threshold for both kernels; apart, closest-hit rays do best at
+// 12% (k_extend 63.6 -> 63.0 ms per benchmark step) and shadow rays stay at
+// 20% (12%: 20.1 -> 21.0 ms).
 constexpr int kRefillLanes = 12;
-constexpr int kPostponePercent = 20;
+constexpr int kPostponePercentClosest = 12;
+constexpr int kPostponePercentAny = 20;
 // Threads per block of the persistent traversal kernels.
 constexpr int kTravBlock = 128;
 // Stack entries with this bit in x are postponed triangle groups
@@ -290,13 +294,14 @@ RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32
         if (Stats) nodes_visited++;
         s.g = make_uint2(cb, nb);
     }
-    // Triangle postponing (Ylitie et al. 2017): when fewer than
-    // kPostponePercent of the lanes in this step still test triangles, the
-    // rest of the group goes on the stack and the lane returns to node
+    // Triangle postponing (Ylitie et al. 2017): when fewer than the
+    // postponing percentage of the lanes in this step still test triangles,
+    // the rest of the group goes on the stack and the lane returns to node
     // traversal with the others (+7% paths/s on the 2.59M-triangle scene).
+    constexpr int kPostpone = AnyHit ? kPostponePercentAny : kPostponePercentClosest;
     const int n_step = __popc(__activemask());
     while (tbits) {
-        if (__popc(__activemask()) * 100 < kPostponePercent * n_step && st.sp < s.tri_room) {
+        if (__popc(__activemask()) * 100 < kPostpone * n_step && st.sp < s.tri_room) {
             st.push(make_uint2(tb | kTriGroup, tbits));
             break;
         }
