@@ -232,14 +232,16 @@ RT_D int traverse(const SceneView& sc, TravRay& r, float& t_hit, float& b1, floa
 // work remains.  `src.load(i, ray, scene)` fetches queue entry i;
 // `src.finish(fin, i, tri, t, b1, b2, tri_v)` is called by the whole warp after
 // every step and stores the result of the lanes whose `fin` is set.
-// Measured on the 2.59M-triangle scene: refilling at 12 idle lanes beat 4, 8
-// and 16; postponing triangles below 20% of the lanes beat 10, 15, 30 and 40
-// with one threshold for both kernels; apart, closest-hit rays do best at
-// 12% (k_extend 63.6 -> 63.0 ms per benchmark step) and shadow rays stay at
-// 20% (12%: 20.1 -> 21.0 ms).
-constexpr int kRefillLanes = 12;
+// Measured on the 2.59M-triangle scene: with one setting for both kernels,
+// refilling at 12 idle lanes beat 4, 8 and 16 and postponing triangles below
+// 20% of the lanes beat 10, 15, 30 and 40.  Apart (per benchmark step):
+// closest-hit rays do best at 12 lanes and 12% (k_extend 63.6 -> 63.0 ms;
+// 8% or 16 lanes 63.5 ms), shadow rays at 8 lanes and 30% (k_shadow 20.2 ->
+// 19.5 ms).
+constexpr int kRefillLanesClosest = 12;
+constexpr int kRefillLanesAny = 8;
 constexpr int kPostponePercentClosest = 12;
-constexpr int kPostponePercentAny = 20;
+constexpr int kPostponePercentAny = 30;
 // Threads per block of the persistent traversal kernels.
 constexpr int kTravBlock = 128;
 // Stack entries with this bit in x are postponed triangle groups
@@ -331,6 +333,7 @@ RT_D bool trav_step(TravState& s, TravStack& st, uint32_t& nodes_visited, uint32
 template <bool AnyHit, bool Stats, class Src>
 RT_D void traverse_queue(Src& src, int* fetch_counter, int total, uint32_t& nodes_visited, uint32_t& tris_tested,
                          uint32_t& rays, uint32_t& overflows) {
+    constexpr int kRefillLanes = AnyHit ? kRefillLanesAny : kRefillLanesClosest;
     const int lane = threadIdx.x & 31;
     TravStack st;
     st.sp = 0;
