@@ -785,67 +785,106 @@ __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_shadow(Ctx c) {
 // sample ends the pixel's launch (devicePrograms.cu:499-501); with PCG32 the
 // first sample of a pixel in the wave sums all of them and a NaN sample is
 // dropped alone.
-__global__ void k_resolve(Ctx c) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    const WaveParams& W = wave_of(c);
-    if (slot >= W.wave_count) return;
-    const Segment& sg = W.seg[find_segment(W, slot)];
-    const JobDesc* jd = c.jobs + sg.job;
-    const JobParams& j = jd->job;
-    const WaveBufs& B = c.wb;
-    int64_t p = sg.path_begin + (slot - sg.slot_begin);
-    int pix = int(p % j.npix);
-    if (j.rng == RT_RNG_LCG) {
-        uint2 rs = B.rng[slot];
-        j.lcg_state[pix] = rs.x;
-        float4 acc = j.acc_color[pix];
-        if (acc.w != 0.0f) return;
-        v3 r = xyz(B.rad[slot]);
-        r += xyz(B.nee0[slot]);
-        r += xyz(B.nee1[slot]);
-        if (any_nan(r)) {
-            j.acc_color[pix].w = 1.0f;
-            atomicAdd(&B.ctl->stats[6], 1ull);
-            return;
+// The slots resolve works on, segment after segment: every slot of an LCG
+// segment (at most one sample per pixel), the first npix slots of a PCG32
+// segment (the first sample of each of its pixels).  Item t lies in segment
+// *sgi at slot *slot; false once t is past the last item.
+RT_D bool resolve_item(const Ctx& c, const WaveParams& W, int t, int* sgi, int* slot) {
+    for (int i = 0; i < W.num_seg; i++) {
+        const Segment& sg = W.seg[i];
+        const JobParams& j = c.jobs[sg.job].job;
+        const int items = j.rng == RT_RNG_LCG ? sg.count : int(min(int64_t(sg.count), j.npix));
+        if (t < items) {
+            *sgi = i;
+            *slot = sg.slot_begin + t;
+            return true;
         }
-        float4 a = B.aov_a[slot];
-        float2 n = B.aov_n[slot];
-        j.acc_color[pix] = make_float4(acc.x + r.x, acc.y + r.y, acc.z + r.z, 0.0f);
-        float4 aa = j.acc_albedo[pix], an = j.acc_normal[pix];
-        j.acc_albedo[pix] = make_float4(aa.x + a.x, aa.y + a.y, aa.z + a.z, 0.f);
-        j.acc_normal[pix] = make_float4(an.x + a.w, an.y + n.x, an.z + n.y, 0.f);
-        return;
+        t -= items;
     }
-    // PCG32: is this the first sample of `pix` inside the segment?
-    int64_t first = sg.path_begin;
-    if (p - j.npix >= first) return;
-    float4 acc = j.acc_color[pix], aa = j.acc_albedo[pix], an = j.acc_normal[pix];
-    int64_t end = sg.path_begin + sg.count;
+    return false;
+}
+
+// One path's sample: radiance, the two pending NEE terms, first-hit AOVs.
+struct ResolveSample {
+    float4 r, e, f, a;
+    float2 n;
+};
+RT_D ResolveSample resolve_load(const WaveBufs& B, int sl) {
+    return ResolveSample{B.rad[sl], B.nee0[sl], B.nee1[sl], B.aov_a[sl], B.aov_n[sl]};
+}
+// Adds the sample to the sums; a NaN sample is left out (returns false).
+RT_D bool resolve_add(const ResolveSample& x, float4& acc, float4& aa, float4& an) {
+    v3 r = xyz(x.r);
+    r += xyz(x.e);
+    r += xyz(x.f);
+    if (any_nan(r)) return false;
+    acc.x += r.x;
+    acc.y += r.y;
+    acc.z += r.z;
+    aa.x += x.a.x;
+    aa.y += x.a.y;
+    aa.z += x.a.z;
+    an.x += x.a.w;
+    an.y += x.n.x;
+    an.z += x.n.y;
+    return true;
+}
+
+// A grid-stride loop over the wave's resolve items (a fixed grid: launching
+// a thread per slot left all but the first sample's threads of a PCG32
+// wave, 31 of 32 on the benchmark frame, to be scheduled only to return).
+__global__ void __launch_bounds__(256) k_resolve(Ctx c) {
+    const WaveParams& W = wave_of(c);
+    const WaveBufs& B = c.wb;
     unsigned nans = 0;
-    for (int64_t q = p; q < end; q += j.npix) {
-        int sl = sg.slot_begin + int(q - sg.path_begin);
-        v3 r = xyz(B.rad[sl]);
-        r += xyz(B.nee0[sl]);
-        r += xyz(B.nee1[sl]);
-        if (any_nan(r)) {
-            nans++;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x;; t += gridDim.x * blockDim.x) {
+        int sgi = 0, slot = 0;
+        if (!resolve_item(c, W, t, &sgi, &slot)) break;
+        const Segment& sg = W.seg[sgi];
+        const JobParams& j = c.jobs[sg.job].job;
+        const int64_t p = sg.path_begin + (slot - sg.slot_begin);
+        const int pix = int(p % j.npix);
+        if (j.rng == RT_RNG_LCG) {
+            uint2 rs = B.rng[slot];
+            j.lcg_state[pix] = rs.x;
+            float4 acc = j.acc_color[pix];
+            if (acc.w != 0.0f) continue;
+            v3 r = xyz(B.rad[slot]);
+            r += xyz(B.nee0[slot]);
+            r += xyz(B.nee1[slot]);
+            if (any_nan(r)) {
+                j.acc_color[pix].w = 1.0f;
+                nans++;
+                continue;
+            }
+            float4 a = B.aov_a[slot];
+            float2 n = B.aov_n[slot];
+            j.acc_color[pix] = make_float4(acc.x + r.x, acc.y + r.y, acc.z + r.z, 0.0f);
+            float4 aa = j.acc_albedo[pix], an = j.acc_normal[pix];
+            j.acc_albedo[pix] = make_float4(aa.x + a.x, aa.y + a.y, aa.z + a.z, 0.f);
+            j.acc_normal[pix] = make_float4(an.x + a.w, an.y + n.x, an.z + n.y, 0.f);
             continue;
         }
-        float4 a = B.aov_a[sl];
-        float2 n = B.aov_n[sl];
-        acc.x += r.x;
-        acc.y += r.y;
-        acc.z += r.z;
-        aa.x += a.x;
-        aa.y += a.y;
-        aa.z += a.z;
-        an.x += a.w;
-        an.y += n.x;
-        an.z += n.y;
+        // PCG32: this pixel's samples in the segment, in sample order
+        float4 acc = j.acc_color[pix], aa = j.acc_albedo[pix], an = j.acc_normal[pix];
+        const int64_t end = sg.path_begin + sg.count;
+        const int step = int(j.npix);
+        int sl = slot;
+        int64_t q = p;
+        // four samples' loads in flight at a time; the sums keep sample order
+        for (; q + 3 * j.npix < end; q += 4 * j.npix, sl += 4 * step) {
+            const ResolveSample x0 = resolve_load(B, sl), x1 = resolve_load(B, sl + step),
+                                x2 = resolve_load(B, sl + 2 * step), x3 = resolve_load(B, sl + 3 * step);
+            nans += resolve_add(x0, acc, aa, an) ? 0u : 1u;
+            nans += resolve_add(x1, acc, aa, an) ? 0u : 1u;
+            nans += resolve_add(x2, acc, aa, an) ? 0u : 1u;
+            nans += resolve_add(x3, acc, aa, an) ? 0u : 1u;
+        }
+        for (; q < end; q += j.npix, sl += step) nans += resolve_add(resolve_load(B, sl), acc, aa, an) ? 0u : 1u;
+        j.acc_color[pix] = acc;
+        j.acc_albedo[pix] = aa;
+        j.acc_normal[pix] = an;
     }
-    j.acc_color[pix] = acc;
-    j.acc_albedo[pix] = aa;
-    j.acc_normal[pix] = an;
     if (nans) atomicAdd(&B.ctl->stats[6], (unsigned long long)nans);
 }
 
@@ -1277,7 +1316,10 @@ void launch_shadow(const Ctx& c, const LaunchShape& s, bool stats, cudaStream_t 
     else
         k_shadow<false><<<s.blocks_shadow, kBlock, 0, st>>>(c);
 }
-void launch_resolve(const Ctx& c, cudaStream_t st) { k_resolve<<<grid_for(c.wb.capacity, 256), 256, 0, st>>>(c); }
+void launch_resolve(const Ctx& c, cudaStream_t st) {
+    // enough threads for a few items each on the benchmark frame (2M pixels)
+    k_resolve<<<std::min(grid_for(c.wb.capacity, 256), 2048u), 256, 0, st>>>(c);
+}
 void launch_next_wave(const Ctx& c, cudaStream_t st) { k_next_wave<<<1, 1, 0, st>>>(c.wave_index, c.wave_ring); }
 void launch_finalize(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_finalize<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
