@@ -257,6 +257,17 @@ struct rt_renderer {
     uint32_t guide_seed = 1;
     bool graph_guided = false;
     const void* graph_mix = nullptr;
+    // Pinned staging of each Render()'s launch parameters and wave table, so
+    // that their copies are true asynchronous DMA; a ring, so that the host
+    // can queue a few frames ahead before it waits for a buffer's last copy.
+    struct HostStage {
+        void* ptr = nullptr;
+        size_t bytes = 0;
+        cudaEvent_t copied = nullptr;  // recorded after the copies that read ptr
+    };
+    static constexpr int kStages = 3;
+    HostStage stage[kStages];
+    int stage_next = 0;
 };
 
 namespace {
@@ -480,6 +491,10 @@ rt_status rt_renderer_destroy(rt_renderer* r) {
     if (r->ev1) cudaEventDestroy(r->ev1);
     if (r->fork.side) cudaStreamSynchronize(r->fork.side);
     rth::destroy_fork(r->fork);
+    for (auto& hs : r->stage) {
+        if (hs.copied) cudaEventDestroy(hs.copied);
+        if (hs.ptr) cudaFreeHost(hs.ptr);
+    }
     if (r->own_stream && r->stream) cudaStreamDestroy(r->stream);
     delete r;
     return RT_OK;
@@ -591,7 +606,6 @@ rt_status rt_renderer_render(rt_renderer* r) {
     j.rgba8 = r->rgba8.as<uint32_t>();
     r->frame++;
     cudaStream_t s = r->stream;
-    RT_CUDA(cudaMemcpyAsync(r->job.ptr, &hj, sizeof(hj), cudaMemcpyHostToDevice, s), "upload launch parameters");
     const int64_t trained_paths = train_waves * npix;
     const int64_t nwaves = train_waves + (total - trained_paths + cap - 1) / cap;
     std::vector<WaveParams> waves(static_cast<size_t>(nwaves));
@@ -608,8 +622,26 @@ rt_status rt_renderer_render(rt_renderer* r) {
         begin += wp.wave_count;
     }
     RT_CUDA(r->segs.alloc(waves.size() * sizeof(WaveParams)), "allocate wave table");
-    RT_CUDA(cudaMemcpyAsync(r->segs.ptr, waves.data(), waves.size() * sizeof(WaveParams), cudaMemcpyHostToDevice, s),
-            "upload wave table");
+    {  // launch parameters and wave table through the next pinned staging buffer
+        rt_renderer::HostStage& hs = r->stage[r->stage_next];
+        r->stage_next = (r->stage_next + 1) % rt_renderer::kStages;
+        const size_t wbytes = waves.size() * sizeof(WaveParams), need = sizeof(hj) + wbytes;
+        if (hs.copied) RT_CUDA(cudaEventSynchronize(hs.copied), "staging buffer reuse");
+        if (hs.bytes < need) {
+            if (hs.ptr) cudaFreeHost(hs.ptr);
+            hs.ptr = nullptr;
+            hs.bytes = 0;
+            RT_CUDA(cudaHostAlloc(&hs.ptr, need, cudaHostAllocDefault), "allocate pinned staging");
+            hs.bytes = need;
+        }
+        if (!hs.copied) RT_CUDA(cudaEventCreateWithFlags(&hs.copied, cudaEventDisableTiming), "staging event");
+        char* h = static_cast<char*>(hs.ptr);
+        std::memcpy(h, &hj, sizeof(hj));
+        std::memcpy(h + sizeof(hj), waves.data(), wbytes);
+        RT_CUDA(cudaMemcpyAsync(r->job.ptr, h, sizeof(hj), cudaMemcpyHostToDevice, s), "upload launch parameters");
+        RT_CUDA(cudaMemcpyAsync(r->segs.ptr, h + sizeof(hj), wbytes, cudaMemcpyHostToDevice, s), "upload wave table");
+        RT_CUDA(cudaEventRecord(hs.copied, s), "staging event");
+    }
     r->h2d_bytes = int64_t(sizeof(hj) + waves.size() * sizeof(WaveParams));
     if (!r->wave_index.ptr) RT_CUDA(r->wave_index.alloc(sizeof(int)), "allocate wave counter");
     RT_CUDA(cudaMemsetAsync(r->wave_index.ptr, 0, sizeof(int), s), "clear wave counter");
