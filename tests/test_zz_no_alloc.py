@@ -1,6 +1,9 @@
 """rt_renderer_trace_noalloc: the ray queries of rt_renderer_trace (host
 buffers) staged in the library's fixed device array instead of buffers
-allocated per call.
+allocated per call.  It serves callers that cannot allocate device memory
+during a query: a render or serving loop whose other streams must not be
+stalled by the device-wide synchronisation of cudaMalloc/cudaFree, and a
+process whose own memory pool already holds the rest of the GPU's memory.
 
 Tolerance: the same traversal code runs on the same wide BVH, so primitive ids
 must be identical and t, u, v equal within 1e-6 relative (they are expected to
