@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(kRaygenBlock) k_raygen(Ctx c) {
     if (slot == 0) {
         ctl->count[0] = W.wave_count;
         ctl->count[1] = 0;
-        ctl->shadow_count = 0;
+        ctl->shadow_count[0] = 0;
+        ctl->shadow_count[1] = 0;
         ctl->fetch_ext = 0;
         ctl->fetch_shade = 0;
         ctl->fetch_shadow = 0;
@@ -637,12 +638,12 @@ __global__ void __launch_bounds__(kBlock) k_shade(Ctx c) {
         if (cont) B.queue[nxt][qp] = slot;
         int sp = warp_append(&ctl->sample_count, defer, lane);
         if (defer) B.squeue[sp] = slot;
-        int p0 = warp_append(&ctl->shadow_count, sh0, lane);
+        int p0 = warp_append(&ctl->shadow_count[cur], sh0, lane);
         if (sh0) {
             B.sh_o[p0] = f4(s0o, s0t);
             B.sh_d[p0] = f4(s0d, __int_as_float(slot * 2 + 0));
         }
-        int p1 = warp_append(&ctl->shadow_count, sh1, lane);
+        int p1 = warp_append(&ctl->shadow_count[cur], sh1, lane);
         if (sh1) {
             B.sh_o[p1] = f4(s1o, s1t);
             B.sh_d[p1] = f4(s1d, __int_as_float(slot * 2 + 1));
@@ -668,12 +669,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_sample(Ctx c) {
     const int bounce = c.bounce;
     const int total = ctl->sample_count;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // k_shade is done with these: this bounce's shadow queue length moves
-        // to shadow_total for k_shadow, and the counters the next k_extend and
-        // k_shade append to start from zero here, so that k_shadow and the next
-        // k_extend share no counter and may run side by side
-        ctl->shadow_total = ctl->shadow_count;
-        ctl->shadow_count = 0;
+        // the next k_shade appends its shadow rays to entry nxt (k_shadow of
+        // the bounce before it has finished), the next k_extend its paths to
+        // the shade buckets; this bounce's k_shadow, which may run beside this
+        // kernel, reads entry bounce & 1 only
+        ctl->shadow_count[nxt] = 0;
         for (int b = 0; b < kShadeBuckets; b++) ctl->bucket[b] = 0;
     }
     const WaveBufs& B = c.wb;
@@ -767,7 +767,7 @@ struct ShadowSrc {
 template <bool Stats>
 __global__ void __launch_bounds__(kBlock, kTravMinBlocks) k_shadow(Ctx c) {
     WaveCtl* ctl = c.wb.ctl;
-    const int total = ctl->shadow_total;
+    const int total = ctl->shadow_count[c.bounce & 1];
     uint32_t nodes = 0, tris = 0, rays = 0, overflows = 0;
     ShadowSrc src{&c};
     traverse_queue<true, Stats>(src, &ctl->fetch_shadow, total, nodes, tris, rays, overflows);
@@ -1078,8 +1078,8 @@ __global__ void k_query_stage(Ctx c, const float4* __restrict__ rays, int n, int
     if (i == 0) {
         ctl->count[0] = any_hit ? 0 : n;
         ctl->count[1] = 0;
-        ctl->shadow_count = 0;
-        ctl->shadow_total = any_hit ? n : 0;
+        ctl->shadow_count[0] = any_hit ? n : 0;
+        ctl->shadow_count[1] = 0;
         ctl->fetch_ext = 0;
         ctl->fetch_shade = 0;
         ctl->fetch_shadow = 0;
@@ -1250,8 +1250,9 @@ static unsigned grid_for(int64_t n, int block) { return unsigned((n + block - 1)
 void launch_begin(const JobDesc& hj, const JobDesc* dj, cudaStream_t st) {
     k_begin<<<grid_for(hj.job.npix, 256), 256, 0, st>>>(dj);
 }
-void launch_shadow_and_next_extend(Ctx c, const LaunchShape& s, cudaStream_t st, const WaveFork* f) {
+void launch_sample_shadow_and_next_extend(Ctx c, const LaunchShape& s, cudaStream_t st, const WaveFork* f) {
     if (f == nullptr) {
+        launch_sample(c, s, false, st);
         launch_shadow(c, s, false, st);
         c.bounce += 1;
         launch_extend(c, s, false, st);
@@ -1261,6 +1262,7 @@ void launch_shadow_and_next_extend(Ctx c, const LaunchShape& s, cudaStream_t st,
     cudaStreamWaitEvent(f->side, f->fork, 0);
     launch_shadow(c, s, false, f->side);
     cudaEventRecord(f->join, f->side);
+    launch_sample(c, s, false, st);
     c.bounce += 1;
     launch_extend(c, s, false, st);
     cudaStreamWaitEvent(st, f->join, 0);

@@ -51,7 +51,10 @@ struct Segment {
 
 struct WaveCtl {
     int count[2];
-    int shadow_count;
+    // shadow rays queued by k_shade at bounces of parity 0 / 1: k_shadow of
+    // bounce b reads entry b & 1 while k_sample of bounce b clears entry
+    // (b + 1) & 1 for the next k_shade, so the two kernels may run side by side
+    int shadow_count[2];
     int fetch_ext;
     int fetch_shade;
     int fetch_shadow;
@@ -62,7 +65,6 @@ struct WaveCtl {
     int bucket[kShadeBuckets];    // extend results per shade bucket
     int sample_count;             // paths k_shade left at BSDF sampling (k_sample's queue)
     int fetch_sample;
-    int shadow_total;             // length of this bounce's shadow queue, taken by k_sample from shadow_count
 };
 
 // Per-slot path state of a wave.  A slot's eight float4 fields of path state lie together in one 128-byte
@@ -181,17 +183,18 @@ struct WaveFork {
     cudaStream_t side;
     cudaEvent_t fork, join;
 };
-// The shadow rays of bounce c.bounce and the closest hits of the next bounce
-// share no data: k_shadow reads the shadow queue and its length
-// (shadow_total) and clears the NEE fields of occluded slots; k_extend reads
-// the path queue and writes the hit fields, the shade buckets and the
-// counters of the next k_shade and k_sample; the counters either used to
-// reset for the other (shadow_count, the buckets) are reset by k_sample
-// before both.  So with `f` k_shadow runs on f->side as a parallel branch of
-// the stream (or of the wave's graph when capturing), joined back before the
-// next k_shade, and the tail of one kernel overlaps the other.  Without `f`
-// the two run one after the other on `st`.
-void launch_shadow_and_next_extend(rtd::Ctx c, const LaunchShape& s, cudaStream_t st, const WaveFork* f);
+// After k_shade of bounce c.bounce: its shadow rays, and its BSDF sampling
+// followed by the next bounce's closest hits, share no data: k_shadow reads
+// the shadow queue and its length (shadow_count[bounce & 1]) and clears the
+// NEE fields of occluded slots; k_sample reads and writes the other fields of
+// the slots it samples and clears shadow_count[(bounce + 1) & 1] and the
+// shade buckets; k_extend reads the path queue and writes the hit fields,
+// the shade buckets and the counters of the next k_shade and k_sample.  So
+// with `f` k_shadow runs on f->side as a parallel branch of the stream (or of
+// the wave's graph when capturing), joined back before the next k_shade, and
+// the kernels fill each other's tails.  Without `f` the three run one after
+// the other on `st`.
+void launch_sample_shadow_and_next_extend(rtd::Ctx c, const LaunchShape& s, cudaStream_t st, const WaveFork* f);
 cudaError_t create_fork(WaveFork& f);  // on the current device; on failure nothing stays allocated
 void destroy_fork(WaveFork& f);
 void launch_resolve(const rtd::Ctx& c, cudaStream_t st);

@@ -703,17 +703,18 @@ rt_status rt_renderer_render(rt_renderer* r) {
                 r->timer.marks.push_back({3, i0 + 2});
                 r->timer.marks.push_back({2, i0 + 3});
             }
-        } else {  // a bounce's k_shadow beside the next bounce's k_extend
+        } else {  // a bounce's k_shadow beside its k_sample and the next bounce's k_extend
             rth::launch_extend(c, r->shape, false, s);
             for (int bnc = 0; bnc < o.max_depth; bnc++) {
                 c.bounce = bnc;
                 if (guided) rtgh::launch_infer(c, net, gsms, s);
                 rth::launch_shade(c, r->shape, false, s);
-                rth::launch_sample(c, r->shape, false, s);
-                if (bnc + 1 < o.max_depth)
-                    rth::launch_shadow_and_next_extend(c, r->shape, s, r->have_fork ? &r->fork : nullptr);
-                else
+                if (bnc + 1 < o.max_depth) {
+                    rth::launch_sample_shadow_and_next_extend(c, r->shape, s, r->have_fork ? &r->fork : nullptr);
+                } else {
+                    rth::launch_sample(c, r->shape, false, s);
                     rth::launch_shadow(c, r->shape, false, s);
+                }
             }
         }
         rth::launch_resolve(c, s);

@@ -308,11 +308,12 @@ void issue_wave(rt_server* s, const Ctx& c0, int depth, int gscene, bool trainin
         c.bounce = b;
         if (gscene >= 0) rtgh::launch_infer(c, net, gsms, s->stream);
         rth::launch_shade(c, s->shape, false, s->stream);
-        rth::launch_sample(c, s->shape, false, s->stream);
-        if (b + 1 < depth)  // this bounce's k_shadow beside the next bounce's k_extend
-            rth::launch_shadow_and_next_extend(c, s->shape, s->stream, &s->fork);
-        else
+        if (b + 1 < depth) {  // this bounce's k_shadow beside its k_sample and the next bounce's k_extend
+            rth::launch_sample_shadow_and_next_extend(c, s->shape, s->stream, &s->fork);
+        } else {
+            rth::launch_sample(c, s->shape, false, s->stream);
             rth::launch_shadow(c, s->shape, false, s->stream);
+        }
     }
     rth::launch_resolve(c, s->stream);
     if (training)
